@@ -1,0 +1,345 @@
+/* tacuda-b200: B200-native (sm_100a) implementation of TACUDA's batched
+ * indicator path behind its C ABI.
+ *
+ * Every declaration below except the ct_b200_* block keeps the name, argument
+ * list, argument meaning and status codes of the reference's include/tacuda.h
+ * (TACUDA 0.9.3) or include/tacuda_device.h; the comment beside each gives the
+ * reference line it replaces. Matrices are series-major (numSeries rows of
+ * seriesLen float32, row i contiguous) in device memory owned by the caller.
+ * stream == 0 is the legacy default stream: the call is ordered after prior
+ * work on it and returns when the batch is done. A non-null stream only
+ * enqueues work (no host synchronisation) and, apart from the first call on a
+ * device, allocates nothing, so it can be captured in a CUDA graph.
+ * maxConcurrency is accepted for compatibility and ignored: every batch call
+ * is one kernel launch.
+ *
+ * The ct_b200_* block is append-only new surface (multi-indicator fused
+ * launches, ragged rows through a plan, int32 candles, per-series alpha with
+ * its adjoint); the reference has no counterpart for it.
+ */
+#ifndef TACUDA_B200_H
+#define TACUDA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+#if defined(_WIN32)
+#define CTAPI_EXPORT __declspec(dllexport)
+#else
+#define CTAPI_EXPORT __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* include/tacuda.h:32-40 */
+typedef enum ctStatus {
+  CT_STATUS_SUCCESS = 0,
+  CT_STATUS_ALLOC_FAILED = 1,
+  CT_STATUS_COPY_FAILED = 2,
+  CT_STATUS_KERNEL_FAILED = 3,
+  CT_STATUS_INVALID_ARGUMENT = 4,
+  CT_STATUS_DEVICE_ERROR = 5,
+  CT_STATUS_UNSUPPORTED = 6,
+} ctStatus_t;
+
+CTAPI_EXPORT const char* ct_status_string(ctStatus_t status); /* tacuda.h:45 */
+CTAPI_EXPORT const char* ct_get_last_error(void);             /* tacuda.h:54 */
+CTAPI_EXPORT const char* ct_version(void);                    /* tacuda.h:70 */
+
+/* ---- device batch API (include/tacuda.h:893-2950) ---- */
+
+CTAPI_EXPORT ctStatus_t ct_sma_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:904 */
+CTAPI_EXPORT ctStatus_t ct_ema_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:909 */
+CTAPI_EXPORT ctStatus_t ct_wma_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:958 */
+CTAPI_EXPORT ctStatus_t ct_rsi_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:914 */
+CTAPI_EXPORT ctStatus_t ct_atr_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int period, float initial, int maxConcurrency, cudaStream_t stream); /* tacuda.h:919 */
+CTAPI_EXPORT ctStatus_t ct_macd_batch_d(const float *d_inputs, float *d_macds, float *d_signals, float *d_hists, int seriesLen, int numSeries, int fastPeriod, int slowPeriod, int signalPeriod, int maType, int maxConcurrency, cudaStream_t stream); /* tacuda.h:926 */
+CTAPI_EXPORT ctStatus_t ct_bbands_batch_d(const float *d_inputs, float *d_uppers, float *d_middles, float *d_lowers, int seriesLen, int numSeries, int period, float upperMul, float lowerMul, int maxConcurrency, cudaStream_t stream); /* tacuda.h:933 */
+CTAPI_EXPORT ctStatus_t ct_stochastic_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, float *d_ks, float *d_ds, int seriesLen, int numSeries, int kPeriod, int dPeriod, int maxConcurrency, cudaStream_t stream); /* tacuda.h:940 */
+CTAPI_EXPORT ctStatus_t ct_dema_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:967 */
+CTAPI_EXPORT ctStatus_t ct_tema_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:977 */
+CTAPI_EXPORT ctStatus_t ct_t3_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, float vFactor, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1169 */
+CTAPI_EXPORT ctStatus_t ct_stddev_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1055 */
+CTAPI_EXPORT ctStatus_t ct_var_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1065 */
+CTAPI_EXPORT ctStatus_t ct_sum_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1074 */
+CTAPI_EXPORT ctStatus_t ct_max_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1083 */
+CTAPI_EXPORT ctStatus_t ct_min_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1092 */
+CTAPI_EXPORT ctStatus_t ct_linearreg_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1101 */
+CTAPI_EXPORT ctStatus_t ct_natr_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1180 */
+CTAPI_EXPORT ctStatus_t ct_adx_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1194 */
+CTAPI_EXPORT ctStatus_t ct_dx_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1221 */
+CTAPI_EXPORT ctStatus_t ct_willr_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1262 */
+CTAPI_EXPORT ctStatus_t ct_cci_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1276 */
+CTAPI_EXPORT ctStatus_t ct_trange_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1288 */
+CTAPI_EXPORT ctStatus_t ct_obv_batch_d(const float *d_closes, const float *d_volumes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1440 */
+CTAPI_EXPORT ctStatus_t ct_mfi_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, const float *d_volumes, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1453 */
+CTAPI_EXPORT ctStatus_t ct_ad_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, const float *d_volumes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1468 */
+CTAPI_EXPORT ctStatus_t ct_adosc_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, const float *d_volumes, float *d_outputs, int seriesLen, int numSeries, int fastPeriod, int slowPeriod, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1483 */
+CTAPI_EXPORT ctStatus_t ct_correl_batch_d(const float *d_xs, const float *d_ys, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1826 */
+
+/* candlestick patterns: float signal (+-100/+-80/+-200), warm-up 0 */
+CTAPI_EXPORT ctStatus_t ct_cdl_doji_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1877 */
+CTAPI_EXPORT ctStatus_t ct_cdl_hammer_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1891 */
+CTAPI_EXPORT ctStatus_t ct_cdl_inverted_hammer_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1908 */
+CTAPI_EXPORT ctStatus_t ct_cdl_bullish_engulfing_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1926 */
+CTAPI_EXPORT ctStatus_t ct_cdl_bearish_engulfing_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1944 */
+CTAPI_EXPORT ctStatus_t ct_cdl_three_white_soldiers_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1962 */
+CTAPI_EXPORT ctStatus_t ct_cdl_abandoned_baby_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1980 */
+CTAPI_EXPORT ctStatus_t ct_cdl_advance_block_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1998 */
+CTAPI_EXPORT ctStatus_t ct_cdl_belt_hold_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2015 */
+CTAPI_EXPORT ctStatus_t ct_cdl_breakaway_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2031 */
+CTAPI_EXPORT ctStatus_t ct_cdl_two_crows_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2047 */
+CTAPI_EXPORT ctStatus_t ct_cdl_three_black_crows_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2064 */
+CTAPI_EXPORT ctStatus_t ct_cdl_three_inside_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2081 */
+CTAPI_EXPORT ctStatus_t ct_cdl_three_outside_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2099 */
+CTAPI_EXPORT ctStatus_t ct_cdl_three_line_strike_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2117 */
+CTAPI_EXPORT ctStatus_t ct_cdl_three_stars_in_south_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2135 */
+CTAPI_EXPORT ctStatus_t ct_cdl_closing_marubozu_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2153 */
+CTAPI_EXPORT ctStatus_t ct_cdl_conceal_baby_swallow_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2171 */
+CTAPI_EXPORT ctStatus_t ct_cdl_counterattack_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2189 */
+CTAPI_EXPORT ctStatus_t ct_cdl_dark_cloud_cover_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2207 */
+CTAPI_EXPORT ctStatus_t ct_cdl_doji_star_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2224 */
+CTAPI_EXPORT ctStatus_t ct_cdl_dragonfly_doji_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2241 */
+CTAPI_EXPORT ctStatus_t ct_cdl_engulfing_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2258 */
+CTAPI_EXPORT ctStatus_t ct_cdl_evening_doji_star_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2275 */
+CTAPI_EXPORT ctStatus_t ct_cdl_evening_star_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2292 */
+CTAPI_EXPORT ctStatus_t ct_cdl_gap_side_side_white_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2310 */
+CTAPI_EXPORT ctStatus_t ct_cdl_gravestone_doji_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2328 */
+CTAPI_EXPORT ctStatus_t ct_cdl_hanging_man_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2345 */
+CTAPI_EXPORT ctStatus_t ct_cdl_harami_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2361 */
+CTAPI_EXPORT ctStatus_t ct_cdl_harami_cross_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2377 */
+CTAPI_EXPORT ctStatus_t ct_cdl_high_wave_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2394 */
+CTAPI_EXPORT ctStatus_t ct_cdl_hikkake_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2410 */
+CTAPI_EXPORT ctStatus_t ct_cdl_hikkake_mod_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2426 */
+CTAPI_EXPORT ctStatus_t ct_cdl_homing_pigeon_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2444 */
+CTAPI_EXPORT ctStatus_t ct_cdl_identical_three_crows_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2462 */
+CTAPI_EXPORT ctStatus_t ct_cdl_in_neck_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2479 */
+CTAPI_EXPORT ctStatus_t ct_cdl_kicking_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2495 */
+CTAPI_EXPORT ctStatus_t ct_cdl_kicking_by_length_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2512 */
+CTAPI_EXPORT ctStatus_t ct_cdl_ladder_bottom_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2530 */
+CTAPI_EXPORT ctStatus_t ct_cdl_long_legged_doji_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2548 */
+CTAPI_EXPORT ctStatus_t ct_cdl_long_line_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2565 */
+CTAPI_EXPORT ctStatus_t ct_cdl_marubozu_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2581 */
+CTAPI_EXPORT ctStatus_t ct_cdl_matching_low_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2597 */
+CTAPI_EXPORT ctStatus_t ct_cdl_mat_hold_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2614 */
+CTAPI_EXPORT ctStatus_t ct_cdl_morning_doji_star_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2631 */
+CTAPI_EXPORT ctStatus_t ct_cdl_morning_star_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2648 */
+CTAPI_EXPORT ctStatus_t ct_cdl_on_neck_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2665 */
+CTAPI_EXPORT ctStatus_t ct_cdl_piercing_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2681 */
+CTAPI_EXPORT ctStatus_t ct_cdl_rickshaw_man_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2697 */
+CTAPI_EXPORT ctStatus_t ct_cdl_rise_fall3_methods_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2715 */
+CTAPI_EXPORT ctStatus_t ct_cdl_separating_lines_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2733 */
+CTAPI_EXPORT ctStatus_t ct_cdl_shooting_star_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2751 */
+CTAPI_EXPORT ctStatus_t ct_cdl_short_line_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2768 */
+CTAPI_EXPORT ctStatus_t ct_cdl_spinning_top_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2784 */
+CTAPI_EXPORT ctStatus_t ct_cdl_stalled_pattern_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2802 */
+CTAPI_EXPORT ctStatus_t ct_cdl_stick_sandwich_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2820 */
+CTAPI_EXPORT ctStatus_t ct_cdl_takuri_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2836 */
+CTAPI_EXPORT ctStatus_t ct_cdl_tasuki_gap_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2852 */
+CTAPI_EXPORT ctStatus_t ct_cdl_thrusting_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2868 */
+CTAPI_EXPORT ctStatus_t ct_cdl_tristar_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2884 */
+CTAPI_EXPORT ctStatus_t ct_cdl_unique_3_river_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2901 */
+CTAPI_EXPORT ctStatus_t ct_cdl_upside_gap_2_crows_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2919 */
+CTAPI_EXPORT ctStatus_t ct_cdl_xside_gap_3_methods_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:2937 */
+
+/* ---- single-series device API (include/tacuda_device.h:130-540) ---- */
+CTAPI_EXPORT ctStatus_t ct_sma_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:130 */
+CTAPI_EXPORT ctStatus_t ct_ema_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:136 */
+CTAPI_EXPORT ctStatus_t ct_wma_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:142 */
+CTAPI_EXPORT ctStatus_t ct_dema_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:145 */
+CTAPI_EXPORT ctStatus_t ct_tema_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:148 */
+CTAPI_EXPORT ctStatus_t ct_t3_d(const float* d_input, float* d_output, int size, int period, float vFactor, cudaStream_t stream); /* tacuda_device.h:158 */
+CTAPI_EXPORT ctStatus_t ct_rsi_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:165 */
+CTAPI_EXPORT ctStatus_t ct_atr_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, int period, float percentile, cudaStream_t stream); /* tacuda_device.h:193 */
+CTAPI_EXPORT ctStatus_t ct_natr_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:203 */
+CTAPI_EXPORT ctStatus_t ct_trange_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:207 */
+CTAPI_EXPORT ctStatus_t ct_adx_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:215 */
+CTAPI_EXPORT ctStatus_t ct_dx_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:223 */
+CTAPI_EXPORT ctStatus_t ct_macd_d(const float* d_input, float* d_macd, float* d_signal, float* d_hist, int size, int fastPeriod, int slowPeriod, int signalPeriod, int maType, cudaStream_t stream); /* tacuda_device.h:239 */
+CTAPI_EXPORT ctStatus_t ct_stochastic_d(const float* d_high, const float* d_low, const float* d_close, float* d_slowK, float* d_slowD, int size, int kPeriod, int dPeriod, cudaStream_t stream); /* tacuda_device.h:251 */
+CTAPI_EXPORT ctStatus_t ct_willr_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:262 */
+CTAPI_EXPORT ctStatus_t ct_cci_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:266 */
+CTAPI_EXPORT ctStatus_t ct_bbands_d(const float* d_input, float* d_upper, float* d_middle, float* d_lower, int size, int period, float nbDevUp, float nbDevDn, cudaStream_t stream); /* tacuda_device.h:279 */
+CTAPI_EXPORT ctStatus_t ct_ad_d(const float* d_high, const float* d_low, const float* d_close, const float* d_volume, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:298 */
+CTAPI_EXPORT ctStatus_t ct_adosc_d(const float* d_high, const float* d_low, const float* d_close, const float* d_volume, float* d_output, int size, int fastPeriod, int slowPeriod, cudaStream_t stream); /* tacuda_device.h:302 */
+CTAPI_EXPORT ctStatus_t ct_obv_d(const float* d_close, const float* d_volume, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:307 */
+CTAPI_EXPORT ctStatus_t ct_mfi_d(const float* d_high, const float* d_low, const float* d_close, const float* d_volume, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:310 */
+CTAPI_EXPORT ctStatus_t ct_stddev_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:319 */
+CTAPI_EXPORT ctStatus_t ct_var_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:322 */
+CTAPI_EXPORT ctStatus_t ct_sum_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:325 */
+CTAPI_EXPORT ctStatus_t ct_max_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:328 */
+CTAPI_EXPORT ctStatus_t ct_min_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:331 */
+CTAPI_EXPORT ctStatus_t ct_linearreg_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:357 */
+CTAPI_EXPORT ctStatus_t ct_correl_d(const float* d_x, const float* d_y, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:540 */
+CTAPI_EXPORT ctStatus_t ct_cdl_doji_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:555 */
+CTAPI_EXPORT ctStatus_t ct_cdl_hammer_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:559 */
+CTAPI_EXPORT ctStatus_t ct_cdl_inverted_hammer_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:565 */
+CTAPI_EXPORT ctStatus_t ct_cdl_bullish_engulfing_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:571 */
+CTAPI_EXPORT ctStatus_t ct_cdl_bearish_engulfing_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:577 */
+CTAPI_EXPORT ctStatus_t ct_cdl_three_white_soldiers_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:583 */
+CTAPI_EXPORT ctStatus_t ct_cdl_abandoned_baby_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:590 */
+CTAPI_EXPORT ctStatus_t ct_cdl_advance_block_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:596 */
+CTAPI_EXPORT ctStatus_t ct_cdl_belt_hold_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:602 */
+CTAPI_EXPORT ctStatus_t ct_cdl_breakaway_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:608 */
+CTAPI_EXPORT ctStatus_t ct_cdl_two_crows_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:614 */
+CTAPI_EXPORT ctStatus_t ct_cdl_three_black_crows_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:620 */
+CTAPI_EXPORT ctStatus_t ct_cdl_three_inside_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:626 */
+CTAPI_EXPORT ctStatus_t ct_cdl_three_outside_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:632 */
+CTAPI_EXPORT ctStatus_t ct_cdl_three_line_strike_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:638 */
+CTAPI_EXPORT ctStatus_t ct_cdl_three_stars_in_south_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:644 */
+CTAPI_EXPORT ctStatus_t ct_cdl_closing_marubozu_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:651 */
+CTAPI_EXPORT ctStatus_t ct_cdl_conceal_baby_swallow_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:657 */
+CTAPI_EXPORT ctStatus_t ct_cdl_counterattack_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:664 */
+CTAPI_EXPORT ctStatus_t ct_cdl_dark_cloud_cover_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:670 */
+CTAPI_EXPORT ctStatus_t ct_cdl_doji_star_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:676 */
+CTAPI_EXPORT ctStatus_t ct_cdl_dragonfly_doji_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:682 */
+CTAPI_EXPORT ctStatus_t ct_cdl_engulfing_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:688 */
+CTAPI_EXPORT ctStatus_t ct_cdl_evening_doji_star_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:694 */
+CTAPI_EXPORT ctStatus_t ct_cdl_evening_star_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:700 */
+CTAPI_EXPORT ctStatus_t ct_cdl_gap_side_side_white_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:706 */
+CTAPI_EXPORT ctStatus_t ct_cdl_gravestone_doji_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:712 */
+CTAPI_EXPORT ctStatus_t ct_cdl_hanging_man_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:718 */
+CTAPI_EXPORT ctStatus_t ct_cdl_harami_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:724 */
+CTAPI_EXPORT ctStatus_t ct_cdl_harami_cross_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:730 */
+CTAPI_EXPORT ctStatus_t ct_cdl_high_wave_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:736 */
+CTAPI_EXPORT ctStatus_t ct_cdl_hikkake_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:742 */
+CTAPI_EXPORT ctStatus_t ct_cdl_hikkake_mod_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:748 */
+CTAPI_EXPORT ctStatus_t ct_cdl_homing_pigeon_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:754 */
+CTAPI_EXPORT ctStatus_t ct_cdl_identical_three_crows_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:760 */
+CTAPI_EXPORT ctStatus_t ct_cdl_in_neck_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:767 */
+CTAPI_EXPORT ctStatus_t ct_cdl_kicking_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:773 */
+CTAPI_EXPORT ctStatus_t ct_cdl_kicking_by_length_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:779 */
+CTAPI_EXPORT ctStatus_t ct_cdl_ladder_bottom_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:785 */
+CTAPI_EXPORT ctStatus_t ct_cdl_long_legged_doji_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:791 */
+CTAPI_EXPORT ctStatus_t ct_cdl_long_line_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:797 */
+CTAPI_EXPORT ctStatus_t ct_cdl_marubozu_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:803 */
+CTAPI_EXPORT ctStatus_t ct_cdl_matching_low_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:809 */
+CTAPI_EXPORT ctStatus_t ct_cdl_mat_hold_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:815 */
+CTAPI_EXPORT ctStatus_t ct_cdl_morning_doji_star_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:821 */
+CTAPI_EXPORT ctStatus_t ct_cdl_morning_star_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:827 */
+CTAPI_EXPORT ctStatus_t ct_cdl_on_neck_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:833 */
+CTAPI_EXPORT ctStatus_t ct_cdl_piercing_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:839 */
+CTAPI_EXPORT ctStatus_t ct_cdl_rickshaw_man_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:845 */
+CTAPI_EXPORT ctStatus_t ct_cdl_rise_fall3_methods_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:851 */
+CTAPI_EXPORT ctStatus_t ct_cdl_separating_lines_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:857 */
+CTAPI_EXPORT ctStatus_t ct_cdl_shooting_star_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:863 */
+CTAPI_EXPORT ctStatus_t ct_cdl_short_line_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:869 */
+CTAPI_EXPORT ctStatus_t ct_cdl_spinning_top_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:875 */
+CTAPI_EXPORT ctStatus_t ct_cdl_stalled_pattern_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:881 */
+CTAPI_EXPORT ctStatus_t ct_cdl_stick_sandwich_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:887 */
+CTAPI_EXPORT ctStatus_t ct_cdl_takuri_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:893 */
+CTAPI_EXPORT ctStatus_t ct_cdl_tasuki_gap_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:899 */
+CTAPI_EXPORT ctStatus_t ct_cdl_thrusting_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:905 */
+CTAPI_EXPORT ctStatus_t ct_cdl_tristar_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:911 */
+CTAPI_EXPORT ctStatus_t ct_cdl_unique_3_river_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:917 */
+CTAPI_EXPORT ctStatus_t ct_cdl_upside_gap_2_crows_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:923 */
+CTAPI_EXPORT ctStatus_t ct_cdl_xside_gap_3_methods_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:929 */
+
+/* ---- host batch API (include/tacuda.h:848-890): host matrices, staged
+ * through device memory on the given stream (stream 0: synchronous) ---- */
+CTAPI_EXPORT ctStatus_t ct_sma_batch(const float *host_inputs, float *host_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:848 */
+CTAPI_EXPORT ctStatus_t ct_ema_batch(const float *host_inputs, float *host_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:853 */
+CTAPI_EXPORT ctStatus_t ct_rsi_batch(const float *host_inputs, float *host_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:858 */
+CTAPI_EXPORT ctStatus_t ct_atr_batch(const float *host_highs, const float *host_lows, const float *host_closes, float *host_outputs, int seriesLen, int numSeries, int period, float initial, int maxConcurrency, cudaStream_t stream); /* tacuda.h:863 */
+CTAPI_EXPORT ctStatus_t ct_macd_batch(const float *host_inputs, float *host_macds, float *host_signals, float *host_hists, int seriesLen, int numSeries, int fastPeriod, int slowPeriod, int signalPeriod, int maType, int maxConcurrency, cudaStream_t stream); /* tacuda.h:870 */
+CTAPI_EXPORT ctStatus_t ct_bbands_batch(const float *host_inputs, float *host_uppers, float *host_middles, float *host_lowers, int seriesLen, int numSeries, int period, float upperMul, float lowerMul, int maxConcurrency, cudaStream_t stream); /* tacuda.h:877 */
+CTAPI_EXPORT ctStatus_t ct_stochastic_batch(const float *host_highs, const float *host_lows, const float *host_closes, float *host_ks, float *host_ds, int seriesLen, int numSeries, int kPeriod, int dPeriod, int maxConcurrency, cudaStream_t stream); /* tacuda.h:885 */
+
+/* ========================================================================
+ * ct_b200_*: new surface with no counterpart in the reference.
+ * ======================================================================== */
+
+/* Families of a fused job (same arithmetic as the matching ct_*_batch_d). */
+typedef enum ctB200Family {
+  CT_B200_SMA = 0, CT_B200_EMA, CT_B200_WMA, CT_B200_RSI, CT_B200_MACD, CT_B200_ATR,
+  CT_B200_NATR, CT_B200_TRANGE, CT_B200_ADX, CT_B200_DX, CT_B200_BBANDS, CT_B200_STOCH,
+  CT_B200_CCI, CT_B200_OBV, CT_B200_AD, CT_B200_ADOSC, CT_B200_MFI, CT_B200_WILLR,
+  CT_B200_SUM, CT_B200_MIN, CT_B200_MAX, CT_B200_STDDEV, CT_B200_VAR, CT_B200_LINEARREG,
+  CT_B200_CORREL, CT_B200_DEMA, CT_B200_TEMA, CT_B200_T3, CT_B200_CDL
+} ctB200Family_t;
+
+/* Input planes of a batch. */
+typedef enum ctB200Plane {
+  CT_B200_OPEN = 0, CT_B200_HIGH, CT_B200_LOW, CT_B200_CLOSE, CT_B200_VOLUME, CT_B200_AUX
+} ctB200Plane_t;
+
+/* The batch's input planes (device pointers; unused planes may be NULL).
+ * Uniform rows: offsets == NULL, numSeries rows of seriesLen bars. Ragged rows
+ * (plans only): row s spans [offsets[s], offsets[s+1]) of every plane. */
+typedef struct ctB200Series {
+  const float* planes[6];
+  const int64_t* offsets;
+  int64_t seriesLen;
+  int numSeries;
+} ctB200Series;
+
+/* One indicator of a fused launch. params/fparams follow the argument order of
+ * the family's ct_*_batch_d (e.g. MACD: fast, slow, signal; BBANDS: period and
+ * fparams up, down; STOCH: kPeriod, dPeriod; T3: period, fparams vFactor;
+ * STDDEV: period, fparams nbDev). inputs[] maps the family's inputs to planes;
+ * a negative first entry selects the defaults (close; high, low, close;
+ * high, low, close, volume; close, volume for OBV; close, aux for CORREL).
+ * outputs[] are float32 matrices laid out like the planes. CDL: cdl_mask bit k
+ * selects pattern k (order of the ct_cdl_*_batch_d declarations above), written
+ * to outputs[0] + k * cdl_stride elements, as int32 when cdl_int32 != 0. */
+typedef struct ctB200Job {
+  int family;
+  int params[3];
+  double fparams[2];
+  int inputs[4];
+  void* outputs[3];
+  uint64_t cdl_mask;
+  int64_t cdl_stride;
+  int cdl_int32;
+} ctB200Job;
+
+/* Evaluate all jobs over a uniform batch in one kernel launch. */
+CTAPI_EXPORT ctStatus_t ct_b200_fused_batch_d(const ctB200Series* series, const ctB200Job* jobs,
+                                              int numJobs, cudaStream_t stream);
+
+/* Host-memory variant: planes and outputs are host pointers; the call copies
+ * inputs in, launches once and copies outputs back on `stream` (stream 0:
+ * returns when done). */
+CTAPI_EXPORT ctStatus_t ct_b200_fused_batch(const ctB200Series* hostSeries, const ctB200Job* hostJobs,
+                                            int numJobs, cudaStream_t stream);
+
+/* Plans: a reusable schedule for a (possibly ragged) batch and job set. Creating
+ * a plan may allocate and copy (series order, tuned launch shape); executing
+ * one only launches, so executions can be captured in CUDA graphs. The job
+ * families and parameters at execution must match those at creation; output
+ * and input pointers may change. hostOffsets: numSeries+1 row starts on the
+ * host (NULL for uniform rows of seriesLen). */
+typedef struct ctB200Plan ctB200Plan;
+CTAPI_EXPORT ctStatus_t ct_b200_plan_create(const ctB200Job* jobs, int numJobs, const int64_t* hostOffsets,
+                                            int numSeries, int64_t seriesLen, ctB200Plan** plan);
+CTAPI_EXPORT ctStatus_t ct_b200_plan_execute(const ctB200Plan* plan, const ctB200Series* series,
+                                             const ctB200Job* jobs, int numJobs, cudaStream_t stream);
+CTAPI_EXPORT ctStatus_t ct_b200_plan_destroy(ctB200Plan* plan);
+/* Time the candidate launch shapes of a plan on the given data and keep the
+ * fastest (also stored in the autotuner cache). Synchronises `stream`. */
+CTAPI_EXPORT ctStatus_t ct_b200_plan_autotune(ctB200Plan* plan, const ctB200Series* series,
+                                              const ctB200Job* jobs, int numJobs, cudaStream_t stream);
+/* Launch shape chosen by a plan: bars per lane, warps per block, blocks. */
+CTAPI_EXPORT ctStatus_t ct_b200_plan_describe(const ctB200Plan* plan, int* barsPerLane, int* warpsPerBlock,
+                                              int* blocks);
+
+/* All selected candle patterns of a uniform batch in one pass, int32 signals
+ * (pattern k of mask at d_out + k * seriesLen * numSeries). */
+CTAPI_EXPORT ctStatus_t ct_b200_cdl_batch_d(const float* d_opens, const float* d_highs, const float* d_lows,
+                                            const float* d_closes, int32_t* d_out, int seriesLen, int numSeries,
+                                            uint64_t patternMask, cudaStream_t stream);
+CTAPI_EXPORT int ct_b200_cdl_count(void);
+CTAPI_EXPORT const char* ct_b200_cdl_name(int pattern);
+CTAPI_EXPORT int ct_b200_cdl_lookback(int pattern);
+
+/* Number of kernel launches this library issued from the calling process
+ * (diagnostics; the batch entry points issue one each). */
+CTAPI_EXPORT unsigned long long ct_b200_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TACUDA_B200_H */

@@ -1,0 +1,928 @@
+// extern "C" boundary of the library: the reference's batch / single-series
+// entry points (same names, arguments, status codes and stream semantics as
+// include/tacuda.h and include/tacuda_device.h of TACUDA 0.9.3) plus the
+// append-only ct_b200_* surface. Every batch call is one launch of the fused
+// engine (engine.cu) with one or more jobs.
+#include <tacuda.h>
+
+#include "engine.h"
+#include "families.cuh"
+#include "scheduler.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <string>
+#include <vector>
+
+namespace {
+
+using tb::Job;
+using tb::Launch;
+
+thread_local std::string t_last_error;
+std::atomic<unsigned long long> g_launches{0};
+
+void clear_error() { t_last_error.clear(); }
+
+ctStatus_t fail(ctStatus_t st, const std::string& msg) {
+  t_last_error = msg;
+  return st;
+}
+
+ctStatus_t cuda_fail(ctStatus_t st, const char* where, cudaError_t e) {
+  return fail(st, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+// Minimum valid period of each family's first integer parameter.
+int min_period(int family) {
+  switch (family) {
+    case tb::F_OBV: case tb::F_AD: case tb::F_TRANGE: case tb::F_CDL: return 0;
+    default: return 1;
+  }
+}
+
+int default_inputs(int family, int* in) {
+  switch (family) {
+    case tb::F_ATR: case tb::F_NATR: case tb::F_TRANGE: case tb::F_ADX: case tb::F_DX:
+    case tb::F_STOCH: case tb::F_WILLR: case tb::F_CCI:
+      in[0] = tb::P_HIGH; in[1] = tb::P_LOW; in[2] = tb::P_CLOSE; return 3;
+    case tb::F_AD: case tb::F_ADOSC: case tb::F_MFI:
+      in[0] = tb::P_HIGH; in[1] = tb::P_LOW; in[2] = tb::P_CLOSE; in[3] = tb::P_VOLUME; return 4;
+    case tb::F_OBV: in[0] = tb::P_CLOSE; in[1] = tb::P_VOLUME; return 2;
+    case tb::F_CORREL: in[0] = tb::P_CLOSE; in[1] = tb::P_AUX; return 2;
+    case tb::F_CDL:
+      in[0] = tb::P_OPEN; in[1] = tb::P_HIGH; in[2] = tb::P_LOW; in[3] = tb::P_CLOSE; return 4;
+    default: in[0] = tb::P_CLOSE; return 1;
+  }
+}
+
+int output_count(int family) {
+  switch (family) {
+    case tb::F_MACD: case tb::F_BBANDS: return 3;
+    case tb::F_STOCH: return 2;
+    default: return 1;
+  }
+}
+
+constexpr int kMaxWindow = 4096;  // largest window period staged in shared memory
+
+// Build an engine job from reference-style parameters; precomputes TA-Lib's
+// coefficients on the host so the device uses the identical doubles.
+ctStatus_t make_job(const ctB200Job& u, Job& j, const char* who) {
+  std::memset(&j, 0, sizeof(j));
+  j.family = u.family;
+  if (u.family < 0 || u.family >= tb::F_COUNT) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": unknown family");
+  for (int i = 0; i < 3; ++i) j.ip[i] = u.params[i];
+  const int f = u.family;
+  const int mp = min_period(f);
+  if (mp > 0 && u.params[0] < mp) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": invalid period");
+  if ((f == tb::F_MACD && (u.params[1] < 1 || u.params[2] < 1)) ||
+      (f == tb::F_STOCH && u.params[1] < 1) || (f == tb::F_ADOSC && u.params[1] < 1))
+    return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": invalid period");
+  switch (f) {
+    case tb::F_SMA: case tb::F_SUM: case tb::F_WMA: case tb::F_BBANDS: case tb::F_STDDEV: case tb::F_VAR:
+    case tb::F_LINEARREG: case tb::F_MIN: case tb::F_MAX: case tb::F_WILLR: case tb::F_CCI: case tb::F_MFI:
+    case tb::F_CORREL:
+      if (u.params[0] > kMaxWindow) return fail(CT_STATUS_UNSUPPORTED, std::string(who) + ": window period above 4096");
+      break;
+    case tb::F_STOCH:
+      if (u.params[0] > kMaxWindow || u.params[1] > 32)
+        return fail(CT_STATUS_UNSUPPORTED, std::string(who) + ": STOCH kPeriod above 4096 or dPeriod above 32");
+      break;
+    default: break;
+  }
+  double b, k;
+  switch (f) {
+    case tb::F_EMA: case tb::F_DEMA: case tb::F_TEMA:
+      tb::talib_ema_coeffs(u.params[0], b, k);
+      j.fp[0] = b; j.fp[1] = k;
+      break;
+    case tb::F_T3:
+      k = 2.0 / (u.params[0] + 1.0);
+      j.fp[0] = 1.0 - k; j.fp[1] = k; j.fp[2] = u.fparams[0];
+      break;
+    case tb::F_MACD: {
+      int fast = u.params[0], slow = u.params[1];
+      if (slow < fast) std::swap(fast, slow);  // TA-Lib swaps reversed periods
+      j.ip[0] = fast; j.ip[1] = slow; j.ip[2] = u.params[2];
+      tb::talib_ema_coeffs(fast, j.fp[0], j.fp[1]);
+      tb::talib_ema_coeffs(slow, j.fp[2], j.fp[3]);
+      break;
+    }
+    case tb::F_ATR: case tb::F_NATR:
+      j.fp[0] = (double)(u.params[0] - 1) / (double)u.params[0];
+      j.fp[1] = 1.0 - j.fp[0];
+      break;
+    case tb::F_BBANDS: j.fp[0] = u.fparams[0]; j.fp[1] = u.fparams[1]; break;
+    case tb::F_STDDEV: j.fp[0] = u.fparams[0] == 0.0 ? 1.0 : u.fparams[0]; break;
+    default: break;
+  }
+  int def[4] = {0, 0, 0, 0};
+  const int nin = default_inputs(f, def);
+  for (int i = 0; i < 4; ++i) j.in[i] = def[i];
+  if (u.inputs[0] >= 0) {
+    for (int i = 0; i < nin; ++i) {
+      if (u.inputs[i] < 0 || u.inputs[i] >= tb::P_COUNT) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": bad input plane");
+      j.in[i] = u.inputs[i];
+    }
+    if ((f == tb::F_CCI || f == tb::F_MFI) &&
+        (j.in[0] != tb::P_HIGH || j.in[1] != tb::P_LOW || j.in[2] != tb::P_CLOSE))
+      return fail(CT_STATUS_UNSUPPORTED, std::string(who) + ": CCI/MFI read the high/low/close planes");
+  }
+  const int nout = f == tb::F_CDL ? 1 : output_count(f);
+  for (int i = 0; i < nout; ++i) {
+    if (!u.outputs[i]) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": null output");
+    j.out[i] = u.outputs[i];
+  }
+  if (f == tb::F_CDL) {
+    j.cdl_mask = u.cdl_mask;
+    j.cdl_stride = u.cdl_stride;
+    j.cdl_int32 = u.cdl_int32;
+    if (u.cdl_mask == 0 || (u.cdl_mask >> tb::kCdlPatterns) != 0)
+      return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": bad candle mask");
+  }
+  return CT_STATUS_SUCCESS;
+}
+
+ctStatus_t check_planes(const Launch& L, const char* who) {
+  for (int j = 0; j < L.njobs; ++j) {
+    const Job& jb = L.jobs[j];
+    int def[4];
+    const int nin = default_inputs(jb.family, def);
+    for (int i = 0; i < nin; ++i)
+      if (!L.plane[jb.in[i]]) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": null input");
+    if ((jb.family == tb::F_CCI || jb.family == tb::F_MFI) &&
+        (!L.plane[tb::P_HIGH] || !L.plane[tb::P_LOW] || !L.plane[tb::P_CLOSE]))
+      return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": null input");
+  }
+  return CT_STATUS_SUCCESS;
+}
+
+ctStatus_t finish(cudaStream_t stream, const char* who) {
+  if (stream == 0) {
+    const cudaError_t e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) return cuda_fail(CT_STATUS_DEVICE_ERROR, who, e);
+  }
+  return CT_STATUS_SUCCESS;
+}
+
+ctStatus_t launch(Launch& L, long long total, long long maxlen, const tb::SchedulePlan* forced, cudaStream_t stream,
+                  const char* who, tb::LaunchStats* stats = nullptr) {
+  const tb::SchedulePlan plan = forced ? *forced : tb::plan_for(L, total, maxlen);
+  const cudaError_t e = tb::launch_batch(L, plan, stream, stats);
+  if (e != cudaSuccess) return cuda_fail(CT_STATUS_KERNEL_FAILED, who, e);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return CT_STATUS_SUCCESS;
+}
+
+// One-job uniform batch helper used by every reference entry point.
+ctStatus_t run_single(const float* const planes[tb::P_COUNT], const ctB200Job& u, int seriesLen, int numSeries,
+                      cudaStream_t stream, const char* who) {
+  clear_error();
+  if (seriesLen <= 0 || numSeries <= 0) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": null pointer or invalid size");
+  Launch L;
+  std::memset(&L, 0, sizeof(L));
+  for (int p = 0; p < tb::P_COUNT; ++p) L.plane[p] = planes[p];
+  L.T = seriesLen;
+  L.S = numSeries;
+  L.njobs = 1;
+  ctStatus_t st = make_job(u, L.jobs[0], who);
+  if (st != CT_STATUS_SUCCESS) {
+    if (st == CT_STATUS_INVALID_ARGUMENT && t_last_error.find("null output") != std::string::npos)
+      t_last_error = std::string(who) + ": null pointer or invalid size";
+    return st;
+  }
+  st = check_planes(L, who);
+  if (st != CT_STATUS_SUCCESS) return fail(st, std::string(who) + ": null pointer or invalid size");
+  st = launch(L, (long long)seriesLen * numSeries, seriesLen, nullptr, stream, who);
+  if (st != CT_STATUS_SUCCESS) return st;
+  return finish(stream, who);
+}
+
+ctB200Job job_of(int family, int p0 = 0, int p1 = 0, int p2 = 0, double f0 = 0.0, double f1 = 0.0) {
+  ctB200Job u;
+  std::memset(&u, 0, sizeof(u));
+  u.family = family;
+  u.params[0] = p0; u.params[1] = p1; u.params[2] = p2;
+  u.fparams[0] = f0; u.fparams[1] = f1;
+  u.inputs[0] = -1;
+  return u;
+}
+
+struct Planes {
+  const float* p[tb::P_COUNT] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+};
+
+Planes close_only(const float* c) { Planes P; P.p[tb::P_CLOSE] = c; return P; }
+Planes hlc(const float* h, const float* l, const float* c) {
+  Planes P; P.p[tb::P_HIGH] = h; P.p[tb::P_LOW] = l; P.p[tb::P_CLOSE] = c; return P;
+}
+Planes hlcv(const float* h, const float* l, const float* c, const float* v) {
+  Planes P = hlc(h, l, c); P.p[tb::P_VOLUME] = v; return P;
+}
+Planes ohlc(const float* o, const float* h, const float* l, const float* c) {
+  Planes P = hlc(h, l, c); P.p[tb::P_OPEN] = o; return P;
+}
+
+const char* const kCdlNames[tb::kCdlPatterns] = {
+#define TB_CDL(name, lb) #name,
+#include "candle_list.inc"
+#undef TB_CDL
+};
+const int kCdlLookback[tb::kCdlPatterns] = {
+#define TB_CDL(name, lb) lb,
+#include "candle_list.inc"
+#undef TB_CDL
+};
+
+ctStatus_t run_cdl(const float* o, const float* h, const float* l, const float* c, void* out, int seriesLen,
+                   int numSeries, uint64_t mask, int as_int, cudaStream_t stream, const char* who) {
+  ctB200Job u = job_of(tb::F_CDL);
+  u.outputs[0] = out;
+  u.cdl_mask = mask;
+  u.cdl_stride = as_int ? (int64_t)seriesLen * numSeries : 0;
+  u.cdl_int32 = as_int;
+  if (!o || !h || !l || !c || !out) {
+    clear_error();
+    return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": null pointer or invalid size");
+  }
+  const Planes P = ohlc(o, h, l, c);
+  return run_single(P.p, u, seriesLen, numSeries, stream, who);
+}
+
+int cdl_index(const char* name) {
+  for (int k = 0; k < tb::kCdlPatterns; ++k)
+    if (std::strcmp(kCdlNames[k], name) == 0) return k;
+  return -1;
+}
+
+}  // namespace
+
+struct ctB200Plan {
+  std::vector<Job> jobs;
+  int njobs = 0;
+  int numSeries = 0;
+  long long seriesLen = 0;
+  bool ragged = false;
+  long long total = 0, maxlen = 0;
+  int* d_order = nullptr;
+  tb::SchedulePlan sched;
+  tb::LaunchStats stats;
+  int device = 0;
+};
+
+extern "C" {
+
+const char* ct_status_string(ctStatus_t s) {
+  switch (s) {
+    case CT_STATUS_SUCCESS: return "success";
+    case CT_STATUS_ALLOC_FAILED: return "allocation failed";
+    case CT_STATUS_COPY_FAILED: return "copy failed";
+    case CT_STATUS_KERNEL_FAILED: return "kernel failed";
+    case CT_STATUS_INVALID_ARGUMENT: return "invalid argument";
+    case CT_STATUS_DEVICE_ERROR: return "device error";
+    case CT_STATUS_UNSUPPORTED: return "unsupported";
+  }
+  return "unknown status";
+}
+
+const char* ct_get_last_error(void) { return t_last_error.c_str(); }
+const char* ct_version(void) { return "0.9.3-b200"; }
+unsigned long long ct_b200_launch_count(void) { return g_launches.load(); }
+
+// ------------------------------------------------------------ batch API
+
+#define TB_S1(NAME, FAM)                                                                              \
+  ctStatus_t ct_##NAME##_batch_d(const float* d_inputs, float* d_outputs, int seriesLen, int numSeries, \
+                                 int period, int, cudaStream_t stream) {                              \
+    ctB200Job u = job_of(FAM, period);                                                                \
+    u.outputs[0] = d_outputs;                                                                         \
+    const Planes P = close_only(d_inputs);                                                            \
+    return run_single(P.p, u, seriesLen, numSeries, stream, "ct_" #NAME "_batch_d");                  \
+  }                                                                                                   \
+  ctStatus_t ct_##NAME##_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream) { \
+    ctB200Job u = job_of(FAM, period);                                                                \
+    u.outputs[0] = d_output;                                                                          \
+    const Planes P = close_only(d_input);                                                             \
+    return run_single(P.p, u, size, 1, stream, "ct_" #NAME "_d");                                     \
+  }
+
+TB_S1(sma, tb::F_SMA)
+TB_S1(ema, tb::F_EMA)
+TB_S1(wma, tb::F_WMA)
+TB_S1(rsi, tb::F_RSI)
+TB_S1(dema, tb::F_DEMA)
+TB_S1(tema, tb::F_TEMA)
+TB_S1(stddev, tb::F_STDDEV)
+TB_S1(var, tb::F_VAR)
+TB_S1(sum, tb::F_SUM)
+TB_S1(max, tb::F_MAX)
+TB_S1(min, tb::F_MIN)
+TB_S1(linearreg, tb::F_LINEARREG)
+#undef TB_S1
+
+#define TB_HLC(NAME, FAM)                                                                                  \
+  ctStatus_t ct_##NAME##_batch_d(const float* d_highs, const float* d_lows, const float* d_closes,         \
+                                 float* d_outputs, int seriesLen, int numSeries, int period, int,          \
+                                 cudaStream_t stream) {                                                    \
+    ctB200Job u = job_of(FAM, period);                                                                     \
+    u.outputs[0] = d_outputs;                                                                              \
+    const Planes P = hlc(d_highs, d_lows, d_closes);                                                       \
+    return run_single(P.p, u, seriesLen, numSeries, stream, "ct_" #NAME "_batch_d");                       \
+  }                                                                                                        \
+  ctStatus_t ct_##NAME##_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, \
+                           int size, int period, cudaStream_t stream) {                                    \
+    ctB200Job u = job_of(FAM, period);                                                                     \
+    u.outputs[0] = d_output;                                                                               \
+    const Planes P = hlc(d_high, d_low, d_close);                                                          \
+    return run_single(P.p, u, size, 1, stream, "ct_" #NAME "_d");                                          \
+  }
+
+TB_HLC(natr, tb::F_NATR)
+TB_HLC(adx, tb::F_ADX)
+TB_HLC(dx, tb::F_DX)
+TB_HLC(willr, tb::F_WILLR)
+TB_HLC(cci, tb::F_CCI)
+#undef TB_HLC
+
+ctStatus_t ct_atr_batch_d(const float* d_highs, const float* d_lows, const float* d_closes, float* d_outputs,
+                          int seriesLen, int numSeries, int period, float, int, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_ATR, period);
+  u.outputs[0] = d_outputs;
+  const Planes P = hlc(d_highs, d_lows, d_closes);
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_atr_batch_d");
+}
+ctStatus_t ct_atr_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, int size,
+                    int period, float, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_ATR, period);
+  u.outputs[0] = d_output;
+  const Planes P = hlc(d_high, d_low, d_close);
+  return run_single(P.p, u, size, 1, stream, "ct_atr_d");
+}
+
+ctStatus_t ct_trange_batch_d(const float* d_highs, const float* d_lows, const float* d_closes, float* d_outputs,
+                             int seriesLen, int numSeries, int, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_TRANGE);
+  u.outputs[0] = d_outputs;
+  const Planes P = hlc(d_highs, d_lows, d_closes);
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_trange_batch_d");
+}
+ctStatus_t ct_trange_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, int size,
+                       cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_TRANGE);
+  u.outputs[0] = d_output;
+  const Planes P = hlc(d_high, d_low, d_close);
+  return run_single(P.p, u, size, 1, stream, "ct_trange_d");
+}
+
+static ctStatus_t macd_common(const float* in, float* m, float* s, float* h, int len, int n, int fast, int slow,
+                              int signal, int maType, cudaStream_t stream, const char* who) {
+  if (maType != 1) {
+    clear_error();
+    return fail(CT_STATUS_UNSUPPORTED, std::string(who) + ": only maType = CT_MA_EMA is implemented");
+  }
+  ctB200Job u = job_of(tb::F_MACD, fast, slow, signal);
+  u.outputs[0] = m; u.outputs[1] = s; u.outputs[2] = h;
+  const Planes P = close_only(in);
+  return run_single(P.p, u, len, n, stream, who);
+}
+ctStatus_t ct_macd_batch_d(const float* d_inputs, float* d_macds, float* d_signals, float* d_hists, int seriesLen,
+                           int numSeries, int fastPeriod, int slowPeriod, int signalPeriod, int maType, int,
+                           cudaStream_t stream) {
+  return macd_common(d_inputs, d_macds, d_signals, d_hists, seriesLen, numSeries, fastPeriod, slowPeriod,
+                     signalPeriod, maType, stream, "ct_macd_batch_d");
+}
+ctStatus_t ct_macd_d(const float* d_input, float* d_macd, float* d_signal, float* d_hist, int size, int fastPeriod,
+                     int slowPeriod, int signalPeriod, int maType, cudaStream_t stream) {
+  return macd_common(d_input, d_macd, d_signal, d_hist, size, 1, fastPeriod, slowPeriod, signalPeriod, maType,
+                     stream, "ct_macd_d");
+}
+
+ctStatus_t ct_bbands_batch_d(const float* d_inputs, float* d_uppers, float* d_middles, float* d_lowers,
+                             int seriesLen, int numSeries, int period, float upperMul, float lowerMul, int,
+                             cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_BBANDS, period, 0, 0, upperMul, lowerMul);
+  u.outputs[0] = d_uppers; u.outputs[1] = d_middles; u.outputs[2] = d_lowers;
+  const Planes P = close_only(d_inputs);
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_bbands_batch_d");
+}
+ctStatus_t ct_bbands_d(const float* d_input, float* d_upper, float* d_middle, float* d_lower, int size, int period,
+                       float nbDevUp, float nbDevDn, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_BBANDS, period, 0, 0, nbDevUp, nbDevDn);
+  u.outputs[0] = d_upper; u.outputs[1] = d_middle; u.outputs[2] = d_lower;
+  const Planes P = close_only(d_input);
+  return run_single(P.p, u, size, 1, stream, "ct_bbands_d");
+}
+
+ctStatus_t ct_stochastic_batch_d(const float* d_highs, const float* d_lows, const float* d_closes, float* d_ks,
+                                 float* d_ds, int seriesLen, int numSeries, int kPeriod, int dPeriod, int,
+                                 cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_STOCH, kPeriod, dPeriod);
+  u.outputs[0] = d_ks; u.outputs[1] = d_ds;
+  const Planes P = hlc(d_highs, d_lows, d_closes);
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_stochastic_batch_d");
+}
+ctStatus_t ct_stochastic_d(const float* d_high, const float* d_low, const float* d_close, float* d_slowK,
+                           float* d_slowD, int size, int kPeriod, int dPeriod, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_STOCH, kPeriod, dPeriod);
+  u.outputs[0] = d_slowK; u.outputs[1] = d_slowD;
+  const Planes P = hlc(d_high, d_low, d_close);
+  return run_single(P.p, u, size, 1, stream, "ct_stochastic_d");
+}
+
+ctStatus_t ct_t3_batch_d(const float* d_inputs, float* d_outputs, int seriesLen, int numSeries, int period,
+                         float vFactor, int, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_T3, period, 0, 0, vFactor);
+  u.outputs[0] = d_outputs;
+  const Planes P = close_only(d_inputs);
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_t3_batch_d");
+}
+ctStatus_t ct_t3_d(const float* d_input, float* d_output, int size, int period, float vFactor, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_T3, period, 0, 0, vFactor);
+  u.outputs[0] = d_output;
+  const Planes P = close_only(d_input);
+  return run_single(P.p, u, size, 1, stream, "ct_t3_d");
+}
+
+ctStatus_t ct_obv_batch_d(const float* d_closes, const float* d_volumes, float* d_outputs, int seriesLen,
+                          int numSeries, int, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_OBV);
+  u.outputs[0] = d_outputs;
+  Planes P = close_only(d_closes);
+  P.p[tb::P_VOLUME] = d_volumes;
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_obv_batch_d");
+}
+ctStatus_t ct_obv_d(const float* d_close, const float* d_volume, float* d_output, int size, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_OBV);
+  u.outputs[0] = d_output;
+  Planes P = close_only(d_close);
+  P.p[tb::P_VOLUME] = d_volume;
+  return run_single(P.p, u, size, 1, stream, "ct_obv_d");
+}
+
+ctStatus_t ct_mfi_batch_d(const float* d_highs, const float* d_lows, const float* d_closes, const float* d_volumes,
+                          float* d_outputs, int seriesLen, int numSeries, int period, int, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_MFI, period);
+  u.outputs[0] = d_outputs;
+  const Planes P = hlcv(d_highs, d_lows, d_closes, d_volumes);
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_mfi_batch_d");
+}
+ctStatus_t ct_mfi_d(const float* d_high, const float* d_low, const float* d_close, const float* d_volume,
+                    float* d_output, int size, int period, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_MFI, period);
+  u.outputs[0] = d_output;
+  const Planes P = hlcv(d_high, d_low, d_close, d_volume);
+  return run_single(P.p, u, size, 1, stream, "ct_mfi_d");
+}
+
+ctStatus_t ct_ad_batch_d(const float* d_highs, const float* d_lows, const float* d_closes, const float* d_volumes,
+                         float* d_outputs, int seriesLen, int numSeries, int, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_AD);
+  u.outputs[0] = d_outputs;
+  const Planes P = hlcv(d_highs, d_lows, d_closes, d_volumes);
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_ad_batch_d");
+}
+ctStatus_t ct_ad_d(const float* d_high, const float* d_low, const float* d_close, const float* d_volume,
+                   float* d_output, int size, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_AD);
+  u.outputs[0] = d_output;
+  const Planes P = hlcv(d_high, d_low, d_close, d_volume);
+  return run_single(P.p, u, size, 1, stream, "ct_ad_d");
+}
+
+ctStatus_t ct_adosc_batch_d(const float* d_highs, const float* d_lows, const float* d_closes,
+                            const float* d_volumes, float* d_outputs, int seriesLen, int numSeries, int fastPeriod,
+                            int slowPeriod, int, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_ADOSC, fastPeriod, slowPeriod);
+  u.outputs[0] = d_outputs;
+  const Planes P = hlcv(d_highs, d_lows, d_closes, d_volumes);
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_adosc_batch_d");
+}
+ctStatus_t ct_adosc_d(const float* d_high, const float* d_low, const float* d_close, const float* d_volume,
+                      float* d_output, int size, int fastPeriod, int slowPeriod, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_ADOSC, fastPeriod, slowPeriod);
+  u.outputs[0] = d_output;
+  const Planes P = hlcv(d_high, d_low, d_close, d_volume);
+  return run_single(P.p, u, size, 1, stream, "ct_adosc_d");
+}
+
+ctStatus_t ct_correl_batch_d(const float* d_xs, const float* d_ys, float* d_outputs, int seriesLen, int numSeries,
+                             int period, int, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_CORREL, period);
+  u.outputs[0] = d_outputs;
+  Planes P = close_only(d_xs);
+  P.p[tb::P_AUX] = d_ys;
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_correl_batch_d");
+}
+ctStatus_t ct_correl_d(const float* d_x, const float* d_y, float* d_output, int size, int period,
+                       cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_CORREL, period);
+  u.outputs[0] = d_output;
+  Planes P = close_only(d_x);
+  P.p[tb::P_AUX] = d_y;
+  return run_single(P.p, u, size, 1, stream, "ct_correl_d");
+}
+
+// ------------------------------------------------------------ candles
+
+#define TB_CDL(NAME, LB)                                                                                     \
+  ctStatus_t ct_cdl_##NAME##_batch_d(const float* d_opens, const float* d_highs, const float* d_lows,        \
+                                     const float* d_closes, float* d_outputs, int seriesLen, int numSeries,  \
+                                     int, cudaStream_t stream) {                                            \
+    return run_cdl(d_opens, d_highs, d_lows, d_closes, d_outputs, seriesLen, numSeries,                     \
+                   1ull << cdl_index(#NAME), 0, stream, "ct_cdl_" #NAME "_batch_d");                         \
+  }                                                                                                          \
+  ctStatus_t ct_cdl_##NAME##_d(const float* d_open, const float* d_high, const float* d_low,                 \
+                               const float* d_close, float* d_output, int size, cudaStream_t stream) {       \
+    return run_cdl(d_open, d_high, d_low, d_close, d_output, size, 1, 1ull << cdl_index(#NAME), 0, stream,  \
+                   "ct_cdl_" #NAME "_d");                                                                    \
+  }
+#include "candle_list.inc"
+#undef TB_CDL
+
+ctStatus_t ct_b200_cdl_batch_d(const float* d_opens, const float* d_highs, const float* d_lows,
+                               const float* d_closes, int32_t* d_out, int seriesLen, int numSeries,
+                               uint64_t patternMask, cudaStream_t stream) {
+  if (patternMask == 0 || (patternMask >> tb::kCdlPatterns) != 0) {
+    clear_error();
+    return fail(CT_STATUS_INVALID_ARGUMENT, "ct_b200_cdl_batch_d: bad pattern mask");
+  }
+  return run_cdl(d_opens, d_highs, d_lows, d_closes, d_out, seriesLen, numSeries, patternMask, 1, stream,
+                 "ct_b200_cdl_batch_d");
+}
+
+int ct_b200_cdl_count(void) { return tb::kCdlPatterns; }
+const char* ct_b200_cdl_name(int k) { return (k >= 0 && k < tb::kCdlPatterns) ? kCdlNames[k] : nullptr; }
+int ct_b200_cdl_lookback(int k) { return (k >= 0 && k < tb::kCdlPatterns) ? kCdlLookback[k] : -1; }
+
+// ------------------------------------------------------------ fused API
+
+static ctStatus_t build_launch(const ctB200Series* series, const ctB200Job* jobs, int numJobs, Launch& L,
+                               const char* who) {
+  if (!series || !jobs || numJobs <= 0 || numJobs > tb::kMaxJobs)
+    return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": null pointer or bad job count");
+  if (series->numSeries <= 0 || (!series->offsets && series->seriesLen <= 0))
+    return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": invalid size");
+  std::memset(&L, 0, sizeof(L));
+  for (int p = 0; p < tb::P_COUNT; ++p) L.plane[p] = series->planes[p];
+  L.offsets = reinterpret_cast<const long long*>(series->offsets);
+  L.T = series->seriesLen;
+  L.S = series->numSeries;
+  L.njobs = numJobs;
+  for (int j = 0; j < numJobs; ++j) {
+    const ctStatus_t st = make_job(jobs[j], L.jobs[j], who);
+    if (st != CT_STATUS_SUCCESS) return st;
+  }
+  return check_planes(L, who);
+}
+
+ctStatus_t ct_b200_fused_batch_d(const ctB200Series* series, const ctB200Job* jobs, int numJobs,
+                                 cudaStream_t stream) {
+  clear_error();
+  const char* who = "ct_b200_fused_batch_d";
+  Launch L;
+  ctStatus_t st = build_launch(series, jobs, numJobs, L, who);
+  if (st != CT_STATUS_SUCCESS) return st;
+  if (L.offsets) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": ragged rows need a plan");
+  st = launch(L, L.T * (long long)L.S, L.T, nullptr, stream, who);
+  if (st != CT_STATUS_SUCCESS) return st;
+  return finish(stream, who);
+}
+
+ctStatus_t ct_b200_fused_batch(const ctB200Series* hs, const ctB200Job* hjobs, int numJobs, cudaStream_t stream) {
+  clear_error();
+  const char* who = "ct_b200_fused_batch";
+  Launch L;
+  ctStatus_t st = build_launch(hs, hjobs, numJobs, L, who);
+  if (st != CT_STATUS_SUCCESS) return st;
+  if (L.offsets) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": ragged rows need a plan");
+  const size_t n = (size_t)L.T * L.S;
+  const size_t bytes = n * sizeof(float);
+  // device buffers from the stream-ordered pool
+  std::vector<void*> owned;
+  auto alloc = [&](size_t b) -> void* {
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, b, stream) != cudaSuccess) return nullptr;
+    owned.push_back(p);
+    return p;
+  };
+  auto release = [&]() { for (void* p : owned) cudaFreeAsync(p, stream); };
+  const float* hplanes[tb::P_COUNT];
+  for (int p = 0; p < tb::P_COUNT; ++p) {
+    hplanes[p] = L.plane[p];
+    if (!L.plane[p]) continue;
+    void* d = alloc(bytes);
+    if (!d) { release(); return fail(CT_STATUS_ALLOC_FAILED, std::string(who) + ": device allocation failed"); }
+    if (cudaMemcpyAsync(d, L.plane[p], bytes, cudaMemcpyHostToDevice, stream) != cudaSuccess) {
+      release();
+      return fail(CT_STATUS_COPY_FAILED, std::string(who) + ": host to device copy failed");
+    }
+    L.plane[p] = static_cast<const float*>(d);
+  }
+  std::vector<std::pair<void*, std::pair<void*, size_t>>> back;  // device, host, bytes
+  for (int j = 0; j < L.njobs; ++j) {
+    Job& jb = L.jobs[j];
+    if (jb.family == tb::F_CDL) {
+      int cnt = 0;
+      for (int k = 0; k < tb::kCdlPatterns; ++k) cnt += (jb.cdl_mask >> k) & 1;
+      const size_t span = jb.cdl_stride > 0 ? (size_t)jb.cdl_stride * (tb::kCdlPatterns - 1) + n : n;
+      (void)cnt;
+      const size_t b = span * 4;
+      void* d = alloc(b);
+      if (!d) { release(); return fail(CT_STATUS_ALLOC_FAILED, std::string(who) + ": device allocation failed"); }
+      back.push_back({d, {jb.out[0], b}});
+      jb.out[0] = d;
+      continue;
+    }
+    for (int o = 0; o < output_count(jb.family); ++o) {
+      void* d = alloc(bytes);
+      if (!d) { release(); return fail(CT_STATUS_ALLOC_FAILED, std::string(who) + ": device allocation failed"); }
+      back.push_back({d, {jb.out[o], bytes}});
+      jb.out[o] = d;
+    }
+  }
+  (void)hplanes;
+  st = launch(L, (long long)n, L.T, nullptr, stream, who);
+  if (st != CT_STATUS_SUCCESS) { release(); return st; }
+  for (auto& b : back) {
+    if (cudaMemcpyAsync(b.second.first, b.first, b.second.second, cudaMemcpyDeviceToHost, stream) != cudaSuccess) {
+      release();
+      return fail(CT_STATUS_COPY_FAILED, std::string(who) + ": device to host copy failed");
+    }
+  }
+  release();
+  if (stream == 0 || true) {
+    const cudaError_t e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_fail(CT_STATUS_DEVICE_ERROR, who, e);
+  }
+  return CT_STATUS_SUCCESS;
+}
+
+// ------------------------------------------------------------ plans
+
+ctStatus_t ct_b200_plan_create(const ctB200Job* jobs, int numJobs, const int64_t* hostOffsets, int numSeries,
+                               int64_t seriesLen, ctB200Plan** out) {
+  clear_error();
+  const char* who = "ct_b200_plan_create";
+  if (!out || !jobs || numJobs <= 0 || numJobs > tb::kMaxJobs || numSeries <= 0 || (!hostOffsets && seriesLen <= 0))
+    return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": null pointer or invalid size");
+  ctB200Plan* plan = new (std::nothrow) ctB200Plan();
+  if (!plan) return fail(CT_STATUS_ALLOC_FAILED, std::string(who) + ": out of host memory");
+  plan->njobs = numJobs;
+  plan->numSeries = numSeries;
+  plan->seriesLen = seriesLen;
+  plan->ragged = hostOffsets != nullptr;
+  plan->jobs.resize(numJobs);
+  for (int j = 0; j < numJobs; ++j) {
+    ctB200Job u = jobs[j];
+    // outputs are supplied at execution; validate shape with a placeholder
+    for (int o = 0; o < 3; ++o) if (!u.outputs[o]) u.outputs[o] = reinterpret_cast<void*>(16);
+    const ctStatus_t st = make_job(u, plan->jobs[j], who);
+    if (st != CT_STATUS_SUCCESS) { delete plan; return st; }
+  }
+  Launch L;
+  std::memset(&L, 0, sizeof(L));
+  L.S = numSeries;
+  L.njobs = numJobs;
+  for (int j = 0; j < numJobs; ++j) L.jobs[j] = plan->jobs[j];
+  cudaGetDevice(&plan->device);
+  if (plan->ragged) {
+    std::vector<long long> len(numSeries);
+    long long total = 0, mx = 0;
+    for (int s = 0; s < numSeries; ++s) {
+      len[s] = hostOffsets[s + 1] - hostOffsets[s];
+      if (len[s] < 0) { delete plan; return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": offsets decrease"); }
+      total += len[s];
+      mx = std::max(mx, len[s]);
+    }
+    std::vector<int> order(numSeries);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return len[a] > len[b]; });
+    if (cudaMalloc(&plan->d_order, sizeof(int) * numSeries) != cudaSuccess) {
+      delete plan;
+      return fail(CT_STATUS_ALLOC_FAILED, std::string(who) + ": device allocation failed");
+    }
+    if (cudaMemcpy(plan->d_order, order.data(), sizeof(int) * numSeries, cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaFree(plan->d_order);
+      delete plan;
+      return fail(CT_STATUS_COPY_FAILED, std::string(who) + ": order upload failed");
+    }
+    plan->total = total;
+    plan->maxlen = mx;
+  } else {
+    plan->total = seriesLen * (long long)numSeries;
+    plan->maxlen = seriesLen;
+  }
+  plan->sched = tb::plan_for(L, plan->total, plan->maxlen);
+  *out = plan;
+  return CT_STATUS_SUCCESS;
+}
+
+static ctStatus_t plan_launch(const ctB200Plan* plan, const ctB200Series* series, const ctB200Job* jobs,
+                              int numJobs, const tb::SchedulePlan& sched, cudaStream_t stream, const char* who,
+                              tb::LaunchStats* stats) {
+  if (!plan) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": null plan");
+  Launch L;
+  ctStatus_t st = build_launch(series, jobs, numJobs, L, who);
+  if (st != CT_STATUS_SUCCESS) return st;
+  if (numJobs != plan->njobs || series->numSeries != plan->numSeries || (series->offsets != nullptr) != plan->ragged ||
+      (!plan->ragged && series->seriesLen != plan->seriesLen))
+    return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": batch does not match the plan");
+  for (int j = 0; j < numJobs; ++j) {
+    const Job& a = L.jobs[j];
+    const Job& b = plan->jobs[j];
+    if (a.family != b.family || a.ip[0] != b.ip[0] || a.ip[1] != b.ip[1] || a.ip[2] != b.ip[2])
+      return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": jobs do not match the plan");
+  }
+  L.order = plan->d_order;
+  return launch(L, plan->total, plan->maxlen, &sched, stream, who, stats);
+}
+
+ctStatus_t ct_b200_plan_execute(const ctB200Plan* plan, const ctB200Series* series, const ctB200Job* jobs,
+                                int numJobs, cudaStream_t stream) {
+  clear_error();
+  const char* who = "ct_b200_plan_execute";
+  const ctStatus_t st = plan_launch(plan, series, jobs, numJobs, plan ? plan->sched : tb::SchedulePlan{}, stream,
+                                    who, nullptr);
+  if (st != CT_STATUS_SUCCESS) return st;
+  return finish(stream, who);
+}
+
+ctStatus_t ct_b200_plan_autotune(ctB200Plan* plan, const ctB200Series* series, const ctB200Job* jobs, int numJobs,
+                                 cudaStream_t stream) {
+  clear_error();
+  const char* who = "ct_b200_plan_autotune";
+  if (!plan) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": null plan");
+  const int ks[3] = {4, 8, 16};
+  const int ws[3] = {4, 8, 16};
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  tb::SchedulePlan bestPlan = plan->sched;
+  for (int ki : ks) {
+    if (ki == 4 && plan->maxlen > 4096) continue;
+    for (int wi : ws) {
+      tb::SchedulePlan cand;
+      cand.k = ki;
+      cand.warps_per_block = wi;
+      ctStatus_t st = plan_launch(plan, series, jobs, numJobs, cand, stream, who, nullptr);  // warm-up
+      if (st != CT_STATUS_SUCCESS) continue;
+      cudaEventRecord(e0, stream);
+      for (int r = 0; r < 3; ++r) plan_launch(plan, series, jobs, numJobs, cand, stream, who, nullptr);
+      cudaEventRecord(e1, stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess) continue;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) { best = ms; bestPlan = cand; }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  clear_error();
+  plan->sched = bestPlan;
+  Launch L;
+  std::memset(&L, 0, sizeof(L));
+  L.S = plan->numSeries;
+  L.njobs = plan->njobs;
+  for (int j = 0; j < plan->njobs; ++j) L.jobs[j] = plan->jobs[j];
+  tb::remember_plan(tb::shape_key(L, plan->total, plan->maxlen), bestPlan);
+  return CT_STATUS_SUCCESS;
+}
+
+ctStatus_t ct_b200_plan_describe(const ctB200Plan* plan, int* barsPerLane, int* warpsPerBlock, int* blocks) {
+  clear_error();
+  if (!plan) return fail(CT_STATUS_INVALID_ARGUMENT, "ct_b200_plan_describe: null plan");
+  if (barsPerLane) *barsPerLane = plan->sched.k;
+  if (warpsPerBlock) *warpsPerBlock = plan->sched.warps_per_block;
+  if (blocks) *blocks = plan->sched.max_blocks;
+  return CT_STATUS_SUCCESS;
+}
+
+ctStatus_t ct_b200_plan_destroy(ctB200Plan* plan) {
+  clear_error();
+  if (!plan) return CT_STATUS_SUCCESS;
+  if (plan->d_order) {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(plan->device);
+    cudaFree(plan->d_order);
+    cudaSetDevice(cur);
+  }
+  delete plan;
+  return CT_STATUS_SUCCESS;
+}
+
+// ------------------------------------------------------------ host batch API
+
+static ctStatus_t host_run(const std::vector<const float*>& hin, const std::vector<float*>& hout, size_t n,
+                           cudaStream_t stream, const char* who,
+                           ctStatus_t (*dev)(const std::vector<const float*>&, const std::vector<float*>&, void*,
+                                             cudaStream_t),
+                           void* ctx) {
+  std::vector<void*> owned;
+  auto release = [&]() { for (void* p : owned) cudaFreeAsync(p, stream); };
+  std::vector<const float*> din;
+  std::vector<float*> dout;
+  for (const float* h : hin) {
+    void* d = nullptr;
+    if (cudaMallocAsync(&d, n * 4, stream) != cudaSuccess) { release(); return fail(CT_STATUS_ALLOC_FAILED, std::string(who) + ": device allocation failed"); }
+    owned.push_back(d);
+    if (cudaMemcpyAsync(d, h, n * 4, cudaMemcpyHostToDevice, stream) != cudaSuccess) { release(); return fail(CT_STATUS_COPY_FAILED, std::string(who) + ": copy failed"); }
+    din.push_back(static_cast<const float*>(d));
+  }
+  for (size_t i = 0; i < hout.size(); ++i) {
+    void* d = nullptr;
+    if (cudaMallocAsync(&d, n * 4, stream) != cudaSuccess) { release(); return fail(CT_STATUS_ALLOC_FAILED, std::string(who) + ": device allocation failed"); }
+    owned.push_back(d);
+    dout.push_back(static_cast<float*>(d));
+  }
+  // run on a private non-null stream view so the device call does not sync early
+  ctStatus_t st = dev(din, dout, ctx, stream == 0 ? cudaStreamPerThread : stream);
+  if (st != CT_STATUS_SUCCESS) { release(); return st; }
+  cudaStream_t s2 = stream == 0 ? cudaStreamPerThread : stream;
+  for (size_t i = 0; i < hout.size(); ++i)
+    if (cudaMemcpyAsync(hout[i], dout[i], n * 4, cudaMemcpyDeviceToHost, s2) != cudaSuccess) { release(); return fail(CT_STATUS_COPY_FAILED, std::string(who) + ": copy failed"); }
+  release();
+  const cudaError_t e = cudaStreamSynchronize(s2);
+  if (e != cudaSuccess) return cuda_fail(CT_STATUS_DEVICE_ERROR, who, e);
+  return CT_STATUS_SUCCESS;
+}
+
+struct HostArgs { int len, n, p0, p1, p2, p3; float f0, f1; };
+
+#define TB_HOST_S1(NAME)                                                                                   \
+  ctStatus_t ct_##NAME##_batch(const float* host_inputs, float* host_outputs, int seriesLen, int numSeries, \
+                               int period, int, cudaStream_t stream) {                                     \
+    clear_error();                                                                                         \
+    if (!host_inputs || !host_outputs || seriesLen <= 0 || numSeries <= 0)                                  \
+      return fail(CT_STATUS_INVALID_ARGUMENT, "ct_" #NAME "_batch: null pointer or invalid size");          \
+    HostArgs a{seriesLen, numSeries, period, 0, 0, 0, 0.f, 0.f};                                           \
+    return host_run({host_inputs}, {host_outputs}, (size_t)seriesLen * numSeries, stream, "ct_" #NAME "_batch", \
+                    [](const std::vector<const float*>& i, const std::vector<float*>& o, void* c, cudaStream_t s) { \
+                      const HostArgs& h = *static_cast<HostArgs*>(c);                                      \
+                      return ct_##NAME##_batch_d(i[0], o[0], h.len, h.n, h.p0, 0, s);                      \
+                    }, &a);                                                                                \
+  }
+TB_HOST_S1(sma)
+TB_HOST_S1(ema)
+TB_HOST_S1(rsi)
+#undef TB_HOST_S1
+
+ctStatus_t ct_atr_batch(const float* h, const float* l, const float* c, float* out, int seriesLen, int numSeries,
+                        int period, float, int, cudaStream_t stream) {
+  clear_error();
+  if (!h || !l || !c || !out || seriesLen <= 0 || numSeries <= 0)
+    return fail(CT_STATUS_INVALID_ARGUMENT, "ct_atr_batch: null pointer or invalid size");
+  HostArgs a{seriesLen, numSeries, period, 0, 0, 0, 0.f, 0.f};
+  return host_run({h, l, c}, {out}, (size_t)seriesLen * numSeries, stream, "ct_atr_batch",
+                  [](const std::vector<const float*>& i, const std::vector<float*>& o, void* x, cudaStream_t s) {
+                    const HostArgs& q = *static_cast<HostArgs*>(x);
+                    return ct_atr_batch_d(i[0], i[1], i[2], o[0], q.len, q.n, q.p0, 0.f, 0, s);
+                  }, &a);
+}
+
+ctStatus_t ct_macd_batch(const float* in, float* m, float* sg, float* hs, int seriesLen, int numSeries, int fast,
+                         int slow, int signal, int maType, int, cudaStream_t stream) {
+  clear_error();
+  if (!in || !m || !sg || !hs || seriesLen <= 0 || numSeries <= 0)
+    return fail(CT_STATUS_INVALID_ARGUMENT, "ct_macd_batch: null pointer or invalid size");
+  HostArgs a{seriesLen, numSeries, fast, slow, signal, maType, 0.f, 0.f};
+  return host_run({in}, {m, sg, hs}, (size_t)seriesLen * numSeries, stream, "ct_macd_batch",
+                  [](const std::vector<const float*>& i, const std::vector<float*>& o, void* x, cudaStream_t s) {
+                    const HostArgs& q = *static_cast<HostArgs*>(x);
+                    return ct_macd_batch_d(i[0], o[0], o[1], o[2], q.len, q.n, q.p0, q.p1, q.p2, q.p3, 0, s);
+                  }, &a);
+}
+
+ctStatus_t ct_bbands_batch(const float* in, float* u, float* mid, float* lo, int seriesLen, int numSeries, int period,
+                           float upperMul, float lowerMul, int, cudaStream_t stream) {
+  clear_error();
+  if (!in || !u || !mid || !lo || seriesLen <= 0 || numSeries <= 0)
+    return fail(CT_STATUS_INVALID_ARGUMENT, "ct_bbands_batch: null pointer or invalid size");
+  HostArgs a{seriesLen, numSeries, period, 0, 0, 0, upperMul, lowerMul};
+  return host_run({in}, {u, mid, lo}, (size_t)seriesLen * numSeries, stream, "ct_bbands_batch",
+                  [](const std::vector<const float*>& i, const std::vector<float*>& o, void* x, cudaStream_t s) {
+                    const HostArgs& q = *static_cast<HostArgs*>(x);
+                    return ct_bbands_batch_d(i[0], o[0], o[1], o[2], q.len, q.n, q.p0, q.f0, q.f1, 0, s);
+                  }, &a);
+}
+
+ctStatus_t ct_stochastic_batch(const float* h, const float* l, const float* c, float* k, float* d, int seriesLen,
+                               int numSeries, int kPeriod, int dPeriod, int, cudaStream_t stream) {
+  clear_error();
+  if (!h || !l || !c || !k || !d || seriesLen <= 0 || numSeries <= 0)
+    return fail(CT_STATUS_INVALID_ARGUMENT, "ct_stochastic_batch: null pointer or invalid size");
+  HostArgs a{seriesLen, numSeries, kPeriod, dPeriod, 0, 0, 0.f, 0.f};
+  return host_run({h, l, c}, {k, d}, (size_t)seriesLen * numSeries, stream, "ct_stochastic_batch",
+                  [](const std::vector<const float*>& i, const std::vector<float*>& o, void* x, cudaStream_t s) {
+                    const HostArgs& q = *static_cast<HostArgs*>(x);
+                    return ct_stochastic_batch_d(i[0], i[1], i[2], o[0], o[1], q.len, q.n, q.p0, q.p1, 0, s);
+                  }, &a);
+}
+
+}  // extern "C"

@@ -1,0 +1,56 @@
+// Launch descriptors shared by the host scheduler and the device engine.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tb {
+
+// Indicator families the engine evaluates. Each maps to one reference batch
+// entry point (ct_<family>_batch_d) except CDL, which evaluates any subset of
+// the candle patterns in one pass.
+enum Family : int {
+  F_SMA = 0, F_EMA, F_WMA, F_RSI, F_MACD, F_ATR, F_NATR, F_TRANGE, F_ADX, F_DX,
+  F_BBANDS, F_STOCH, F_CCI, F_OBV, F_AD, F_ADOSC, F_MFI, F_WILLR, F_SUM, F_MIN,
+  F_MAX, F_STDDEV, F_VAR, F_LINEARREG, F_CORREL, F_DEMA, F_TEMA, F_T3, F_CDL,
+  F_COUNT
+};
+
+// Input planes of a launch. Single-input families read in[0] of their job.
+enum Plane : int { P_OPEN = 0, P_HIGH, P_LOW, P_CLOSE, P_VOLUME, P_AUX, P_COUNT };
+
+constexpr int kMaxJobs = 24;
+constexpr int kMaxOut = 3;
+constexpr int kCdlPatterns = 63;
+
+struct Job {
+  int family;
+  int ip[3];        // integer parameters (periods) in reference order
+  double fp[4];     // real parameters and host-precomputed coefficients
+  int in[4];        // plane index of each logical input
+  void* out[kMaxOut];
+  // CDL only: pattern k is written to out[0] + k * cdl_stride elements when bit
+  // k of the mask is set; int32 when cdl_int32 else float32.
+  uint64_t cdl_mask;
+  long long cdl_stride;
+  int cdl_int32;
+  int halo;         // bars of history this job reads before a round
+};
+
+struct Launch {
+  const float* plane[P_COUNT];
+  const long long* offsets;  // ragged row starts (S+1 entries) or nullptr
+  const int* order;          // processing order of series (longest first) or nullptr
+  long long T;               // uniform row length when offsets == nullptr
+  int S;
+  int njobs;
+  int halo;                  // multiple of 32, >= every job's halo
+  unsigned plane_mask;       // planes staged in shared memory
+  int need_tp;               // stage the FP64 typical price ((h+l)+c)/3
+  int* sched;                // [0] series counter, [1] finished warps (self-resetting)
+  int total_warps;
+  int* err;                  // device error word (0 = ok)
+  Job jobs[kMaxJobs];
+};
+
+}  // namespace tb

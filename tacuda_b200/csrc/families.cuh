@@ -1,0 +1,1020 @@
+// Per-round device implementations of the indicator families.
+//
+// A "round" is TILE = 32*K consecutive bars of one series handled by one warp
+// (lane l owns K consecutive bars). Recurrences are evaluated as piecewise
+// affine maps in FP64: each lane composes its K maps, a warp shuffle scan
+// stitches the lanes, then every lane replays its bars with the exact TA-Lib
+// arithmetic starting from its incoming state. Windows read the staged halo.
+//
+// Arithmetic per family follows the pinned TA-Lib 0.8.3 C
+// (src/compat/talib08_formulas.inc in the reference, "talib08" below) or, for
+// families the vendored set lacks, the reference kernels; the citations are on
+// each round function. Outputs are float32 with NaN warm-up.
+#pragma once
+
+#include "common.cuh"
+#include "engine.h"
+
+namespace tb {
+
+// Carry of one job between rounds of a series (kept in shared memory).
+struct Carry {
+  long long f;  // first bar that counts (after leading NaNs), -1 = not found yet
+  double v[10];
+};
+
+template <int K>
+struct Ctx {
+  static constexpr int TILE = 32 * K;
+  static constexpr int EXT = 64;                                 // front extension of a line
+  static constexpr int LINE = (TILE + EXT) + (TILE + EXT) / 16 + 1;  // padded doubles per line
+  int lane;
+  long long n;     // row length
+  long long t0;    // first bar of the round
+  int L;           // bars in the round
+  int H;           // staged halo
+  long long base;  // row offset in the planes
+  float* sp[P_COUNT];
+  double* tp;      // typical price plane (padded like sp) or nullptr
+  double* dscr;    // per-warp FP64 scratch lines
+  float* stage[kMaxOut];
+  int* istage;
+
+  __device__ __forceinline__ long long gb0() const { return t0 + (long long)lane * K; }
+  __device__ __forceinline__ bool valid(long long t) const { return t < t0 + L; }
+  __device__ __forceinline__ float x(int p, long long t) const { return sp[p][pad((int)(t - t0) + H)]; }
+  __device__ __forceinline__ double typ(long long t) const {
+    const int i = (int)(t - t0) + H;
+    return tp[i + (i >> 4)];
+  }
+  // Scratch line entry for round-relative bar idx in [-EXT, TILE).
+  __device__ __forceinline__ double& eline(int ln, int idx) const {
+    const int i = idx + EXT;
+    return dscr[ln * LINE + i + (i >> 4)];
+  }
+  __device__ __forceinline__ double& line(int ln, int k) const { return eline(ln, lane * K + k); }
+  __device__ __forceinline__ void put(int j, int k, float v) const { stage[j][pad(lane * K + k)] = v; }
+
+  // Coalesced copy of staged output j to out[base + t0 .. + L).
+  __device__ __forceinline__ void flush(int j, float* out) const {
+    __syncwarp();
+    float* dst = out + base + t0;
+    for (int i = lane; i < L; i += 32) dst[i] = stage[j][pad(i)];
+    __syncwarp();
+  }
+};
+
+// First bar from which a single-input recurrence counts: the first non-NaN bar
+// of the row (src/api/BatchFused.cu:34-41 skips a leading NaN run). Resolved
+// once per series; warp-uniform. -1 while the row is all NaN so far.
+template <int K>
+__device__ __forceinline__ long long resolve_start(const Ctx<K>& c, const Carry& cy, int plane) {
+  if (cy.f >= 0) return cy.f;
+  long long first = 0x7fffffffffffffffll;
+  for (int k = 0; k < K; ++k) {
+    const long long t = c.gb0() + k;
+    if (c.valid(t) && !isnan(c.x(plane, t))) { first = t; break; }
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) first = min(first, __shfl_xor_sync(kFull, first, d));
+  return first == 0x7fffffffffffffffll ? -1 : first;
+}
+
+// Value held after the last valid bar of the round (exact replay state).
+template <int K>
+__device__ __forceinline__ double round_tail(const Ctx<K>& c, double v) {
+  return __shfl_sync(kFull, v, (c.L - 1) / K);
+}
+
+// ----------------------------------------------------------------- EMA core
+
+// One EMA stage in TA-Lib order (talib08:5546-5627): inputs counted from
+// `start` are summed, the mean of the first p seeds the average at count
+// start+p-1, later bars apply y = fma(beta, y, k*x). Period 1 copies.
+struct EmaStage {
+  int p, start;
+  double beta, k, inv;
+  __device__ __forceinline__ void map(long long cnt, double x, double& a, double& b) const {
+    if (cnt < start) { a = 1.0; b = 0.0; return; }
+    if (p == 1) { a = 0.0; b = x; return; }
+    const long long r = cnt - start;
+    if (r < p - 1) { a = 1.0; b = x; }
+    else if (r == p - 1) { a = inv; b = x * inv; }
+    else { a = beta; b = k * x; }
+  }
+  __device__ __forceinline__ double step(long long cnt, double y, double x) const {
+    if (cnt < start) return y;
+    if (p == 1) return x;
+    const long long r = cnt - start;
+    if (r < p - 1) return y + x;
+    if (r == p - 1) return (y + x) / p;
+    return fma(beta, y, k * x);
+  }
+  __device__ __forceinline__ bool ready(long long cnt) const { return cnt >= start + p - 1; }
+};
+
+// Scan one EMA-like stage over the round. in(t, k) gives the FP64 input of the
+// lane's k-th bar; sink(k, cnt, y) receives the state after it (cnt = -1
+// before the series starts). Returns the state after the round.
+template <int K, class Stage, class In, class Sink>
+__device__ __forceinline__ double stage_round(const Ctx<K>& c, long long f, const Stage& st,
+                                              double carry, In in, Sink sink) {
+  double A = 1.0, B = 0.0;
+  const long long g0 = c.gb0();
+  if (f >= 0) {
+#pragma unroll 4
+    for (int k = 0; k < K; ++k) {
+      const long long t = g0 + k;
+      if (!c.valid(t)) break;
+      if (t < f) continue;
+      double a, b;
+      st.map(t - f, in(t, k), a, b);
+      B = fma(a, B, b);
+      A *= a;
+    }
+  }
+  warp_scan_affine(A, B, c.lane);
+  const double Ae = shfl_excl(A, 1.0, c.lane), Be = shfl_excl(B, 0.0, c.lane);
+  double y = fma(Ae, carry, Be);
+#pragma unroll 4
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    if (f < 0 || t < f) { sink(k, -1ll, y); continue; }
+    y = st.step(t - f, y, in(t, k));
+    sink(k, t - f, y);
+  }
+  return round_tail(c, y);
+}
+
+__host__ __device__ inline void talib_ema_coeffs(int p, double& beta, double& k) {
+  double b = (double)(p - 1) / (double)(p + 1);
+  double kk = 1.0 - b;
+  if (b < 0.5) b = 1.0 - kk;
+  beta = b;
+  k = kk;
+}
+
+// EMA(p): talib08:5546-5627 TA_EMA; leading NaNs skipped (BatchFused.cu:34-41).
+// fp[0] = beta, fp[1] = k (host-precomputed TA-Lib coefficients).
+template <int K>
+__device__ void ema_round(const Ctx<K>& c, const Job& j, Carry& cy) {
+  const int pl = j.in[0];
+  const long long f = resolve_start(c, cy, pl);
+  const EmaStage st{j.ip[0], 0, j.fp[0], j.fp[1], 1.0 / j.ip[0]};
+  cy.v[0] = stage_round(
+      c, f, st, cy.v[0], [&](long long t, int) { return (double)c.x(pl, t); },
+      [&](int k, long long cnt, double v) { c.put(0, k, (cnt >= 0 && st.ready(cnt)) ? (float)v : qnan()); });
+  cy.f = f;
+  c.flush(0, (float*)j.out[0]);
+}
+
+// DEMA / TEMA / T3: cascades of EMA stages, stage s seeded with the mean of the
+// first p values of stage s-1 (talib08:4846-4945 DEMA, 17496-17612 TEMA,
+// 17331-17481 T3). DEMA/TEMA use TA_EMA's coefficients, T3 k=2/(p+1) with
+// fma(1-k, e, k*x) and the GD combination; fp[0]=beta fp[1]=k, fp[2]=vfactor.
+// Scratch lines: 0 = running stage value, 1.. = stage values kept for the
+// combination (DEMA: e1; TEMA: e1 e2; T3: e3 e4 e5).
+template <int K>
+__device__ void cascade_round(const Ctx<K>& c, const Job& j, Carry& cy, int stages) {
+  const int pl = j.in[0];
+  const long long f = resolve_start(c, cy, pl);
+  const int p = j.ip[0];
+  const double beta = j.fp[0], kk = j.fp[1];
+  double c1 = 0, c2 = 0, c3 = 0, c4 = 0;
+  if (stages == 6) {
+    const double v = j.fp[2], tr = v * v;
+    c1 = -(tr * v);
+    c2 = 3.0 * (tr - c1);
+    c3 = -6.0 * tr - 3.0 * (v - c1);
+    c4 = fma(3.0, tr, fma(3.0, v, 1.0) - c1);
+  }
+  const int lb = stages * (p - 1);
+  for (int s = 0; s < stages; ++s) {
+    const EmaStage st{p, s * (p - 1), beta, kk, 1.0 / p};
+    const bool last = s == stages - 1;
+    // which kept line (if any) stores this stage's value
+    int keep = -1;
+    if (stages == 2 && s == 0) keep = 1;
+    if (stages == 3 && s < 2) keep = 1 + s;
+    if (stages == 6 && s >= 2 && s <= 4) keep = s - 1;
+    cy.v[s] = stage_round(
+        c, f, st, cy.v[s],
+        [&](long long t, int k) { return s == 0 ? (double)c.x(pl, t) : c.line(0, k); },
+        [&](int k, long long cnt, double v) {
+          c.line(0, k) = v;
+          if (keep >= 0) c.line(keep, k) = v;
+          if (last) {
+            float o = qnan();
+            if (cnt >= lb) {
+              if (p == 1) o = (float)v;
+              else if (stages == 2) o = (float)(2.0 * c.line(1, k) - v);
+              else if (stages == 3) o = (float)(v + (3.0 * c.line(1, k) - 3.0 * c.line(2, k)));
+              else o = (float)fma(c4, c.line(1, k), fma(c3, c.line(2, k), fma(c1, v, c2 * c.line(3, k))));
+            }
+            c.put(0, k, o);
+          }
+        });
+  }
+  cy.f = f;
+  c.flush(0, (float*)j.out[0]);
+}
+
+// ----------------------------------------------------------------- RSI
+
+// RSI(p): talib08:13996-14115 TA_RSI. Gains and losses of the first p changes
+// are summed and multiplied by 1/p; afterwards g = (g*(p-1) + gain)/p via the
+// same multiply by 1/p; 100*g/(g+l), 50 when both are zero. A NaN change makes
+// the row NaN from there on (StreamStates.h:663). Leading NaNs skipped.
+template <int K>
+__device__ void rsi_round(const Ctx<K>& c, const Job& j, Carry& cy) {
+  const int pl = j.in[0];
+  const long long f = resolve_start(c, cy, pl);
+  const int p = j.ip[0];
+  const double inv = 1.0 / (double)p, pm1 = (double)(p - 1);
+  const double steady = pm1 * inv;
+  double A = 1.0, B[2] = {0.0, 0.0};
+  const long long g0 = c.gb0();
+  auto change = [&](long long t, double& g, double& l) {
+    const double d = (double)c.x(pl, t) - (double)c.x(pl, t - 1);
+    if (isnan(d)) { g = l = d; return; }
+    g = d > 0.0 ? d : 0.0;
+    l = g - d;
+  };
+  if (f >= 0) {
+#pragma unroll 4
+    for (int k = 0; k < K; ++k) {
+      const long long t = g0 + k;
+      if (!c.valid(t)) break;
+      const long long cnt = t - f;
+      if (cnt <= 0) continue;
+      double g, l, a;
+      change(t, g, l);
+      if (cnt < p) a = 1.0;
+      else if (cnt == p) { a = inv; g *= inv; l *= inv; }
+      else { a = steady; g *= inv; l *= inv; }
+      B[0] = fma(a, B[0], g);
+      B[1] = fma(a, B[1], l);
+      A *= a;
+    }
+  }
+  warp_scan_affine_shared<2>(A, B, c.lane);
+  const double Ae = shfl_excl(A, 1.0, c.lane);
+  double gain = fma(Ae, cy.v[0], shfl_excl(B[0], 0.0, c.lane));
+  double loss = fma(Ae, cy.v[1], shfl_excl(B[1], 0.0, c.lane));
+#pragma unroll 4
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    const long long cnt = f < 0 ? -1 : t - f;
+    if (cnt > 0) {
+      double g, l;
+      change(t, g, l);
+      if (isnan(g)) { gain = loss = g; }
+      else if (cnt < p) { gain += g; loss += l; }
+      else if (cnt == p) { gain = (gain + g) * inv; loss = (loss + l) * inv; }
+      else {
+        gain = (gain * pm1 + g) * inv;
+        loss = (loss * pm1 + l) * inv;
+      }
+    }
+    float o = qnan();
+    if (cnt >= p) {
+      const double tot = gain + loss;
+      o = isnan(tot) ? qnan() : (tot > 0.0 ? (float)(100.0 * (gain / tot)) : 50.0f);
+    }
+    c.put(0, k, o);
+  }
+  cy.v[0] = round_tail(c, gain);
+  cy.v[1] = round_tail(c, loss);
+  cy.f = f;
+  c.flush(0, (float*)j.out[0]);
+}
+
+// ----------------------------------------------------------------- MACD
+
+// Fast/slow averages of MACD (talib08:9316-9505 TA_MACD): slow seeded with the
+// mean of the first `slow` bars, fast with the mean of the `fast` bars ending at
+// the same bar (slow-1), then fma(beta, y, k*x) each.
+struct MacdLine {
+  int fast, slow;
+  double fb, fk, sb, sk;
+};
+
+// MACD(fast, slow, signal): two scans (fast/slow lines, then the signal line
+// over the FP64 MACD values: mean of the first `signal` values, then EMA).
+// Reversed periods are swapped on the host. Outputs start at slow+signal-2.
+// fp: [fb, fk, sb, sk]; the signal coefficients are derived from ip[2].
+template <int K>
+__device__ void macd_round(const Ctx<K>& c, const Job& j, Carry& cy) {
+  const int pl = j.in[0];
+  const long long f = resolve_start(c, cy, pl);
+  const int fast = j.ip[0], slow = j.ip[1], sig = j.ip[2];
+  const EmaStage slowSt{slow, 0, j.fp[2], j.fp[3], 1.0 / slow};
+  const EmaStage fastSt{fast, slow - fast, j.fp[0], j.fp[1], 1.0 / fast};
+  double gb, gk;
+  talib_ema_coeffs(sig, gb, gk);
+  const long long start = slow - 1, ready = start + sig - 1;
+  // fast and slow lines: two independent affine channels
+  double Af = 1.0, Bf = 0.0, As = 1.0, Bs = 0.0;
+  const long long g0 = c.gb0();
+  if (f >= 0) {
+#pragma unroll 4
+    for (int k = 0; k < K; ++k) {
+      const long long t = g0 + k;
+      if (!c.valid(t)) break;
+      if (t < f) continue;
+      const double x = c.x(pl, t);
+      double a, b;
+      slowSt.map(t - f, x, a, b);
+      Bs = fma(a, Bs, b); As *= a;
+      fastSt.map(t - f, x, a, b);
+      Bf = fma(a, Bf, b); Af *= a;
+    }
+  }
+  warp_scan_affine(As, Bs, c.lane);
+  warp_scan_affine(Af, Bf, c.lane);
+  double ys = fma(shfl_excl(As, 1.0, c.lane), cy.v[1], shfl_excl(Bs, 0.0, c.lane));
+  double yf = fma(shfl_excl(Af, 1.0, c.lane), cy.v[0], shfl_excl(Bf, 0.0, c.lane));
+#pragma unroll 4
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    double m = 0.0;
+    if (f >= 0 && t >= f) {
+      const double x = c.x(pl, t);
+      ys = slowSt.step(t - f, ys, x);
+      yf = fastSt.step(t - f, yf, x);
+      m = yf - ys;
+    }
+    c.line(0, k) = m;
+  }
+  cy.v[0] = round_tail(c, yf);
+  cy.v[1] = round_tail(c, ys);
+  // signal line: accumulate MACD from `start`, seed at `ready`, then EMA
+  struct SigStage {
+    int sig; long long start, ready; double gb, gk, inv;
+    __device__ __forceinline__ void map(long long cnt, double m, double& a, double& b) const {
+      if (cnt < start) { a = 1.0; b = 0.0; }
+      else if (cnt < ready) { a = 1.0; b = m; }
+      else if (cnt == ready) { a = inv; b = m * inv; }
+      else if (sig == 1) { a = 0.0; b = m; }
+      else { a = gb; b = gk * m; }
+    }
+    __device__ __forceinline__ double step(long long cnt, double y, double m) const {
+      if (cnt < start) return y;
+      if (cnt < ready) return y + m;
+      if (cnt == ready) return (y + m) / sig;
+      return sig == 1 ? m : fma(gb, y, gk * m);
+    }
+  } sst{sig, start, ready, gb, gk, 1.0 / sig};
+  cy.v[2] = stage_round(
+      c, f, sst, cy.v[2], [&](long long, int k) { return c.line(0, k); },
+      [&](int k, long long cnt, double s) {
+        const bool ok = cnt >= ready;
+        const double m = c.line(0, k);
+        c.put(0, k, ok ? (float)m : qnan());
+        c.put(1, k, ok ? (float)s : qnan());
+        c.put(2, k, ok ? (float)(m - s) : qnan());
+      });
+  cy.f = f;
+  c.flush(0, (float*)j.out[0]);
+  c.flush(1, (float*)j.out[1]);
+  c.flush(2, (float*)j.out[2]);
+}
+
+// ----------------------------------------------------------------- ATR family
+
+// ATR(p): talib08:1931-2057 TA_ATR: mean of the true ranges of bars 1..p (first
+// output at bar p), then fma(wb, y, wa*tr) with wb = (p-1)/p, wa = 1-wb.
+// NATR (StreamStates.h:708-721): 100*ATR/close in FP64, 0 for a zero close;
+// period 1 keeps the unnormalised true range. TRANGE: true range from bar 1.
+// fp[0] = wb, fp[1] = wa. mode: 0 ATR, 1 NATR, 2 TRANGE.
+template <int K>
+__device__ void atr_round(const Ctx<K>& c, const Job& j, Carry& cy, int mode) {
+  const int ph = j.in[0], plo = j.in[1], pc = j.in[2];
+  const int p = mode == 2 ? 1 : j.ip[0];
+  const double wb = j.fp[0], wa = j.fp[1], inv = 1.0 / p;
+  auto tr = [&](long long t) {
+    return true_range((double)c.x(ph, t), (double)c.x(plo, t), (double)c.x(pc, t - 1));
+  };
+  const long long g0 = c.gb0();
+  if (mode == 2) {
+    for (int k = 0; k < K; ++k) {
+      const long long t = g0 + k;
+      if (!c.valid(t)) break;
+      c.put(0, k, t >= 1 ? (float)tr(t) : qnan());
+    }
+    c.flush(0, (float*)j.out[0]);
+    return;
+  }
+  double A = 1.0, B = 0.0;
+#pragma unroll 4
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    if (t == 0) continue;
+    const double r = tr(t);
+    double a, b;
+    if (t < p) { a = 1.0; b = r; }
+    else if (t == p) { a = inv; b = r * inv; }
+    else { a = wb; b = wa * r; }
+    B = fma(a, B, b);
+    A *= a;
+  }
+  warp_scan_affine(A, B, c.lane);
+  double y = fma(shfl_excl(A, 1.0, c.lane), cy.v[0], shfl_excl(B, 0.0, c.lane));
+#pragma unroll 4
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    if (t >= 1) {
+      const double r = tr(t);
+      if (t < p) y += r;
+      else if (t == p) y = (y + r) / p;
+      else y = fma(wb, y, wa * r);
+    }
+    float o = qnan();
+    if (t >= p) {
+      if (mode == 0 || p == 1) o = (float)y;
+      else {
+        const double cl = c.x(pc, t);
+        o = cl == 0.0 ? 0.0f : (float)((y / cl) * 100.0);
+      }
+    }
+    c.put(0, k, o);
+  }
+  cy.v[0] = round_tail(c, y);
+  c.flush(0, (float*)j.out[0]);
+}
+
+// ----------------------------------------------------------------- ADX / DX
+
+// ADX(p) / DX(p) as the reference computes them (src/indicators/DX.cu:18-52,
+// 85-135; ADX.cu:44-124; BatchShort.cu:168-230): bar 0 contributes TR = H-L and
+// no movement; TR, +DM, -DM are summed over bars 0..p-1, then S = a*S + x with
+// a = (p-1)/p; DX = 100|DI+ - DI-|/(DI+ + DI-) from bar p (0 when TR or the DI
+// sum is 0); ADX is the mean of DX over bars p..2p-1, then a*ADX + DX/p.
+// The reference keeps DI/DX in float; this path keeps them in FP64.
+template <int K>
+__device__ void adx_round(const Ctx<K>& c, const Job& j, Carry& cy, bool adx) {
+  const int ph = j.in[0], plo = j.in[1], pc = j.in[2];
+  const int p = j.ip[0];
+  const double a = ((double)p - 1.0) / (double)p;
+  auto moves = [&](long long t, double& r, double& pl, double& mi) {
+    if (t == 0) {
+      r = (double)c.x(ph, 0) - (double)c.x(plo, 0);
+      pl = mi = 0.0;
+      return;
+    }
+    const float up = c.x(ph, t) - c.x(ph, t - 1), dn = c.x(plo, t - 1) - c.x(plo, t);
+    pl = (up > 0.0f && up > dn) ? up : 0.0f;
+    mi = (dn > 0.0f && dn > up) ? dn : 0.0f;
+    const double hh = c.x(ph, t), ll = c.x(plo, t), yc = c.x(pc, t - 1);
+    r = fmax(hh - ll, fmax(fabs(hh - yc), fabs(ll - yc)));
+  };
+  const long long g0 = c.gb0();
+  double A = 1.0, B[3] = {0.0, 0.0, 0.0};
+#pragma unroll 2
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    double r, pl, mi;
+    moves(t, r, pl, mi);
+    const double m = t < p ? 1.0 : a;
+    B[0] = fma(m, B[0], r);
+    B[1] = fma(m, B[1], pl);
+    B[2] = fma(m, B[2], mi);
+    A *= m;
+  }
+  warp_scan_affine_shared<3>(A, B, c.lane);
+  const double Ae = shfl_excl(A, 1.0, c.lane);
+  double tr = fma(Ae, cy.v[0], shfl_excl(B[0], 0.0, c.lane));
+  double pd = fma(Ae, cy.v[1], shfl_excl(B[1], 0.0, c.lane));
+  double md = fma(Ae, cy.v[2], shfl_excl(B[2], 0.0, c.lane));
+#pragma unroll 2
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    double r, pl, mi;
+    moves(t, r, pl, mi);
+    double dx = 0.0;
+    if (t < p) { tr += r; pd += pl; md += mi; }
+    else {
+      tr = a * tr + r;
+      pd = a * pd + pl;
+      md = a * md + mi;
+      const double dip = tr > 0.0 ? 100.0 * pd / tr : 0.0;
+      const double dim = tr > 0.0 ? 100.0 * md / tr : 0.0;
+      const double tot = dip + dim;
+      dx = tot > 0.0 ? 100.0 * fabs(dip - dim) / tot : 0.0;
+    }
+    c.line(0, k) = dx;
+    if (!adx) c.put(0, k, t >= p ? (float)dx : qnan());
+  }
+  cy.v[0] = round_tail(c, tr);
+  cy.v[1] = round_tail(c, pd);
+  cy.v[2] = round_tail(c, md);
+  if (adx) {
+    struct AdxStage {
+      int p; double a, inv;
+      __device__ __forceinline__ void map(long long t, double dx, double& m, double& b) const {
+        if (t < p) { m = 1.0; b = 0.0; }
+        else if (t < 2 * p - 1) { m = 1.0; b = dx; }
+        else if (t == 2 * p - 1) { m = inv; b = dx * inv; }
+        else { m = a; b = dx / p; }
+      }
+      __device__ __forceinline__ double step(long long t, double y, double dx) const {
+        if (t < p) return y;
+        if (t < 2 * p - 1) return y + dx;
+        if (t == 2 * p - 1) return (y + dx) / p;
+        return a * y + dx / p;
+      }
+    } st{p, a, 1.0 / p};
+    cy.v[3] = stage_round(
+        c, 0, st, cy.v[3], [&](long long, int k) { return c.line(0, k); },
+        [&](int k, long long t, double y) { c.put(0, k, t >= 2 * p - 1 ? (float)y : qnan()); });
+  }
+  c.flush(0, (float*)j.out[0]);
+}
+
+// ----------------------------------------------------------------- volume
+
+// OBV (StreamStates.h:446-475): bar 0 adds its volume, later bars the volume
+// signed by the close change; FP64 running sum (exact for float32 volumes).
+// AD (:481-506): ((c-l)-(h-c))/(h-l)*v, skipped for non-finite bars and
+// non-positive ranges. ADOSC (:723-745): EMA(fast) - EMA(slow) of the AD line,
+// both seeded with AD[0], k = 2/(n+1), warm-up max(fast, slow)-1.
+// mode: 0 OBV (in: close, volume), 1 AD, 2 ADOSC (in: h, l, c, v).
+template <int K>
+__device__ void volume_round(const Ctx<K>& c, const Job& j, Carry& cy, int mode) {
+  const long long g0 = c.gb0();
+  auto term = [&](long long t) -> double {
+    if (mode == 0) {
+      const int pc = j.in[0], pv = j.in[1];
+      const double v = c.x(pv, t);
+      if (t == 0) return v;
+      const double pr = c.x(pc, t), pp = c.x(pc, t - 1);
+      const double s = pr > pp ? 1.0 : (pr < pp ? -1.0 : 0.0);
+      return s * v;
+    }
+    const double hi = c.x(j.in[0], t), lo = c.x(j.in[1], t), cl = c.x(j.in[2], t), vo = c.x(j.in[3], t);
+    if (isfinite(hi) && isfinite(lo) && isfinite(cl) && isfinite(vo)) {
+      const double range = hi - lo;
+      if (range > 0.0) return (((cl - lo) - (hi - cl)) / range) * vo;
+    }
+    return 0.0;
+  };
+  double B = 0.0;
+#pragma unroll 4
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    B += term(t);
+  }
+  // prefix sum (all multipliers are 1)
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const double u = __shfl_up_sync(kFull, B, d);
+    if (c.lane >= d) B += u;
+  }
+  double acc = cy.v[0] + shfl_excl(B, 0.0, c.lane);
+#pragma unroll 4
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    acc += term(t);
+    if (mode < 2) c.put(0, k, (float)acc);
+    else c.line(0, k) = acc;
+  }
+  cy.v[0] = round_tail(c, acc);
+  if (mode == 2) {
+    const int fp_ = j.ip[0], sp_ = j.ip[1];
+    const int warm = (fp_ > sp_ ? fp_ : sp_) - 1;
+    struct Osc {
+      double kk;
+      __device__ __forceinline__ void map(long long t, double ad, double& a, double& b) const {
+        if (t == 0) { a = 0.0; b = ad; } else { a = 1.0 - kk; b = kk * ad; }
+      }
+      __device__ __forceinline__ double step(long long t, double y, double ad) const {
+        return t == 0 ? ad : kk * ad + (1.0 - kk) * y;
+      }
+    };
+    const Osc fs{2.0 / (fp_ + 1.0)}, ss{2.0 / (sp_ + 1.0)};
+    cy.v[1] = stage_round(c, 0, fs, cy.v[1], [&](long long, int k) { return c.line(0, k); },
+                          [&](int k, long long, double y) { c.line(1, k) = y; });
+    cy.v[2] = stage_round(c, 0, ss, cy.v[2], [&](long long, int k) { return c.line(0, k); },
+                          [&](int k, long long t, double y) {
+                            c.put(0, k, t >= warm ? (float)(c.line(1, k) - y) : qnan());
+                          });
+  }
+  c.flush(0, (float*)j.out[0]);
+}
+
+// ----------------------------------------------------------------- windows
+
+// Lane-local sliding windows over the staged halo: the first window of the lane
+// is summed directly, later ones slide. NaN inputs only poison the windows that
+// contain them (src/api/BatchFused.cu:73-143 sums every window directly);
+// FP64 sums of float32 values are exact, so sliding equals direct summation.
+
+// SMA(p) (talib08:14748-14812), SUM(p) (BatchFused.cu:133-138), WMA(p)
+// (talib08:19171-19277, weights 1..p over the divider p(p+1)/2).
+// mode: 0 SMA, 1 SUM, 2 WMA.
+template <int K>
+__device__ void sum_window_round(const Ctx<K>& c, const Job& j, int mode) {
+  const int pl = j.in[0], p = j.ip[0];
+  const long long g0 = c.gb0();
+  const long long tf = g0 > p - 1 ? g0 : (long long)(p - 1);
+  double s = 0.0, w = 0.0;
+  int nn = 0;
+  if (tf < g0 + K && c.valid(tf)) {
+    for (int i = 0; i < p; ++i) {
+      const float v = c.x(pl, tf - p + 1 + i);
+      if (isnan(v)) ++nn;
+      else { s += (double)v; w += (double)v * (double)(i + 1); }
+    }
+  }
+  const double divider = (double)p * (p + 1) / 2.0;
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    float o = qnan();
+    if (t >= tf) {
+      if (t > tf) {
+        const float vin = c.x(pl, t), vout = c.x(pl, t - p);
+        if (mode == 2) w -= s;  // weights shift down by one (NaN-free part)
+        if (isnan(vout)) --nn; else s -= (double)vout;
+        if (isnan(vin)) ++nn;
+        else { s += (double)vin; if (mode == 2) w += (double)vin * (double)p; }
+      }
+      if (nn == 0) {
+        if (mode == 0) o = (float)(s / (double)p);
+        else if (mode == 1) o = (float)s;
+        else o = p == 1 ? c.x(pl, t) : (float)(w / divider);
+      }
+    }
+    c.put(0, k, o);
+  }
+  c.flush(0, (float*)j.out[0]);
+}
+
+// BBANDS(p, up, dn) with an SMA middle band (talib08:2068-2283), STDDEV(p, nb)
+// (talib08:16046-16100) and VAR(p) (talib08:18047-18183): population variance
+// of the window from FP64 moments of x - o about a lane-local origin o (the
+// sums are then exact), clamped at zero as the reference's batch path does.
+// The middle band is the exact window sum divided by p, as TA-Lib's.
+// mode: 0 BBANDS, 1 STDDEV, 2 VAR.
+template <int K>
+__device__ void moment_window_round(const Ctx<K>& c, const Job& j, int mode) {
+  const int pl = j.in[0], p = j.ip[0];
+  const long long g0 = c.gb0();
+  const long long tf = g0 > p - 1 ? g0 : (long long)(p - 1);
+  double raw = 0.0, s2 = 0.0, o = 0.0;
+  int nn = 0;
+  if (tf < g0 + K && c.valid(tf)) {
+    const float ov = c.x(pl, tf);
+    o = isnan(ov) ? 0.0 : (double)ov;
+    for (int i = 0; i < p; ++i) {
+      const float v = c.x(pl, tf - p + 1 + i);
+      if (isnan(v)) ++nn;
+      else { raw += (double)v; const double d = (double)v - o; s2 += d * d; }
+    }
+  }
+  const double inv = 1.0 / (double)p, po = (double)p * o;
+  const double up = j.fp[0], dn = j.fp[1];
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    float o0 = qnan(), o1 = qnan(), o2 = qnan();
+    if (t >= tf) {
+      if (t > tf) {
+        const float vin = c.x(pl, t), vout = c.x(pl, t - p);
+        if (isnan(vout)) --nn;
+        else { raw -= (double)vout; const double d = (double)vout - o; s2 -= d * d; }
+        if (isnan(vin)) ++nn;
+        else { raw += (double)vin; const double d = (double)vin - o; s2 += d * d; }
+      }
+      if (nn == 0) {
+        const double m1 = (raw - po) * inv;
+        double var = s2 * inv - m1 * m1;
+        if (!(var > 0.0)) var = 0.0;
+        if (mode == 2) o0 = (float)var;
+        else {
+          const double sd = var != 0.0 ? sqrt(var) : 0.0;
+          if (mode == 1) o0 = (float)(up != 1.0 ? sd * up : sd);
+          else {
+            const double mid = raw / (double)p;
+            if (up == dn) { const double dv = sd * up; o0 = (float)(mid + dv); o2 = (float)(mid - dv); }
+            else { o0 = (float)fma(sd, up, mid); o2 = (float)(mid - sd * dn); }
+            o1 = (float)mid;
+          }
+        }
+      }
+    }
+    c.put(0, k, o0);
+    if (mode == 0) { c.put(1, k, o1); c.put(2, k, o2); }
+  }
+  c.flush(0, (float*)j.out[0]);
+  if (mode == 0) { c.flush(1, (float*)j.out[1]); c.flush(2, (float*)j.out[2]); }
+}
+
+// LINEARREG(p): talib08:9087-9197 TA_LINEARREG: least-squares line of the
+// window evaluated at its last bar, fma(m, p-1, b). Sums are taken about a
+// lane-local origin o (LINEARREG(o + d) = o + LINEARREG(d)) and slide as
+// TA-Lib's: SumXY += SumY - p*y_out, SumY += y_in - y_out.
+template <int K>
+__device__ void linreg_round(const Ctx<K>& c, const Job& j) {
+  const int pl = j.in[0], p = j.ip[0];
+  const long long g0 = c.gb0();
+  const long long tf = g0 > p - 1 ? g0 : (long long)(p - 1);
+  const double sumX = (double)p * (p - 1) * 0.5;
+  const double sumXSqr = (double)p * (p - 1) * (2 * p - 1) / 6.0;
+  const double divisor = sumX * sumX - p * sumXSqr;
+  double sy = 0.0, sxy = 0.0, o = 0.0;
+  int nn = 0;
+  if (tf < g0 + K && c.valid(tf)) {
+    const float ov = c.x(pl, tf);
+    o = isnan(ov) ? 0.0 : (double)ov;
+    for (int i = p - 1; i >= 0; --i) {
+      const float v = c.x(pl, tf - i);
+      if (isnan(v)) ++nn;
+      else { const double d = (double)v - o; sy += d; sxy += (double)i * d; }
+    }
+  }
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    float out = qnan();
+    if (t >= tf) {
+      if (t > tf) {
+        const float vout = c.x(pl, t - p), vin = c.x(pl, t);
+        const double dout = isnan(vout) ? 0.0 : (double)vout - o;
+        const double din = isnan(vin) ? 0.0 : (double)vin - o;
+        sxy = sxy + sy - (double)p * dout;
+        sy = sy - dout + din;
+        nn += (isnan(vin) ? 1 : 0) - (isnan(vout) ? 1 : 0);
+      }
+      if (nn == 0) {
+        const double m = (p * sxy - sumX * sy) / divisor;
+        const double b = (sy - m * sumX) / (double)p;
+        out = (float)(o + fma(m, (double)(p - 1), b));
+      }
+    }
+    c.put(0, k, out);
+  }
+  c.flush(0, (float*)j.out[0]);
+}
+
+// Window extrema over [t-p+1, t] of a float plane; fmaxf/fminf ignore NaN.
+template <int K>
+__device__ __forceinline__ float win_max(const Ctx<K>& c, int pl, long long t, int p) {
+  float v = c.x(pl, t - p + 1);
+  for (int i = 1; i < p; ++i) v = fmaxf(v, c.x(pl, t - p + 1 + i));
+  return v;
+}
+template <int K>
+__device__ __forceinline__ float win_min(const Ctx<K>& c, int pl, long long t, int p) {
+  float v = c.x(pl, t - p + 1);
+  for (int i = 1; i < p; ++i) v = fminf(v, c.x(pl, t - p + 1 + i));
+  return v;
+}
+
+// MIN(p) / MAX(p): BatchFused.cu:110-119 (float extrema; a window reaching
+// into the row's leading NaN run stays NaN, LeadingNaN.cuh:21-27).
+template <int K>
+__device__ void minmax_round(const Ctx<K>& c, const Job& j, Carry& cy, bool is_max) {
+  const int pl = j.in[0], p = j.ip[0];
+  const long long f = resolve_start(c, cy, pl);
+  const long long g0 = c.gb0();
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    float o = qnan();
+    if (t >= p - 1) {
+      o = is_max ? win_max(c, pl, t, p) : win_min(c, pl, t, p);
+      if (f < 0 || t - p + 1 < f) o = qnan();
+    }
+    c.put(0, k, o);
+  }
+  cy.f = f;
+  c.flush(0, (float*)j.out[0]);
+}
+
+// WILLR(p): src/indicators/WILLR.cu:11-30: float window extrema (strict
+// comparisons seeded with the current bar), ((HH - C)/(HH - LL)) * -100 in
+// FP64, clamped to [-100, 0]; 0 for a zero range.
+template <int K>
+__device__ void willr_round(const Ctx<K>& c, const Job& j) {
+  const int ph = j.in[0], plo = j.in[1], pc = j.in[2], p = j.ip[0];
+  const long long g0 = c.gb0();
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    float o = qnan();
+    if (t >= p - 1) {
+      float hi = c.x(ph, t), lo = c.x(plo, t);
+      for (int i = 1; i < p; ++i) {
+        const float h = c.x(ph, t - i), l = c.x(plo, t - i);
+        if (h > hi) hi = h;
+        if (l < lo) lo = l;
+      }
+      const double den = (double)hi - (double)lo;
+      const double v = den == 0.0 ? 0.0 : (((double)hi - (double)c.x(pc, t)) / den) * -100.0;
+      o = isnan(v) ? qnan() : (float)fmin(0.0, fmax(-100.0, v));
+    }
+    c.put(0, k, o);
+  }
+  c.flush(0, (float*)j.out[0]);
+}
+
+// STOCH(k, d) with SMA slowing (talib08:16115-16302): fastK from window
+// extrema with TA-Lib's scaled zero-range test, slowK = SMA_d(fastK),
+// slowD = SMA_d(slowK), both from bar k-1+2(d-1). fastK of the round and of the
+// 2(d-1) bars before it goes to scratch line 0, then each bar averages it.
+template <int K>
+__device__ void stoch_round(const Ctx<K>& c, const Job& j) {
+  const int ph = j.in[0], plo = j.in[1], pc = j.in[2];
+  const int p = j.ip[0], q = j.ip[1];
+  const long long lb = (long long)p - 1 + 2ll * (q - 1);
+  const int ext = 2 * (q - 1);
+  auto fastk = [&](long long t) -> double {
+    if (t < p - 1) return 0.0;
+    double lo = c.x(plo, t - p + 1), hi = c.x(ph, t - p + 1);
+    for (int i = 1; i < p; ++i) {
+      const double l = c.x(plo, t - p + 1 + i), h = c.x(ph, t - p + 1 + i);
+      if (l < lo) lo = l;
+      if (h > hi) hi = h;
+    }
+    const double range = hi - lo;
+    return fabs(range) <= 1e-14 * (fabs(hi) + fabs(lo)) ? 0.0 : ((double)c.x(pc, t) - lo) / range * 100.0;
+  };
+  const long long g0 = c.gb0();
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    c.line(0, k) = fastk(t);
+  }
+  for (int i = c.lane; i < ext; i += 32) c.eline(0, i - ext) = fastk(c.t0 - ext + i);
+  __syncwarp();
+  const double invq = 1.0 / (double)q;
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    float o0 = qnan(), o1 = qnan();
+    if (t >= lb) {
+      const int r = (int)(t - c.t0);
+      double dsum = 0.0, k0 = 0.0;
+      for (int i = 0; i < q; ++i) {
+        double s = 0.0;
+        for (int m = q - 1; m >= 0; --m) s += c.eline(0, r - i - m);
+        const double kv = s * invq;
+        if (i == 0) k0 = kv;
+        dsum += kv;
+      }
+      o0 = (float)k0;
+      o1 = (float)(dsum * invq);
+    }
+    c.put(0, k, o0);
+    c.put(1, k, o1);
+  }
+  c.flush(0, (float*)j.out[0]);
+  c.flush(1, (float*)j.out[1]);
+}
+
+// CCI(p): src/indicators/CCI.cu:11-40: typical price ((h+l)+c)/3 in FP64, its
+// window mean and mean absolute deviation; (tp - sma)/(0.015*md), 0 unless both
+// the numerator and md are nonzero.
+template <int K>
+__device__ void cci_round(const Ctx<K>& c, const Job& j) {
+  const int p = j.ip[0];
+  const long long g0 = c.gb0();
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    float o = qnan();
+    if (t >= p - 1) {
+      double sum = 0.0;
+      for (int i = 0; i < p; ++i) sum += c.typ(t - i);
+      const double sma = sum / p;
+      double dev = 0.0;
+      for (int i = 0; i < p; ++i) dev += fabs(c.typ(t - i) - sma);
+      const double md = dev / p;
+      const double num = c.typ(t) - sma;
+      o = (num != 0.0 && md != 0.0) ? (float)(num / (0.015 * md)) : 0.0f;
+    }
+    c.put(0, k, o);
+  }
+  c.flush(0, (float*)j.out[0]);
+}
+
+// MFI(p): StreamStates.h:749-792 precise::MfiState: money flow tp*v signed by
+// the typical price change (non-finite prices give no flow), positive and
+// negative sums over the last p flows, 100*pos/(pos+neg), 0 when the total is
+// below 1; output from bar p.
+template <int K>
+__device__ void mfi_round(const Ctx<K>& c, const Job& j) {
+  const int pv = j.in[3], p = j.ip[0];
+  const long long g0 = c.gb0();
+  auto flow = [&](long long t, double& pos, double& neg) {
+    pos = neg = 0.0;
+    if (t < 1) return;
+    const double pr = c.typ(t), pp = c.typ(t - 1);
+    if (isfinite(pr) && isfinite(pp)) {
+      const double fl = pr * (double)c.x(pv, t);
+      if (pr > pp) pos = fl;
+      else if (pr < pp) neg = fl;
+    }
+  };
+  const long long tf = g0 > p ? g0 : (long long)p;
+  double ps = 0.0, ns = 0.0;
+  if (tf < g0 + K && c.valid(tf)) {
+    for (int i = p - 1; i >= 0; --i) {
+      double a, b;
+      flow(tf - i, a, b);
+      ps += a; ns += b;
+    }
+  }
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    float o = qnan();
+    if (t >= tf) {
+      if (t > tf) {
+        double a, b;
+        flow(t - p, a, b);
+        ps -= a; ns -= b;
+        flow(t, a, b);
+        ps += a; ns += b;
+        if (ps < 0.0 || ns < 0.0) {  // re-sum a window that cancelled below zero
+          ps = ns = 0.0;
+          for (int i = p - 1; i >= 0; --i) { flow(t - i, a, b); ps += a; ns += b; }
+        }
+      }
+      const double tot = ps + ns;
+      o = tot < 1.0 ? 0.0f : (float)(100.0 * (ps / tot));
+    }
+    c.put(0, k, o);
+  }
+  c.flush(0, (float*)j.out[0]);
+}
+
+// CORREL(p): src/indicators/Correl.cu:23-75: Pearson correlation of the window
+// from FP64 moments about a lane-local origin; 0 when either variance or their
+// product (<= 1e-14) vanishes; 0 from the first non-finite bar of the row on
+// (findInvalidSuffix, Correl.cu:14-21). Carry.f holds that first bar (-1 none).
+template <int K>
+__device__ void correl_round(const Ctx<K>& c, const Job& j, Carry& cy) {
+  const int px = j.in[0], py = j.in[1], p = j.ip[0];
+  const long long g0 = c.gb0();
+  long long bad = cy.f;
+  if (bad < 0) {
+    long long first = 0x7fffffffffffffffll;
+    for (int k = 0; k < K; ++k) {
+      const long long t = g0 + k;
+      if (!c.valid(t)) break;
+      if (!isfinite(c.x(px, t)) || !isfinite(c.x(py, t))) { first = t; break; }
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) first = min(first, __shfl_xor_sync(kFull, first, d));
+    bad = first == 0x7fffffffffffffffll ? -1 : first;
+  }
+  const long long tf = g0 > p - 1 ? g0 : (long long)(p - 1);
+  double sx = 0, sy = 0, sxx = 0, syy = 0, sxy = 0, ox = 0, oy = 0;
+  if (tf < g0 + K && c.valid(tf)) {
+    ox = c.x(px, tf - p + 1);
+    oy = c.x(py, tf - p + 1);
+    if (!isfinite(ox)) ox = 0.0;
+    if (!isfinite(oy)) oy = 0.0;
+    for (int i = 0; i < p; ++i) {
+      const double dx = (double)c.x(px, tf - p + 1 + i) - ox, dy = (double)c.x(py, tf - p + 1 + i) - oy;
+      sx += dx; sy += dy; sxx += dx * dx; syy += dy * dy; sxy += dx * dy;
+    }
+  }
+  const double pp = (double)p;
+  for (int k = 0; k < K; ++k) {
+    const long long t = g0 + k;
+    if (!c.valid(t)) break;
+    float o = qnan();
+    if (t >= tf) {
+      if (t > tf) {
+        const double ax = (double)c.x(px, t - p) - ox, ay = (double)c.x(py, t - p) - oy;
+        const double bx = (double)c.x(px, t) - ox, by = (double)c.x(py, t) - oy;
+        sx += bx - ax; sy += by - ay;
+        sxx += bx * bx - ax * ax; syy += by * by - ay * ay; sxy += bx * by - ax * ay;
+      }
+      if (bad >= 0 && t >= bad) o = 0.0f;
+      else {
+        const double cov = sxy - sx * sy / pp;
+        const double vx = sxx - sx * sx / pp, vy = syy - sy * sy / pp;
+        const double prod = vx * vy;
+        o = (vx > 0.0 && vy > 0.0 && prod > 1e-14) ? (float)(cov / sqrt(prod)) : 0.0f;
+      }
+    }
+    c.put(0, k, o);
+  }
+  cy.f = bad;
+  c.flush(0, (float*)j.out[0]);
+}
+
+}  // namespace tb

@@ -1,0 +1,41 @@
+// Launch planning for the batch engine: bars per lane (K), warps per block and
+// grid size, chosen per batch shape and job set. Plans come from a built-in
+// heuristic or from the measured autotuner cache (see scheduler.cpp).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "engine.h"
+
+namespace tb {
+
+struct SchedulePlan {
+  int k = 8;               // bars per lane; a round covers 32*k bars
+  int warps_per_block = 8;
+  int max_blocks = 0;      // 0 = as many as fit
+};
+
+struct LaunchStats {
+  int blocks = 0, warps_per_block = 0, smem_per_block = 0, k = 0, blocks_per_sm = 0;
+};
+
+// Shape summary used as the autotuner key.
+struct ShapeKey {
+  int S_bucket;     // log2 of series count
+  int T_bucket;     // log2 of mean length
+  int Tmax_bucket;  // log2 of max length
+  uint64_t jobs;    // hash of the job families and periods
+  bool operator==(const ShapeKey& o) const {
+    return S_bucket == o.S_bucket && T_bucket == o.T_bucket && Tmax_bucket == o.Tmax_bucket && jobs == o.jobs;
+  }
+};
+
+ShapeKey shape_key(const Launch& L, long long total_bars, long long max_len);
+SchedulePlan plan_for(const Launch& L, long long total_bars, long long max_len);
+void remember_plan(const ShapeKey& key, const SchedulePlan& plan);
+
+cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, cudaStream_t stream, LaunchStats* stats);
+int max_lookback_halo(const Launch& L);
+
+}  // namespace tb

@@ -1,0 +1,80 @@
+"""Helpers for the GPU tests: calling the reference-named C entry points with
+torch device buffers."""
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+import torch
+
+import tacuda_b200 as tb
+
+HLC = ["high", "low", "close"]
+HLCV = ["high", "low", "close", "volume"]
+# name: (C symbol, input planes, outputs, scalars (type, oracle param name or constant))
+SPECS = {
+    "sma": ("ct_sma_batch_d", ["close"], 1, [("i", "period")]),
+    "ema": ("ct_ema_batch_d", ["close"], 1, [("i", "period")]),
+    "wma": ("ct_wma_batch_d", ["close"], 1, [("i", "period")]),
+    "rsi": ("ct_rsi_batch_d", ["close"], 1, [("i", "period")]),
+    "dema": ("ct_dema_batch_d", ["close"], 1, [("i", "period")]),
+    "tema": ("ct_tema_batch_d", ["close"], 1, [("i", "period")]),
+    "t3": ("ct_t3_batch_d", ["close"], 1, [("i", "period"), ("f", "vfactor")]),
+    "stddev": ("ct_stddev_batch_d", ["close"], 1, [("i", "period")]),
+    "var": ("ct_var_batch_d", ["close"], 1, [("i", "period")]),
+    "sum": ("ct_sum_batch_d", ["close"], 1, [("i", "period")]),
+    "max": ("ct_max_batch_d", ["close"], 1, [("i", "period")]),
+    "min": ("ct_min_batch_d", ["close"], 1, [("i", "period")]),
+    "linearreg": ("ct_linearreg_batch_d", ["close"], 1, [("i", "period")]),
+    "atr": ("ct_atr_batch_d", HLC, 1, [("i", "period"), ("f", 0.0)]),
+    "natr": ("ct_natr_batch_d", HLC, 1, [("i", "period")]),
+    "trange": ("ct_trange_batch_d", HLC, 1, []),
+    "adx": ("ct_adx_batch_d", HLC, 1, [("i", "period")]),
+    "dx": ("ct_dx_batch_d", HLC, 1, [("i", "period")]),
+    "willr": ("ct_willr_batch_d", HLC, 1, [("i", "period")]),
+    "cci": ("ct_cci_batch_d", HLC, 1, [("i", "period")]),
+    "macd": ("ct_macd_batch_d", ["close"], 3, [("i", "fast"), ("i", "slow"), ("i", "signal"), ("i", 1)]),
+    "bbands": ("ct_bbands_batch_d", ["close"], 3, [("i", "period"), ("f", "up"), ("f", "dn")]),
+    "stoch": ("ct_stochastic_batch_d", HLC, 2, [("i", "k"), ("i", "d")]),
+    "obv": ("ct_obv_batch_d", ["close", "volume"], 1, []),
+    "mfi": ("ct_mfi_batch_d", HLCV, 1, [("i", "period")]),
+    "ad": ("ct_ad_batch_d", HLCV, 1, []),
+    "adosc": ("ct_adosc_batch_d", HLCV, 1, [("i", "fast"), ("i", "slow")]),
+    "correl": ("ct_correl_batch_d", ["x", "y"], 1, [("i", "period")]),
+}
+
+DEFAULTS = {
+    "sma": dict(period=20), "ema": dict(period=14), "wma": dict(period=14), "rsi": dict(period=14),
+    "dema": dict(period=10), "tema": dict(period=8), "t3": dict(period=5, vfactor=0.7),
+    "stddev": dict(period=20, nbdev=1.0), "var": dict(period=20), "sum": dict(period=20), "max": dict(period=20),
+    "min": dict(period=20), "linearreg": dict(period=14), "atr": dict(period=14), "natr": dict(period=14),
+    "trange": {}, "adx": dict(period=14), "dx": dict(period=14), "willr": dict(period=14), "cci": dict(period=14),
+    "macd": dict(fast=12, slow=26, signal=9), "bbands": dict(period=20, up=2.0, dn=2.0), "stoch": dict(k=14, d=3),
+    "obv": {}, "mfi": dict(period=14), "ad": {}, "adosc": dict(fast=3, slow=10), "correl": dict(period=30),
+}
+
+
+def device_planes(data: dict, dev="cuda") -> dict:
+    return {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in data.items()}
+
+
+def call_batch_d(name: str, dplanes: dict, params: dict, stream=0, outs=None):
+    """Run ct_<name>_batch_d; returns the list of output tensors."""
+    sym, ins, nout, scal = SPECS[name]
+    S, T = dplanes[ins[0]].shape
+    if outs is None:
+        outs = [torch.full((S, T), 12345.0, device=dplanes[ins[0]].device) for _ in range(nout)]
+    args = [ct.c_void_p(dplanes[k].data_ptr()) for k in ins] + [ct.c_void_p(o.data_ptr()) for o in outs]
+    args += [ct.c_int(T), ct.c_int(S)]
+    for typ, key in scal:
+        v = params[key] if isinstance(key, str) else key
+        args.append(ct.c_int(int(v)) if typ == "i" else ct.c_float(float(v)))
+    args += [ct.c_int(0), ct.c_void_p(stream)]
+    rc = getattr(tb.get_lib(), sym)(*args)
+    tb.call_status(rc, sym)
+    return outs
+
+
+def to_np(ts):
+    torch.cuda.synchronize()
+    return [t.cpu().numpy() for t in ts]

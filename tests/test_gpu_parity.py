@@ -1,0 +1,225 @@
+"""GPU parity: every family through its reference-named C entry point
+(ct_*_batch_d) against the FP64 oracle, over shapes that exercise single and
+multi-round rows, tiny rows and every round width; plus the fused multi-job
+launch, ragged plans and the reference's row-independence invariants."""
+import ctypes as ct
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import tacuda_b200 as tb
+from gpu_util import DEFAULTS, SPECS, call_batch_d, device_planes, to_np
+from oracle import oracle as O
+from tacuda_b200 import synthetic, workloads
+from tolerance import compare
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(1, 1), (2, 16), (17, 19), (67, 234), (3, 513), (4, 3000)]
+
+
+def oracle_data(d):
+    out = dict(d)
+    out["x"] = d["close"]
+    out["y"] = d["open"]
+    return out
+
+
+def run_case(name, params, shape, seed=6):
+    d = oracle_data(synthetic.ohlcv(*shape, seed=seed))
+    got = to_np(call_batch_d(name, device_planes(d), params))
+    ref = O.run(name, d, **params)
+    stats = []
+    for i, (g, r) in enumerate(zip(got, ref)):
+        stats.append(compare(g, r, f"{name}{params}[{i}] {shape}"))
+    return stats
+
+
+@pytest.mark.parametrize("name", sorted(SPECS))
+@pytest.mark.parametrize("shape", SHAPES)
+def test_family_matches_oracle(name, shape):
+    run_case(name, DEFAULTS[name], shape)
+
+
+VARIANTS = {
+    "sma": [dict(period=1), dict(period=2), dict(period=64), dict(period=200)],
+    "ema": [dict(period=1), dict(period=2), dict(period=63), dict(period=500)],
+    "wma": [dict(period=1), dict(period=2), dict(period=64)],
+    "rsi": [dict(period=1), dict(period=2), dict(period=3), dict(period=64)],
+    "atr": [dict(period=1), dict(period=2), dict(period=64)],
+    "natr": [dict(period=1), dict(period=2), dict(period=63)],
+    "adx": [dict(period=2), dict(period=5), dict(period=30)],
+    "dx": [dict(period=1), dict(period=5)],
+    "macd": [dict(fast=26, slow=12, signal=9), dict(fast=2, slow=3, signal=2), dict(fast=5, slow=35, signal=1)],
+    "bbands": [dict(period=2, up=1.5, dn=2.5), dict(period=64, up=2.0, dn=2.0)],
+    "stoch": [dict(k=2, d=1), dict(k=5, d=5), dict(k=30, d=8)],
+    "stddev": [dict(period=2, nbdev=1.0), dict(period=200, nbdev=1.0)],
+    "var": [dict(period=2), dict(period=200)],
+    "linearreg": [dict(period=2), dict(period=200)],
+    "cci": [dict(period=2), dict(period=40)],
+    "mfi": [dict(period=2), dict(period=64)],
+    "willr": [dict(period=1), dict(period=50)],
+    "min": [dict(period=1), dict(period=33)],
+    "max": [dict(period=1), dict(period=33)],
+    "adosc": [dict(fast=10, slow=3), dict(fast=2, slow=2)],
+    "dema": [dict(period=1), dict(period=30)],
+    "tema": [dict(period=2), dict(period=20)],
+    "t3": [dict(period=1, vfactor=0.7), dict(period=8, vfactor=0.4)],
+    "correl": [dict(period=2), dict(period=100)],
+}
+
+
+@pytest.mark.parametrize("name,params", [(n, p) for n, ps in VARIANTS.items() for p in ps])
+def test_parameter_corpus(name, params):
+    run_case(name, params, (7, 1300), seed=17)
+
+
+def test_fused_pass_matches_oracle_and_single_calls():
+    S, T = 67, 700
+    d = synthetic.ohlcv(S, T, seed=8)
+    dp = device_planes(d)
+    outs = {n: torch.full((S, T), 777.0, device="cuda") for n in workloads.PASS13_OUTPUTS}
+    jobs = [tb.make_job(fam, p, fp, [outs[o].data_ptr() for o in on]) for _, fam, p, fp, on in workloads.PASS13]
+    series = tb.make_series({k: v.data_ptr() for k, v in dp.items() if k in tb.PLANE_ID}, S, T)
+    tb.fused_batch_d(series, jobs, 0)
+    torch.cuda.synchronize()
+    for _, fam, p, fp, onames in workloads.PASS13:
+        kw = workloads.ORACLE_PARAMS[fam](p, fp)
+        ref = O.run(fam, d, **kw)
+        single = to_np(call_batch_d(fam, dp, kw))
+        for name, r, s in zip(onames, ref, single):
+            g = outs[name].cpu().numpy()
+            compare(g, r, f"fused {name}")
+            np.testing.assert_array_equal(g.view(np.uint32), s.view(np.uint32), err_msg=f"fused vs single {name}")
+
+
+def test_stream_zero_and_user_stream_agree():
+    d = synthetic.ohlcv(33, 400, seed=9)
+    dp = device_planes(d)
+    a = to_np(call_batch_d("macd", dp, DEFAULTS["macd"]))
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        b = call_batch_d("macd", dp, DEFAULTS["macd"], stream=s.cuda_stream)
+    s.synchronize()
+    b = to_np(b)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x.view(np.uint32), y.view(np.uint32))
+
+
+@pytest.mark.parametrize("name", ["ema", "rsi", "macd", "atr", "adx", "bbands", "stoch", "cci", "mfi", "obv"])
+def test_row_independence(name):
+    """Rows, their order, batch size and (at a fixed round width) future bars
+    cannot change a row (tests/python/batch_fused.py:296-310)."""
+    os.environ["TACUDA_B200_BARS_PER_LANE"] = "8"
+    try:
+        S, T = 67, 234
+        d = oracle_data(synthetic.ohlcv(S, T, seed=6))
+        p = DEFAULTS[name]
+        full = to_np(call_batch_d(name, device_planes(d), p))
+        perm = np.random.default_rng(7).permutation(S)
+        shuf = to_np(call_batch_d(name, device_planes({k: v[perm] for k, v in d.items()}), p))
+        one = to_np(call_batch_d(name, device_planes({k: v[31:32] for k, v in d.items()}), p))
+        pre = to_np(call_batch_d(name, device_planes({k: np.ascontiguousarray(v[:, :117]) for k, v in d.items()}), p))
+        for a, b, c, e in zip(full, shuf, one, pre):
+            np.testing.assert_array_equal(a[perm].view(np.uint32), b.view(np.uint32))
+            np.testing.assert_array_equal(a[31:32].view(np.uint32), c.view(np.uint32))
+            np.testing.assert_array_equal(a[:, :117].view(np.uint32), e.view(np.uint32))
+        for at in (0, 110, 233):
+            bad = {k: v.copy() for k, v in d.items()}
+            for v in bad.values():
+                v[0, at] = np.nan
+            poisoned = to_np(call_batch_d(name, device_planes(bad), p))
+            for a, b in zip(full, poisoned):
+                np.testing.assert_array_equal(a[1:].view(np.uint32), b[1:].view(np.uint32))
+    finally:
+        del os.environ["TACUDA_B200_BARS_PER_LANE"]
+
+
+def test_known_answers_on_gpu():
+    flat = {k: np.full((3, 129), 100.0 if k != "volume" else 1000.0, np.float32)
+            for k in ("open", "high", "low", "close", "volume")}
+    dp = device_planes(flat)
+    for name in ("sma", "ema", "rsi", "macd", "bbands", "cci", "willr", "adx", "stoch", "mfi", "atr"):
+        got = to_np(call_batch_d(name, dp, DEFAULTS[name]))
+        ref = O.run(name, flat, **DEFAULTS[name])
+        for g, r in zip(got, ref):
+            np.testing.assert_array_equal(np.isnan(g), np.isnan(r))
+            np.testing.assert_array_equal(g[~np.isnan(g)], r[~np.isnan(r)].astype(np.float32), err_msg=name)
+    x = np.array([[1e30, 1.0, -1e30, 1.0, np.nan, 2.0]], np.float32)
+    out = to_np(call_batch_d("ema", device_planes({"close": x}), dict(period=1)))[0]
+    np.testing.assert_array_equal(out.view(np.uint32), x.view(np.uint32))
+    x = np.arange(1.0, 40.0, dtype=np.float32)[None, :]
+    m, s, h = to_np(call_batch_d("macd", device_planes({"close": x}), dict(fast=2, slow=3, signal=1)))
+    assert np.all(np.isnan(m[:, :2])) and np.all(m[:, 2:] == 0.5) and np.all(s[:, 2:] == 0.5) and np.all(h[:, 2:] == 0)
+    c = np.array([[1, 2, 1, 2, 1]], np.float32)
+    sv = {"close": c, "high": c + 1, "low": c - 1, "volume": np.array([[10, -1, 10, -1, 10]], np.float32)}
+    out = to_np(call_batch_d("mfi", device_planes(sv), dict(period=2)))[0]
+    np.testing.assert_array_equal(out[:, 2:], -25.0)
+
+
+def test_leading_nan_and_interior_nan_semantics():
+    d = synthetic.ohlcv(5, 600, seed=12)
+    for v in d.values():
+        v[1, :37] = np.nan
+        v[2, 300] = np.nan
+    d = oracle_data(d)
+    dp = device_planes(d)
+    for name in ("ema", "rsi", "macd", "sma", "bbands", "willr", "min", "max", "dema"):
+        got = to_np(call_batch_d(name, dp, DEFAULTS[name]))
+        ref = O.run(name, d, **DEFAULTS[name])
+        for i, (g, r) in enumerate(zip(got, ref)):
+            compare(g, r, f"nan {name}[{i}]")
+
+
+def test_ragged_plan_matches_oracle():
+    lengths = synthetic.ragged_lengths(300, 1, 5000, seed=3)
+    lengths[:5] = [0, 1, 2, 1024, 4097]
+    planes, off = synthetic.ragged_ohlcv(lengths, seed=4)
+    dp = {k: torch.from_numpy(v).to("cuda") for k, v in planes.items()}
+    doff = torch.from_numpy(off).to("cuda")
+    N = int(off[-1])
+    outs = {n: torch.full((N,), 777.0, device="cuda") for n in workloads.PASS13_OUTPUTS}
+    jobs = [tb.make_job(fam, p, fp, [outs[o].data_ptr() for o in on]) for _, fam, p, fp, on in workloads.PASS13]
+    plan = tb.Plan(jobs, len(lengths), 0, off)
+    series = tb.make_series({k: v.data_ptr() for k, v in dp.items()}, len(lengths), 0, doff.data_ptr())
+    plan.execute(series, jobs, 0)
+    torch.cuda.synchronize()
+    for _, fam, p, fp, onames in workloads.PASS13:
+        ref = O.run(fam, planes, offsets=off, **workloads.ORACLE_PARAMS[fam](p, fp))
+        for name, r in zip(onames, ref):
+            g = outs[name].cpu().numpy()
+            for s in range(len(lengths)):
+                a, b = off[s], off[s + 1]
+                if b > a:
+                    compare(g[a:b], r[a:b], f"ragged {name} row {s} len {b - a}")
+    plan.close()
+
+
+def test_graph_capture_replay_equals_eager():
+    S, T = 67, 234
+    d = synthetic.ohlcv(S, T, seed=6)
+    dp = device_planes(d)
+    outs = {n: torch.empty((S, T), device="cuda") for n in workloads.PASS13_OUTPUTS}
+    jobs = [tb.make_job(fam, p, fp, [outs[o].data_ptr() for o in on]) for _, fam, p, fp, on in workloads.PASS13]
+    series = tb.make_series({k: v.data_ptr() for k, v in dp.items()}, S, T)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        tb.fused_batch_d(series, jobs, s.cuda_stream)
+    s.synchronize()
+    eager = {k: v.clone() for k, v in outs.items()}
+    g = torch.cuda.CUDAGraph()
+    n0 = tb.launch_count()
+    with torch.cuda.graph(g, stream=s):
+        tb.fused_batch_d(series, jobs, torch.cuda.current_stream().cuda_stream)
+    assert tb.launch_count() - n0 == 1
+    for _ in range(3):
+        for v in outs.values():
+            v.fill_(float("nan"))
+            v.view(torch.int32).fill_(0x5A5A5A5A)
+        g.replay()
+        torch.cuda.synchronize()
+        for k in outs:
+            assert torch.equal(outs[k].view(torch.int32), eager[k].view(torch.int32)), k
+    del g

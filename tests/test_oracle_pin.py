@@ -1,0 +1,151 @@
+"""CPU: the project's FP64 oracle against the reference's own CPU code.
+
+Pins oracle/ta_oracle.c and oracle/oracle_candles.c against (a) the committed
+golden fixtures generated from the reference build (tests/golden), and (b) the
+reference build itself (oracle/_ref) on fresh seeded data when it is present.
+Families without reference CPU code (ADX, DX, CCI, WILLR, CORREL, SUM, MIN,
+MAX) are pinned by known-answer tests.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tacuda_b200 import synthetic
+from tolerance import compare
+
+GOLD = np.load(Path(__file__).with_name("golden") / "golden_ref.npz")
+CASES = {
+    "sma": dict(period=20), "ema": dict(period=14), "wma": dict(period=14), "rsi": dict(period=14),
+    "stddev": dict(period=20, nbdev=1.0), "var": dict(period=20), "linearreg": dict(period=14),
+    "dema": dict(period=10), "tema": dict(period=8), "t3": dict(period=5, vfactor=0.7),
+    "macd": dict(fast=12, slow=26, signal=9), "bbands": dict(period=20, up=2.0, dn=2.0),
+    "atr": dict(period=14), "trange": {}, "stoch": dict(k=14, d=3), "obv": {}, "ad": {},
+    "mfi": dict(period=14), "adosc": dict(fast=3, slow=10), "natr": dict(period=14),
+}
+
+
+def gold_inputs():
+    return {k[3:]: GOLD[k] for k in GOLD.files if k.startswith("in_")}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_matches_golden(name):
+    d = gold_inputs()
+    res = O.run(name, d, **CASES[name])
+    for i, r in enumerate(res):
+        ref = GOLD[f"{name}_{i}"]
+        # float32-rounded reference states (OBV/AD/ADOSC/MFI/NATR) compare at float precision
+        compare(r, ref, f"{name}[{i}]", rtol=1e-6, row_atol=1e-9 if ref.dtype == np.float64 else 1e-7)
+
+
+def test_oracle_candles_match_golden():
+    d = gold_inputs()
+    for k in range(63):
+        got = O.cdl(k, d["open"], d["high"], d["low"], d["close"])
+        np.testing.assert_array_equal(got, GOLD[f"cdl_{k}"], err_msg=f"candle {k}")
+
+
+def test_golden_fixture_has_signals():
+    total = sum(int(np.count_nonzero(GOLD[f"cdl_{k}"])) for k in range(63))
+    assert total > 500
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference CPU build not present")
+@pytest.mark.parametrize("shape,seed", [((32, 257), 1), ((3, 1200), 2), ((17, 19), 3)])
+def test_oracle_matches_reference_build(shape, seed):
+    d = synthetic.ohlcv(*shape, seed=seed)
+    for name, p in CASES.items():
+        a = O.run(name, d, **p)
+        b = O.ref_run(name, d, **p)
+        for i, (x, y) in enumerate(zip(a, b)):
+            compare(x, y, f"{name}[{i}] {shape}", rtol=1e-6, row_atol=1e-9 if np.asarray(y).dtype == np.float64 else 1e-7)
+    for k in range(63):
+        np.testing.assert_array_equal(O.cdl(k, d["open"], d["high"], d["low"], d["close"]),
+                                      O.ref_cdl(k, d["open"], d["high"], d["low"], d["close"]), err_msg=f"candle {k}")
+
+
+# ---- known answers (tests/cpp/test_edge_cases.cpp, tests/python/batch_fused.py) ----
+
+def flat(T=129, value=100.0):
+    return {k: np.full((3, T), value if k != "volume" else 1000.0, np.float32)
+            for k in ("open", "high", "low", "close", "volume")}
+
+
+def test_flat_series_known_answers():
+    d = flat()
+    assert np.allclose(O.run("sma", d, period=20)[0][:, 19:], 100.0)
+    assert np.allclose(O.run("ema", d, period=14)[0][:, 13:], 100.0)
+    assert np.allclose(O.run("rsi", d, period=14)[0][:, 14:], 50.0)
+    m, s, h = O.run("macd", d, fast=12, slow=26, signal=9)
+    assert np.all(m[:, 33:] == 0.0) and np.all(h[:, 33:] == 0.0)
+    assert np.all(O.run("cci", d, period=14)[0][:, 13:] == 0.0)
+    assert np.all(O.run("willr", d, period=14)[0][:, 13:] == 0.0)
+    assert np.all(O.run("adx", d, period=14)[0][:, 27:] == 0.0)
+    assert np.all(np.isnan(O.run("adx", d, period=14)[0][:, :27]))
+    assert np.all(O.run("correl", {"x": d["close"], "y": d["close"]}, period=10)[0][:, 9:] == 0.0)
+
+
+def test_atr_constant_range_is_range():
+    # H - L = 10 everywhere, closes inside: ATR = 10 (test_edge_cases.cpp:162-183)
+    T = 60
+    c = np.full((1, T), 100.0, np.float32)
+    d = {"high": c + 5, "low": c - 5, "close": c}
+    out = O.run("atr", d, period=14)[0]
+    assert np.allclose(out[:, 14:], 10.0) and np.all(np.isnan(out[:, :14]))
+
+
+def test_ema_period_one_passthrough():
+    x = np.array([[1e30, 1.0, -1e30, 1.0, np.nan, 2.0]], np.float32)
+    out = O.run("ema", {"close": x}, period=1)[0]
+    np.testing.assert_array_equal(out.astype(np.float32), x)
+
+
+def test_macd_2_3_1_constants():
+    x = np.arange(1.0, 40.0, dtype=np.float32)[None, :]
+    m, s, h = O.run("macd", {"close": x}, fast=2, slow=3, signal=1)
+    assert np.all(np.isnan(m[:, :2]))
+    assert np.all(m[:, 2:] == 0.5) and np.all(s[:, 2:] == 0.5) and np.all(h[:, 2:] == 0.0)
+
+
+def test_mfi_signed_volume():
+    c = np.array([[1, 2, 1, 2, 1]], np.float32)
+    d = {"close": c, "high": c + 1, "low": c - 1, "volume": np.array([[10, -1, 10, -1, 10]], np.float32)}
+    out = O.run("mfi", d, period=2)[0]
+    np.testing.assert_array_equal(out[:, 2:], -25.0)
+
+
+def test_minmax_and_sum_windows():
+    x = np.array([[3, 1, 4, 1, 5, 9, 2, 6]], np.float32)
+    np.testing.assert_array_equal(O.run("max", {"close": x}, period=3)[0][0, 2:], [4, 4, 5, 9, 9, 9])
+    np.testing.assert_array_equal(O.run("min", {"close": x}, period=3)[0][0, 2:], [1, 1, 1, 1, 2, 2])
+    np.testing.assert_array_equal(O.run("sum", {"close": x}, period=3)[0][0, 2:], [8, 6, 10, 15, 16, 17])
+
+
+def test_willr_clamp_and_range():
+    d = synthetic.ohlcv(8, 200, seed=4)
+    w = O.run("willr", d, period=14)[0][:, 13:]
+    assert np.all((w <= 0) & (w >= -100))
+
+
+def test_window_nan_only_poisons_its_windows():
+    x = (100 + np.cumsum(np.random.default_rng(0).normal(0, 1, 80))).astype(np.float32)[None, :]
+    y = x.copy()
+    y[0, 40] = np.nan
+    a = O.run("sma", {"close": x}, period=5)[0]
+    b = O.run("sma", {"close": y}, period=5)[0]
+    assert np.all(np.isnan(b[0, 40:45]))
+    np.testing.assert_array_equal(a[0, 45:], b[0, 45:])
+    np.testing.assert_array_equal(a[0, :40], b[0, :40])
+
+
+def test_leading_nan_delays_recurrences():
+    x = (100 + np.cumsum(np.random.default_rng(1).normal(0, 1, 60))).astype(np.float32)
+    y = np.concatenate([np.full(7, np.nan, np.float32), x])[None, :]
+    for name, p in (("ema", dict(period=10)), ("rsi", dict(period=10)), ("macd", dict(fast=3, slow=6, signal=4))):
+        a = O.run(name, {"close": x[None, :]}, **p)
+        b = O.run(name, {"close": y}, **p)
+        for u, v in zip(a, b):
+            assert np.all(np.isnan(v[0, :7]))
+            np.testing.assert_array_equal(u[0], v[0, 7:])
