@@ -72,14 +72,17 @@ static void row_sum(RowCtx* r) {
   }
 }
 
-/* BatchFused.cu:110-119 MIN/MAX: float extrema (fminf/fmaxf ignore NaN). */
+/* BatchFused.cu:110-119 MIN/MAX: float extrema (fminf/fmaxf ignore NaN); a
+ * window starting inside the row's leading NaN run stays NaN
+ * (LeadingNaN.cuh:21-27 in_leading_nan_prefix). */
 static void row_minmax(RowCtx* r, int is_max) {
   const float* x = r->in[0]; int n = r->n, p = r->ip[0]; double* o = r->out[0];
   fill_nan(o, n);
+  const int f = leading_nan(x, n);
   for (int t = p - 1; t < n; ++t) {
     float v = x[t - p + 1];
     for (int k = t - p + 2; k <= t; ++k) v = is_max ? fmaxf(v, x[k]) : fminf(v, x[k]);
-    o[t] = (double)v;
+    o[t] = (t - p + 1 < f) ? kNaN : (double)v;
   }
 }
 
@@ -147,11 +150,42 @@ static double* to_double(const float* x, int n) {
   return d;
 }
 
+/* Apply a TA-Lib window routine to every maximal NaN-free run of the row, so a
+ * NaN only affects the windows containing it (the reference's batch contract;
+ * TA-Lib's running totals would carry it forward). Outputs start NaN. */
+typedef void (*SegFn)(const double* x, int n, int p, double* const* o, const double* fp);
+
+static void by_segments(const float* xf, int n, int p, double* const* outs, int nout, const double* fp, SegFn fn) {
+  for (int j = 0; j < nout; ++j) fill_nan(outs[j], n);
+  double* x = to_double(xf, n);
+  double* tmp[3];
+  for (int j = 0; j < nout; ++j) tmp[j] = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+  int i = 0;
+  while (i < n) {
+    while (i < n && isnan(x[i])) ++i;
+    int e = i;
+    while (e < n && !isnan(x[e])) ++e;
+    if (e - i >= p) {
+      double* o[3] = {tmp[0], nout > 1 ? tmp[1] : NULL, nout > 2 ? tmp[2] : NULL};
+      fn(x + i, e - i, p, o, fp);
+      for (int j = 0; j < nout; ++j)
+        for (int t = i + p - 1; t < e; ++t) outs[j][t] = tmp[j][t - i];
+    }
+    i = e;
+  }
+  for (int j = 0; j < nout; ++j) free(tmp[j]);
+  free(x);
+}
+
+static void seg_var(const double* x, int n, int p, double* const* o, const double* fp) {
+  (void)fp;
+  var_core(x, n, p, o[0]);
+}
+
 /* talib08:18047 TA_VAR (nbdev ignored, as TA_STDDEV passes 1.0). */
 static void row_var(RowCtx* r) {
-  double* d = to_double(r->in[0], r->n);
-  var_core(d, r->n, r->ip[0], r->out[0]);
-  free(d);
+  double* outs[1] = {r->out[0]};
+  by_segments(r->in[0], r->n, r->ip[0], outs, 1, NULL, seg_var);
 }
 
 /* talib08:16046-16100 TA_STDDEV = sqrt(TA_VAR) * nbdev. */
@@ -166,13 +200,10 @@ static void row_stddev(RowCtx* r) {
 /* talib08:2068-2283 TA_BBANDS with MA type SMA: the middle band is the running
  * SMA, the deviation is the shifted-moment variance of TA_VAR's scheme with
  * 32*p reseeding; equal multipliers use add/sub, unequal ones fma. */
-static void row_bbands(RowCtx* r) {
-  const int n = r->n, p = r->ip[0];
-  const double up = r->fp[0], dn = r->fp[1];
-  double *ou = r->out[0], *om = r->out[1], *ol = r->out[2];
-  fill_nan(ou, n); fill_nan(om, n); fill_nan(ol, n);
+static void seg_bbands(const double* x, int n, int p, double* const* outs, const double* fp) {
+  const double up = fp[0], dn = fp[1];
+  double *ou = outs[0], *om = outs[1], *ol = outs[2];
   if (p > n) return;
-  double* x = to_double(r->in[0], n);
   const double inv = 1.0 / (double)p;
   int lb = p - 1, trailing = 0;
   double shift = x[trailing], ma = 0.0, v1 = 0.0, v2 = 0.0, tmp, mean, var;
@@ -222,7 +253,11 @@ static void row_bbands(RowCtx* r) {
       ol[i] = mid - sd * dn;
     }
   }
-  free(x);
+}
+
+static void row_bbands(RowCtx* r) {
+  double* outs[3] = {r->out[0], r->out[1], r->out[2]};
+  by_segments(r->in[0], r->n, r->ip[0], outs, 3, r->fp, seg_bbands);
 }
 
 /* talib08:9087-9197 TA_LINEARREG: least-squares line over the window, value at

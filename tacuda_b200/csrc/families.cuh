@@ -88,19 +88,34 @@ __device__ __forceinline__ double round_tail(const Ctx<K>& c, double v) {
 
 // ----------------------------------------------------------------- EMA core
 
+// Recurrence stages are piecewise affine: bar with count c maps the state y to
+// a(c)*y + w(c)*x + (terms independent of x). The warp scan composes these maps
+// in coordinates shifted by E(c)*o, the state the stage would hold after count
+// c if every input equalled the origin o (a level stage: E = o once seeded,
+// (r+1)*o while summing its seed). The shifted map is y' = a*y + w*(x - o), so
+// a constant series composes to exactly zero offset and every lane starts from
+// the exact level; otherwise the shift only improves the carries' rounding.
+// The lanes then replay their bars with TA-Lib's own arithmetic.
+
 // One EMA stage in TA-Lib order (talib08:5546-5627): inputs counted from
 // `start` are summed, the mean of the first p seeds the average at count
 // start+p-1, later bars apply y = fma(beta, y, k*x). Period 1 copies.
 struct EmaStage {
   int p, start;
   double beta, k, inv;
-  __device__ __forceinline__ void map(long long cnt, double x, double& a, double& b) const {
-    if (cnt < start) { a = 1.0; b = 0.0; return; }
-    if (p == 1) { a = 0.0; b = x; return; }
+  __device__ __forceinline__ void coef(long long cnt, double& a, double& w) const {
+    if (cnt < start) { a = 1.0; w = 0.0; return; }
+    if (p == 1) { a = 0.0; w = 1.0; return; }
     const long long r = cnt - start;
-    if (r < p - 1) { a = 1.0; b = x; }
-    else if (r == p - 1) { a = inv; b = x * inv; }
-    else { a = beta; b = k * x; }
+    if (r < p - 1) { a = 1.0; w = 1.0; }
+    else if (r == p - 1) { a = inv; w = inv; }
+    else { a = beta; w = k; }
+  }
+  // E(cnt) / o after the bar with count cnt
+  __device__ __forceinline__ double expect(long long cnt) const {
+    if (cnt < start) return 0.0;
+    const long long r = cnt - start;
+    return (p > 1 && r < p - 1) ? (double)(r + 1) : 1.0;
   }
   __device__ __forceinline__ double step(long long cnt, double y, double x) const {
     if (cnt < start) return y;
@@ -113,29 +128,47 @@ struct EmaStage {
   __device__ __forceinline__ bool ready(long long cnt) const { return cnt >= start + p - 1; }
 };
 
-// Scan one EMA-like stage over the round. in(t, k) gives the FP64 input of the
-// lane's k-th bar; sink(k, cnt, y) receives the state after it (cnt = -1
-// before the series starts). Returns the state after the round.
+// Scan one stage over the round. in(t, k) gives the FP64 input of the lane's
+// k-th bar; sink(k, cnt, y) receives the state after it (cnt = -1 before the
+// series starts). Returns the state after the round.
 template <int K, class Stage, class In, class Sink>
 __device__ __forceinline__ double stage_round(const Ctx<K>& c, long long f, const Stage& st,
                                               double carry, In in, Sink sink) {
-  double A = 1.0, B = 0.0;
   const long long g0 = c.gb0();
+  // origin: input of the first counted bar of the round (warp-uniform)
+  double o = 0.0;
+  if (f >= 0) {
+    const long long to = c.t0 > f ? c.t0 : f;
+    if (to < c.t0 + c.L) {
+      const int lo = (int)((to - c.t0) / K), ko = (int)((to - c.t0) % K);
+      double v = 0.0;
+      if (c.lane == lo) v = in(to, ko);
+      o = __shfl_sync(kFull, v, lo);
+      if (!isfinite(o)) o = 0.0;
+    }
+  }
+  double A = 1.0, B = 0.0;
   if (f >= 0) {
 #pragma unroll 4
     for (int k = 0; k < K; ++k) {
       const long long t = g0 + k;
       if (!c.valid(t)) break;
       if (t < f) continue;
-      double a, b;
-      st.map(t - f, in(t, k), a, b);
-      B = fma(a, B, b);
+      double a, w;
+      st.coef(t - f, a, w);
+      B = fma(a, B, w * (in(t, k) - o));
       A *= a;
     }
   }
   warp_scan_affine(A, B, c.lane);
   const double Ae = shfl_excl(A, 1.0, c.lane), Be = shfl_excl(B, 0.0, c.lane);
-  double y = fma(Ae, carry, Be);
+  double y = carry;
+  if (f >= 0) {
+    const long long cr = c.t0 - 1 - f, cl = g0 - 1 - f;
+    const double er = cr >= 0 ? st.expect(cr) * o : 0.0;
+    const double el = cl >= 0 ? st.expect(cl) * o : 0.0;
+    y = el + fma(Ae, carry - er, Be);
+  }
 #pragma unroll 4
   for (int k = 0; k < K; ++k) {
     const long long t = g0 + k;
@@ -193,8 +226,7 @@ __device__ void cascade_round(const Ctx<K>& c, const Job& j, Carry& cy, int stag
   for (int s = 0; s < stages; ++s) {
     const EmaStage st{p, s * (p - 1), beta, kk, 1.0 / p};
     const bool last = s == stages - 1;
-    // which kept line (if any) stores this stage's value
-    int keep = -1;
+    int keep = -1;  // kept line storing this stage's value
     if (stages == 2 && s == 0) keep = 1;
     if (stages == 3 && s < 2) keep = 1 + s;
     if (stages == 6 && s >= 2 && s <= 4) keep = s - 1;
@@ -215,6 +247,7 @@ __device__ void cascade_round(const Ctx<K>& c, const Job& j, Carry& cy, int stag
             c.put(0, k, o);
           }
         });
+    __syncwarp();
   }
   cy.f = f;
   c.flush(0, (float*)j.out[0]);
@@ -293,18 +326,39 @@ __device__ void rsi_round(const Ctx<K>& c, const Job& j, Carry& cy) {
 
 // ----------------------------------------------------------------- MACD
 
-// Fast/slow averages of MACD (talib08:9316-9505 TA_MACD): slow seeded with the
-// mean of the first `slow` bars, fast with the mean of the `fast` bars ending at
-// the same bar (slow-1), then fma(beta, y, k*x) each.
-struct MacdLine {
-  int fast, slow;
-  double fb, fk, sb, sk;
+// Signal line of MACD: accumulate the MACD values from `start`, seed with their
+// mean at `ready`, then fma(gb, y, gk*m); signal period 1 copies.
+struct SigStage {
+  int sig;
+  long long start, ready;
+  double gb, gk, inv;
+  __device__ __forceinline__ void coef(long long cnt, double& a, double& w) const {
+    if (cnt < start) { a = 1.0; w = 0.0; }
+    else if (cnt < ready) { a = 1.0; w = 1.0; }
+    else if (cnt == ready) { a = inv; w = inv; }
+    else if (sig == 1) { a = 0.0; w = 1.0; }
+    else { a = gb; w = gk; }
+  }
+  __device__ __forceinline__ double expect(long long cnt) const {
+    if (cnt < start) return 0.0;
+    if (cnt < ready) return (double)(cnt - start + 1);
+    return 1.0;
+  }
+  __device__ __forceinline__ double step(long long cnt, double y, double m) const {
+    if (cnt < start) return y;
+    if (cnt < ready) return y + m;
+    if (cnt == ready) return (y + m) / sig;
+    return sig == 1 ? m : fma(gb, y, gk * m);
+  }
 };
 
-// MACD(fast, slow, signal): two scans (fast/slow lines, then the signal line
-// over the FP64 MACD values: mean of the first `signal` values, then EMA).
-// Reversed periods are swapped on the host. Outputs start at slow+signal-2.
-// fp: [fb, fk, sb, sk]; the signal coefficients are derived from ip[2].
+// MACD(fast, slow, signal): talib08:9316-9505 TA_MACD. The slow average is
+// seeded with the mean of the first `slow` bars, the fast one with the mean of
+// the `fast` bars ending at the same bar (slow-1); both then fma(beta, y, k*x).
+// The signal line runs over the FP64 MACD values; outputs from slow+signal-2.
+// Reversed periods are swapped on the host; fp = [fast beta, fast k, slow
+// beta, slow k]. Leading NaNs skipped. Scratch line 0 carries the slow line,
+// then the MACD line.
 template <int K>
 __device__ void macd_round(const Ctx<K>& c, const Job& j, Carry& cy) {
   const int pl = j.in[0];
@@ -315,59 +369,12 @@ __device__ void macd_round(const Ctx<K>& c, const Job& j, Carry& cy) {
   double gb, gk;
   talib_ema_coeffs(sig, gb, gk);
   const long long start = slow - 1, ready = start + sig - 1;
-  // fast and slow lines: two independent affine channels
-  double Af = 1.0, Bf = 0.0, As = 1.0, Bs = 0.0;
-  const long long g0 = c.gb0();
-  if (f >= 0) {
-#pragma unroll 4
-    for (int k = 0; k < K; ++k) {
-      const long long t = g0 + k;
-      if (!c.valid(t)) break;
-      if (t < f) continue;
-      const double x = c.x(pl, t);
-      double a, b;
-      slowSt.map(t - f, x, a, b);
-      Bs = fma(a, Bs, b); As *= a;
-      fastSt.map(t - f, x, a, b);
-      Bf = fma(a, Bf, b); Af *= a;
-    }
-  }
-  warp_scan_affine(As, Bs, c.lane);
-  warp_scan_affine(Af, Bf, c.lane);
-  double ys = fma(shfl_excl(As, 1.0, c.lane), cy.v[1], shfl_excl(Bs, 0.0, c.lane));
-  double yf = fma(shfl_excl(Af, 1.0, c.lane), cy.v[0], shfl_excl(Bf, 0.0, c.lane));
-#pragma unroll 4
-  for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
-    if (!c.valid(t)) break;
-    double m = 0.0;
-    if (f >= 0 && t >= f) {
-      const double x = c.x(pl, t);
-      ys = slowSt.step(t - f, ys, x);
-      yf = fastSt.step(t - f, yf, x);
-      m = yf - ys;
-    }
-    c.line(0, k) = m;
-  }
-  cy.v[0] = round_tail(c, yf);
-  cy.v[1] = round_tail(c, ys);
-  // signal line: accumulate MACD from `start`, seed at `ready`, then EMA
-  struct SigStage {
-    int sig; long long start, ready; double gb, gk, inv;
-    __device__ __forceinline__ void map(long long cnt, double m, double& a, double& b) const {
-      if (cnt < start) { a = 1.0; b = 0.0; }
-      else if (cnt < ready) { a = 1.0; b = m; }
-      else if (cnt == ready) { a = inv; b = m * inv; }
-      else if (sig == 1) { a = 0.0; b = m; }
-      else { a = gb; b = gk * m; }
-    }
-    __device__ __forceinline__ double step(long long cnt, double y, double m) const {
-      if (cnt < start) return y;
-      if (cnt < ready) return y + m;
-      if (cnt == ready) return (y + m) / sig;
-      return sig == 1 ? m : fma(gb, y, gk * m);
-    }
-  } sst{sig, start, ready, gb, gk, 1.0 / sig};
+  auto px = [&](long long t, int) { return (double)c.x(pl, t); };
+  cy.v[1] = stage_round(c, f, slowSt, cy.v[1], px, [&](int k, long long, double y) { c.line(0, k) = y; });
+  cy.v[0] = stage_round(c, f, fastSt, cy.v[0], px, [&](int k, long long cnt, double y) {
+    c.line(0, k) = cnt >= start ? y - c.line(0, k) : 0.0;
+  });
+  const SigStage sst{sig, start, ready, gb, gk, 1.0 / sig};
   cy.v[2] = stage_round(
       c, f, sst, cy.v[2], [&](long long, int k) { return c.line(0, k); },
       [&](int k, long long cnt, double s) {
@@ -385,55 +392,52 @@ __device__ void macd_round(const Ctx<K>& c, const Job& j, Carry& cy) {
 
 // ----------------------------------------------------------------- ATR family
 
-// ATR(p): talib08:1931-2057 TA_ATR: mean of the true ranges of bars 1..p (first
-// output at bar p), then fma(wb, y, wa*tr) with wb = (p-1)/p, wa = 1-wb.
-// NATR (StreamStates.h:708-721): 100*ATR/close in FP64, 0 for a zero close;
-// period 1 keeps the unnormalised true range. TRANGE: true range from bar 1.
-// fp[0] = wb, fp[1] = wa. mode: 0 ATR, 1 NATR, 2 TRANGE.
+// Wilder average of the true range as TA_ATR computes it: bars 1..p are summed
+// and divided by p at bar p, later bars apply fma(wb, y, wa*tr).
+struct AtrStage {
+  int p;
+  double wb, wa, inv;
+  __device__ __forceinline__ void coef(long long t, double& a, double& w) const {
+    if (t < 1) { a = 1.0; w = 0.0; }
+    else if (t < p) { a = 1.0; w = 1.0; }
+    else if (t == p) { a = inv; w = inv; }
+    else { a = wb; w = wa; }
+  }
+  __device__ __forceinline__ double expect(long long t) const {
+    if (t < 1) return 0.0;
+    return t < p ? (double)t : 1.0;
+  }
+  __device__ __forceinline__ double step(long long t, double y, double r) const {
+    if (t < 1) return y;
+    if (t < p) return y + r;
+    if (t == p) return (y + r) / p;
+    return fma(wb, y, wa * r);
+  }
+};
+
+// ATR(p): talib08:1931-2057 TA_ATR (first output at bar p); wb = (p-1)/p and
+// wa = 1-wb in fp[0..1]. NATR (StreamStates.h:708-721): 100*ATR/close in FP64,
+// 0 for a zero close; period 1 keeps the unnormalised true range. TRANGE:
+// true range from bar 1 (talib08:17625-17690). mode: 0 ATR, 1 NATR, 2 TRANGE.
 template <int K>
 __device__ void atr_round(const Ctx<K>& c, const Job& j, Carry& cy, int mode) {
   const int ph = j.in[0], plo = j.in[1], pc = j.in[2];
-  const int p = mode == 2 ? 1 : j.ip[0];
-  const double wb = j.fp[0], wa = j.fp[1], inv = 1.0 / p;
-  auto tr = [&](long long t) {
-    return true_range((double)c.x(ph, t), (double)c.x(plo, t), (double)c.x(pc, t - 1));
+  auto tr = [&](long long t, int) {
+    return t < 1 ? 0.0 : true_range((double)c.x(ph, t), (double)c.x(plo, t), (double)c.x(pc, t - 1));
   };
   const long long g0 = c.gb0();
   if (mode == 2) {
     for (int k = 0; k < K; ++k) {
       const long long t = g0 + k;
       if (!c.valid(t)) break;
-      c.put(0, k, t >= 1 ? (float)tr(t) : qnan());
+      c.put(0, k, t >= 1 ? (float)tr(t, k) : qnan());
     }
     c.flush(0, (float*)j.out[0]);
     return;
   }
-  double A = 1.0, B = 0.0;
-#pragma unroll 4
-  for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
-    if (!c.valid(t)) break;
-    if (t == 0) continue;
-    const double r = tr(t);
-    double a, b;
-    if (t < p) { a = 1.0; b = r; }
-    else if (t == p) { a = inv; b = r * inv; }
-    else { a = wb; b = wa * r; }
-    B = fma(a, B, b);
-    A *= a;
-  }
-  warp_scan_affine(A, B, c.lane);
-  double y = fma(shfl_excl(A, 1.0, c.lane), cy.v[0], shfl_excl(B, 0.0, c.lane));
-#pragma unroll 4
-  for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
-    if (!c.valid(t)) break;
-    if (t >= 1) {
-      const double r = tr(t);
-      if (t < p) y += r;
-      else if (t == p) y = (y + r) / p;
-      else y = fma(wb, y, wa * r);
-    }
+  const int p = j.ip[0];
+  const AtrStage st{p, j.fp[0], j.fp[1], 1.0 / p};
+  cy.v[0] = stage_round(c, 0, st, cy.v[0], tr, [&](int k, long long t, double y) {
     float o = qnan();
     if (t >= p) {
       if (mode == 0 || p == 1) o = (float)y;
@@ -443,8 +447,7 @@ __device__ void atr_round(const Ctx<K>& c, const Job& j, Carry& cy, int mode) {
       }
     }
     c.put(0, k, o);
-  }
-  cy.v[0] = round_tail(c, y);
+  });
   c.flush(0, (float*)j.out[0]);
 }
 
@@ -518,11 +521,15 @@ __device__ void adx_round(const Ctx<K>& c, const Job& j, Carry& cy, bool adx) {
   if (adx) {
     struct AdxStage {
       int p; double a, inv;
-      __device__ __forceinline__ void map(long long t, double dx, double& m, double& b) const {
-        if (t < p) { m = 1.0; b = 0.0; }
-        else if (t < 2 * p - 1) { m = 1.0; b = dx; }
-        else if (t == 2 * p - 1) { m = inv; b = dx * inv; }
-        else { m = a; b = dx / p; }
+      __device__ __forceinline__ void coef(long long t, double& m, double& w) const {
+        if (t < p) { m = 1.0; w = 0.0; }
+        else if (t < 2 * p - 1) { m = 1.0; w = 1.0; }
+        else if (t == 2 * p - 1) { m = inv; w = inv; }
+        else { m = a; w = inv; }
+      }
+      __device__ __forceinline__ double expect(long long t) const {
+        if (t < p) return 0.0;
+        return t < 2 * p - 1 ? (double)(t - p + 1) : 1.0;
       }
       __device__ __forceinline__ double step(long long t, double y, double dx) const {
         if (t < p) return y;
@@ -593,9 +600,10 @@ __device__ void volume_round(const Ctx<K>& c, const Job& j, Carry& cy, int mode)
     const int warm = (fp_ > sp_ ? fp_ : sp_) - 1;
     struct Osc {
       double kk;
-      __device__ __forceinline__ void map(long long t, double ad, double& a, double& b) const {
-        if (t == 0) { a = 0.0; b = ad; } else { a = 1.0 - kk; b = kk * ad; }
+      __device__ __forceinline__ void coef(long long t, double& a, double& w) const {
+        if (t == 0) { a = 0.0; w = 1.0; } else { a = 1.0 - kk; w = kk; }
       }
+      __device__ __forceinline__ double expect(long long) const { return 1.0; }
       __device__ __forceinline__ double step(long long t, double y, double ad) const {
         return t == 0 ? ad : kk * ad + (1.0 - kk) * y;
       }
