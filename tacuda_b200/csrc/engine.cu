@@ -12,6 +12,7 @@
 #include "families.cuh"
 #include "candles.cuh"
 #include "scheduler.h"
+#include "sp_candles.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -67,26 +68,34 @@ __device__ __forceinline__ void run_job(const Ctx<K>& c, const Job& j, Carry& cy
   }
 }
 
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+
 template <int K>
 __global__ void __launch_bounds__(256) batch_kernel(const __grid_constant__ Launch L, const SmemLayout lay) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int TILE = 32 * K;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  unsigned char* mine = smem + (size_t)warp * lay.bytes_per_warp;
 
   Ctx<K> c;
   c.lane = lane;
   c.H = L.halo;
-  c.tp = L.need_tp ? reinterpret_cast<double*>(mine + lay.off_tp) : nullptr;
-  c.dscr = reinterpret_cast<double*>(mine + lay.off_dscr);
+  c.sm = smem + (size_t)warp * lay.bytes_per_warp;
+  c.off_planes = lay.off_planes;
+  c.plane_len = lay.plane_len;
+  c.off_tp = lay.off_tp;
+  c.off_dscr = lay.off_dscr;
+  c.off_stage = lay.off_stage;
+  c.stage_len = lay.stage_len;
+  c.has_tp = L.need_tp;
+  unsigned slots = 0;
   for (int p = 0; p < P_COUNT; ++p)
-    c.sp[p] = lay.plane_slot[p] >= 0
-                  ? reinterpret_cast<float*>(mine + lay.off_planes) + lay.plane_slot[p] * lay.plane_len
-                  : nullptr;
-  for (int j = 0; j < kMaxOut; ++j)
-    c.stage[j] = reinterpret_cast<float*>(mine + lay.off_stage) + j * lay.stage_len;
-  c.istage = reinterpret_cast<int*>(c.stage[0]);
-  Carry* carry = reinterpret_cast<Carry*>(mine + lay.off_carry);
+    if (lay.plane_slot[p] >= 0) slots |= (unsigned)lay.plane_slot[p] << (4 * p);
+  c.slots = slots;
+  Carry* carry = reinterpret_cast<Carry*>(c.sm + lay.off_carry);
+  float* planes = reinterpret_cast<float*>(c.sm + lay.off_planes);
 
   const int W = gridDim.x * lay.warps;
   const int gw = blockIdx.x * lay.warps + warp;
@@ -97,10 +106,10 @@ __global__ void __launch_bounds__(256) batch_kernel(const __grid_constant__ Laun
     const int s = L.order ? L.order[idx] : (int)idx;
     if (L.offsets) {
       c.base = L.offsets[s];
-      c.n = L.offsets[s + 1] - c.base;
+      c.n = (int)(L.offsets[s + 1] - c.base);
     } else {
       c.base = (long long)s * L.T;
-      c.n = L.T;
+      c.n = (int)L.T;
     }
     for (int j = 0; j < L.njobs; ++j) {
       if (lane == 0) {
@@ -109,27 +118,31 @@ __global__ void __launch_bounds__(256) batch_kernel(const __grid_constant__ Laun
       }
     }
     __syncwarp();
-    for (long long t0 = 0; t0 < c.n; t0 += TILE) {
+    for (int t0 = 0; t0 < c.n; t0 += TILE) {
       c.t0 = t0;
-      c.L = (int)min((long long)TILE, c.n - t0);
-      // stage the input planes (NaN outside the row)
-      const long long tlo = t0 - L.halo;
+      c.L = min(TILE, c.n - t0);
+      // stage the input planes with asynchronous copies, all in flight at once
+      // (bars outside the row read as 0; no family reads them for an output)
+      const int tlo = t0 - L.halo;
       for (int p = 0; p < P_COUNT; ++p) {
         if (!(L.plane_mask & (1u << p))) continue;
-        const float* __restrict__ src = L.plane[p] + c.base;
-        float* dst = c.sp[p];
+        const float* src = L.plane[p] + c.base;
+        float* dst = planes + lay.plane_slot[p] * lay.plane_len;
         for (int i = lane; i < span; i += 32) {
-          const long long t = tlo + i;
-          dst[pad(i)] = (t >= 0 && t < c.n) ? __ldg(src + t) : qnan();
+          const int t = tlo + i;
+          const bool ok = t >= 0 && t < c.n;
+          cp_async4(dst + pad(i), ok ? src + t : src, ok);
         }
       }
+      asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
       __syncwarp();
       if (L.need_tp) {
-        const float* hp = c.sp[P_HIGH];
-        const float* lp = c.sp[P_LOW];
-        const float* cp = c.sp[P_CLOSE];
+        const float* hp = c.plane(P_HIGH);
+        const float* lp = c.plane(P_LOW);
+        const float* cp = c.plane(P_CLOSE);
+        double* tpp = reinterpret_cast<double*>(c.sm + lay.off_tp);
         for (int i = lane; i < span; i += 32)
-          c.tp[i + (i >> 4)] = ((double)hp[pad(i)] + (double)lp[pad(i)] + (double)cp[pad(i)]) / 3.0;
+          tpp[i + (i >> 4)] = ((double)hp[pad(i)] + (double)lp[pad(i)] + (double)cp[pad(i)]) / 3.0;
       }
       __syncwarp();
       for (int j = 0; j < L.njobs; ++j) {
@@ -140,6 +153,95 @@ __global__ void __launch_bounds__(256) batch_kernel(const __grid_constant__ Laun
         __syncwarp();
       }
     }
+  }
+}
+
+// ------------------------------------------------------- series-parallel
+
+__device__ void sp_run_job(sp::Driver& drv, const Job& j, const sp::Stage& st, const sp::Line& ln, int lane) {
+  switch (j.family) {
+    case F_SMA: sp::sp_sum_window(drv, j, st, ln, lane, 0); break;
+    case F_SUM: sp::sp_sum_window(drv, j, st, ln, lane, 1); break;
+    case F_WMA: sp::sp_sum_window(drv, j, st, ln, lane, 2); break;
+    case F_BBANDS: sp::sp_moment_window(drv, j, st, ln, lane, 0); break;
+    case F_STDDEV: sp::sp_moment_window(drv, j, st, ln, lane, 1); break;
+    case F_VAR: sp::sp_moment_window(drv, j, st, ln, lane, 2); break;
+    case F_LINEARREG: sp::sp_linreg(drv, j, st, ln, lane); break;
+    case F_CORREL: sp::sp_correl(drv, j, st, ln, lane); break;
+    case F_MIN: sp::sp_minmax(drv, j, st, ln, lane, false); break;
+    case F_MAX: sp::sp_minmax(drv, j, st, ln, lane, true); break;
+    case F_WILLR: sp::sp_willr(drv, j, st, ln, lane); break;
+    case F_STOCH: sp::sp_stoch(drv, j, st, ln, lane); break;
+    case F_CCI: sp::sp_cci(drv, j, st, ln, lane); break;
+    case F_MFI: sp::sp_mfi(drv, j, st, ln, lane); break;
+    case F_EMA: sp::sp_ema(drv, j, st, ln, lane); break;
+    case F_DEMA: sp::sp_cascade(drv, j, st, ln, lane, 2); break;
+    case F_TEMA: sp::sp_cascade(drv, j, st, ln, lane, 3); break;
+    case F_T3: sp::sp_cascade(drv, j, st, ln, lane, 6); break;
+    case F_RSI: sp::sp_rsi(drv, j, st, ln, lane); break;
+    case F_MACD: sp::sp_macd(drv, j, st, ln, lane); break;
+    case F_ATR: sp::sp_atr(drv, j, st, ln, lane, 0); break;
+    case F_NATR: sp::sp_atr(drv, j, st, ln, lane, 1); break;
+    case F_TRANGE: sp::sp_atr(drv, j, st, ln, lane, 2); break;
+    case F_ADX: sp::sp_adx(drv, j, st, ln, lane, true); break;
+    case F_DX: sp::sp_adx(drv, j, st, ln, lane, false); break;
+    case F_OBV: sp::sp_volume(drv, j, st, ln, lane, 0); break;
+    case F_AD: sp::sp_volume(drv, j, st, ln, lane, 1); break;
+    case F_ADOSC: sp::sp_volume(drv, j, st, ln, lane, 2); break;
+    default:
+      for (int c = 0; c < drv.nchunks; ++c) { drv.begin(c); drv.end(c); }
+  }
+}
+
+__global__ void __launch_bounds__(768) sp_kernel(const __grid_constant__ Launch L, const sp::Layout lay) {
+  // Layout fields used here: warp_off/warp_tp per warp, cdl_* for candle jobs.
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int rows = lay.G * 32;
+  long long* rows_base = reinterpret_cast<long long*>(smem + 2 * (size_t)lay.in_bytes);
+  long long* rows_n = rows_base + rows;
+  int* maxlen_slot = reinterpret_cast<int*>(rows_n + rows);
+  const int group = warp / lay.J;
+  const Job& job = L.jobs[warp % lay.J];
+  sp::Stage st{reinterpret_cast<float*>(smem + lay.warp_off[warp])};
+  sp::Line ln{lay.warp_tp[warp] ? reinterpret_cast<double*>(smem + lay.warp_line[warp]) : nullptr, lay.RS, lay.H};
+  const bool is_cdl = job.family == F_CDL;
+  sp::CdlTable tbl{is_cdl ? reinterpret_cast<double*>(smem + lay.cdl_table_off + (size_t)group * lay.cdl_table_bytes)
+                          : nullptr,
+                   sp::C + sp::kCdlBack};
+  const long long ngs = ((long long)L.S + rows - 1) / rows;
+  for (long long gs = blockIdx.x; gs < ngs; gs += gridDim.x) {
+    __syncthreads();
+    if (threadIdx.x == 0) *maxlen_slot = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < rows; i += blockDim.x) {
+      const long long idx = gs * rows + i;
+      long long b = -1, n = 0;
+      if (idx < L.S) {
+        const int s = L.order ? L.order[idx] : (int)idx;
+        if (L.offsets) { b = L.offsets[s]; n = L.offsets[s + 1] - b; }
+        else { b = (long long)s * L.T; n = L.T; }
+      }
+      rows_base[i] = b;
+      rows_n[i] = n;
+      atomicMax(maxlen_slot, (int)min(n, (long long)0x7fffffff));
+    }
+    __syncthreads();
+    sp::Driver drv;
+    drv.L = &L;
+    drv.lay = &lay;
+    drv.smem = smem;
+    drv.rows_base = rows_base;
+    drv.rows_n = rows_n;
+    drv.nchunks = (*maxlen_slot + sp::C - 1) / sp::C;
+    drv.group = group;
+    drv.lane = lane;
+    drv.my_base = rows_base[group * 32 + lane];
+    drv.my_n = rows_n[group * 32 + lane];
+    if (is_cdl)
+      sp::sp_cdl_job(drv, job, st, lane, tbl, (warp % lay.J) == lay.cdl_first, 1 + group, 32 * lay.cdl_count);
+    else
+      sp_run_job(drv, job, st, ln, lane);
   }
 }
 
@@ -154,7 +256,7 @@ int job_halo(const Job& j) {
       return j.ip[0] - 1;
     case F_MFI: return j.ip[0];
     case F_STOCH: return j.ip[0] - 1 + 2 * (j.ip[1] - 1);
-    case F_CDL: return kCdlHalo;
+    case F_CDL: return 16;  // 10-bar averages anchored up to 5 bars back
     default: return 1;  // previous bar
   }
 }
@@ -225,6 +327,7 @@ struct DeviceInfo {
   int sms = 0;
   int smem_optin = 0;
   bool attr_set[3] = {false, false, false};
+  bool sp_attr = false;
   std::vector<OccEntry> occ;
 };
 
@@ -291,6 +394,91 @@ cudaError_t launch_k(Launch& L, const SchedulePlan& plan, cudaStream_t stream, L
   return cudaGetLastError();
 }
 
+cudaError_t launch_sp(Launch& L, const SchedulePlan& plan, cudaStream_t stream, LaunchStats* stats) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  DeviceInfo& di = device_info(dev);
+  const int J = L.njobs;
+  int G = plan.groups > 0 ? plan.groups : std::max(1, 8 / J);
+  while (G > 1 && G * J > 24) --G;
+  if (G * J > 24) return cudaErrorInvalidConfiguration;
+  sp::Layout lay{};
+  lay.J = J;
+  lay.H = max_lookback_halo(L);
+  lay.RS = lay.H + sp::C + 1;
+  if ((lay.RS & 1) == 0) lay.RS += 1;
+  int slots = 0;
+  for (int p = 0; p < P_COUNT; ++p) {
+    lay.plane_slot[p] = (L.plane_mask & (1u << p)) ? slots : -1;
+    if (L.plane_mask & (1u << p)) lay.slot_plane[slots++] = p;
+  }
+  lay.nplanes = slots;
+  lay.cdl_first = -1;
+  lay.cdl_count = 0;
+  for (int j = 0; j < J; ++j)
+    if (L.jobs[j].family == F_CDL) {
+      if (lay.cdl_first < 0) lay.cdl_first = j;
+      ++lay.cdl_count;
+    }
+  for (;;) {
+    lay.G = G;
+    lay.in_bytes = G * lay.nplanes * 32 * lay.RS * 4;
+    int off = 2 * lay.in_bytes + G * 32 * 16 + 16;
+    off = (off + 15) & ~15;
+    lay.cdl_table_bytes = lay.cdl_count > 0 ? 4 * 32 * (sp::C + sp::kCdlBack) * 8 : 0;
+    lay.cdl_table_off = off;
+    off += G * lay.cdl_table_bytes;
+    for (int w = 0; w < G * J; ++w) {
+      const Job& jb = L.jobs[w % J];
+      const bool line = jb.family == F_STOCH || jb.family == F_CCI || jb.family == F_MFI;
+      const int nout = jb.family == F_CDL ? 1 : (jb.family == F_MACD || jb.family == F_BBANDS ? 3 : (jb.family == F_STOCH ? 2 : 1));
+      lay.warp_off[w] = off;
+      lay.warp_tp[w] = line ? 1 : 0;
+      off += nout * 32 * (sp::C + 1) * 4;
+      off = (off + 15) & ~15;
+      lay.warp_line[w] = off;
+      if (line) off += 32 * lay.RS * 8;
+      off = (off + 15) & ~15;
+    }
+    lay.total = off;
+    if (lay.total <= di.smem_optin || G == 1) break;
+    G = std::max(1, G / 2);
+  }
+  if (lay.total > di.smem_optin) return cudaErrorInvalidConfiguration;
+  const int threads = 32 * G * J;
+  int per_sm = -1;
+  {
+    std::lock_guard<std::mutex> lk(g_mutex);
+    if (!di.sp_attr) {
+      e = cudaFuncSetAttribute(sp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, di.smem_optin);
+      if (e != cudaSuccess) return e;
+      di.sp_attr = true;
+    }
+    for (const OccEntry& o : di.occ)
+      if (o.k == -1 && o.warps == G * J && o.smem == lay.total) per_sm = o.per_sm;
+    if (per_sm < 0) {
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sp_kernel, threads, lay.total);
+      if (e != cudaSuccess) return e;
+      di.occ.push_back({-1, G * J, lay.total, per_sm});
+    }
+  }
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  const long long ngs = ((long long)L.S + 32 * G - 1) / (32 * G);
+  long long cap = (long long)per_sm * di.sms;
+  if (plan.max_blocks > 0) cap = std::min<long long>(cap, plan.max_blocks);
+  const int blocks = (int)std::max<long long>(1, std::min(ngs, cap));
+  sp_kernel<<<blocks, threads, lay.total, stream>>>(L, lay);
+  if (stats) {
+    stats->blocks = blocks;
+    stats->warps_per_block = G * J;
+    stats->smem_per_block = lay.total;
+    stats->k = 0;
+    stats->blocks_per_sm = per_sm;
+  }
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 int max_lookback_halo(const Launch& L) {
@@ -311,6 +499,7 @@ cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, cudaStream_t strea
   L.need_tp = need_tp;
   const int h = max_lookback_halo(L);
   L.halo = ((h + 31) / 32) * 32;
+  if (plan.mode == 1) return launch_sp(L, plan, stream, stats);
   switch (plan.k) {
     case 4: return launch_k<4>(L, plan, stream, stats);
     case 16: return launch_k<16>(L, plan, stream, stats);

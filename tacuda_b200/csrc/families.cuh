@@ -19,7 +19,7 @@ namespace tb {
 
 // Carry of one job between rounds of a series (kept in shared memory).
 struct Carry {
-  long long f;  // first bar that counts (after leading NaNs), -1 = not found yet
+  int f;  // first bar that counts (after leading NaNs), -1 = not found yet
   double v[10];
 };
 
@@ -29,37 +29,45 @@ struct Ctx {
   static constexpr int EXT = 64;                                 // front extension of a line
   static constexpr int LINE = (TILE + EXT) + (TILE + EXT) / 16 + 1;  // padded doubles per line
   int lane;
-  long long n;     // row length
-  long long t0;    // first bar of the round
+  int n;     // row length
+  int t0;    // first bar of the round
   int L;           // bars in the round
   int H;           // staged halo
-  long long base;  // row offset in the planes
-  float* sp[P_COUNT];
-  double* tp;      // typical price plane (padded like sp) or nullptr
-  double* dscr;    // per-warp FP64 scratch lines
-  float* stage[kMaxOut];
-  int* istage;
+  long long base;  // row offset in the planes (64-bit); bar indices within a row are int
+  // This warp's shared memory, addressed from the kernel's extern __shared__
+  // base so every access below compiles to a shared-space load or store.
+  unsigned char* sm;
+  int off_planes, plane_len, off_tp, off_dscr, off_stage, stage_len;
+  unsigned slots;  // 4-bit staged slot of each plane
+  bool has_tp;
 
-  __device__ __forceinline__ long long gb0() const { return t0 + (long long)lane * K; }
-  __device__ __forceinline__ bool valid(long long t) const { return t < t0 + L; }
-  __device__ __forceinline__ float x(int p, long long t) const { return sp[p][pad((int)(t - t0) + H)]; }
-  __device__ __forceinline__ double typ(long long t) const {
-    const int i = (int)(t - t0) + H;
-    return tp[i + (i >> 4)];
+  __device__ __forceinline__ const float* plane(int p) const {
+    return reinterpret_cast<const float*>(sm + off_planes) + (int)((slots >> (4 * p)) & 15u) * plane_len;
+  }
+  __device__ __forceinline__ int gb0() const { return t0 + lane * K; }
+  __device__ __forceinline__ bool valid(int t) const { return t < t0 + L; }
+  __device__ __forceinline__ float x(int p, int t) const { return plane(p)[pad((t - t0) + H)]; }
+  __device__ __forceinline__ double typ(int t) const {
+    const int i = (t - t0) + H;
+    return reinterpret_cast<const double*>(sm + off_tp)[i + (i >> 4)];
   }
   // Scratch line entry for round-relative bar idx in [-EXT, TILE).
   __device__ __forceinline__ double& eline(int ln, int idx) const {
     const int i = idx + EXT;
-    return dscr[ln * LINE + i + (i >> 4)];
+    return reinterpret_cast<double*>(sm + off_dscr)[ln * LINE + i + (i >> 4)];
   }
   __device__ __forceinline__ double& line(int ln, int k) const { return eline(ln, lane * K + k); }
-  __device__ __forceinline__ void put(int j, int k, float v) const { stage[j][pad(lane * K + k)] = v; }
+  __device__ __forceinline__ float* stage(int j) const {
+    return reinterpret_cast<float*>(sm + off_stage) + j * stage_len;
+  }
+  __device__ __forceinline__ void put(int j, int k, float v) const { stage(j)[pad(lane * K + k)] = v; }
 
   // Coalesced copy of staged output j to out[base + t0 .. + L).
   __device__ __forceinline__ void flush(int j, float* out) const {
     __syncwarp();
     float* dst = out + base + t0;
-    for (int i = lane; i < L; i += 32) dst[i] = stage[j][pad(i)];
+    const float* src = stage(j);
+    for (int i = lane; i < L; i += 32) dst[i] = src[pad(i)];
     __syncwarp();
   }
 };
@@ -68,16 +76,16 @@ struct Ctx {
 // of the row (src/api/BatchFused.cu:34-41 skips a leading NaN run). Resolved
 // once per series; warp-uniform. -1 while the row is all NaN so far.
 template <int K>
-__device__ __forceinline__ long long resolve_start(const Ctx<K>& c, const Carry& cy, int plane) {
+__device__ __forceinline__ int resolve_start(const Ctx<K>& c, const Carry& cy, int plane) {
   if (cy.f >= 0) return cy.f;
-  long long first = 0x7fffffffffffffffll;
+  int first = 0x7fffffff;
   for (int k = 0; k < K; ++k) {
-    const long long t = c.gb0() + k;
+    const int t = c.gb0() + k;
     if (c.valid(t) && !isnan(c.x(plane, t))) { first = t; break; }
   }
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) first = min(first, __shfl_xor_sync(kFull, first, d));
-  return first == 0x7fffffffffffffffll ? -1 : first;
+  return first == 0x7fffffff ? -1 : first;
 }
 
 // Value held after the last valid bar of the round (exact replay state).
@@ -103,79 +111,88 @@ __device__ __forceinline__ double round_tail(const Ctx<K>& c, double v) {
 struct EmaStage {
   int p, start;
   double beta, k, inv;
-  __device__ __forceinline__ void coef(long long cnt, double& a, double& w) const {
+  __device__ __forceinline__ void coef(int cnt, double& a, double& w) const {
     if (cnt < start) { a = 1.0; w = 0.0; return; }
     if (p == 1) { a = 0.0; w = 1.0; return; }
-    const long long r = cnt - start;
+    const int r = cnt - start;
     if (r < p - 1) { a = 1.0; w = 1.0; }
     else if (r == p - 1) { a = inv; w = inv; }
     else { a = beta; w = k; }
   }
   // E(cnt) / o after the bar with count cnt
-  __device__ __forceinline__ double expect(long long cnt) const {
+  __device__ __forceinline__ double expect(int cnt) const {
     if (cnt < start) return 0.0;
-    const long long r = cnt - start;
+    const int r = cnt - start;
     return (p > 1 && r < p - 1) ? (double)(r + 1) : 1.0;
   }
-  __device__ __forceinline__ double step(long long cnt, double y, double x) const {
+  __device__ __forceinline__ double step(int cnt, double y, double x) const {
     if (cnt < start) return y;
     if (p == 1) return x;
-    const long long r = cnt - start;
+    const int r = cnt - start;
     if (r < p - 1) return y + x;
     if (r == p - 1) return (y + x) / p;
     return fma(beta, y, k * x);
   }
-  __device__ __forceinline__ bool ready(long long cnt) const { return cnt >= start + p - 1; }
+  __device__ __forceinline__ bool ready(int cnt) const { return cnt >= start + p - 1; }
 };
 
 // Scan one stage over the round. in(t, k) gives the FP64 input of the lane's
 // k-th bar; sink(k, cnt, y) receives the state after it (cnt = -1 before the
 // series starts). Returns the state after the round.
 template <int K, class Stage, class In, class Sink>
-__device__ __forceinline__ double stage_round(const Ctx<K>& c, long long f, const Stage& st,
+__device__ __forceinline__ double stage_round(const Ctx<K>& c, int f, const Stage& st,
                                               double carry, In in, Sink sink) {
-  const long long g0 = c.gb0();
+  const int g0 = c.gb0();
+  // inputs of the lane's bars, evaluated once and kept in registers
+  double xin[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) xin[k] = (f >= 0 && c.valid(g0 + k) && g0 + k >= f) ? in(g0 + k, k) : 0.0;
   // origin: input of the first counted bar of the round (warp-uniform)
   double o = 0.0;
   if (f >= 0) {
-    const long long to = c.t0 > f ? c.t0 : f;
+    const int to = c.t0 > f ? c.t0 : f;
     if (to < c.t0 + c.L) {
-      const int lo = (int)((to - c.t0) / K), ko = (int)((to - c.t0) % K);
+      const int lo = (to - c.t0) / K, ko = (to - c.t0) % K;
       double v = 0.0;
-      if (c.lane == lo) v = in(to, ko);
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        if (k == ko) v = xin[k];
       o = __shfl_sync(kFull, v, lo);
       if (!isfinite(o)) o = 0.0;
     }
   }
   double A = 1.0, B = 0.0;
   if (f >= 0) {
-#pragma unroll 4
+#pragma unroll
     for (int k = 0; k < K; ++k) {
-      const long long t = g0 + k;
-      if (!c.valid(t)) break;
-      if (t < f) continue;
-      double a, w;
-      st.coef(t - f, a, w);
-      B = fma(a, B, w * (in(t, k) - o));
-      A *= a;
+      const int t = g0 + k;
+      if (c.valid(t) && t >= f) {
+        double a, w;
+        st.coef(t - f, a, w);
+        B = fma(a, B, w * (xin[k] - o));
+        A *= a;
+      }
     }
   }
   warp_scan_affine(A, B, c.lane);
   const double Ae = shfl_excl(A, 1.0, c.lane), Be = shfl_excl(B, 0.0, c.lane);
   double y = carry;
   if (f >= 0) {
-    const long long cr = c.t0 - 1 - f, cl = g0 - 1 - f;
+    const int cr = c.t0 - 1 - f, cl = g0 - 1 - f;
     const double er = cr >= 0 ? st.expect(cr) * o : 0.0;
     const double el = cl >= 0 ? st.expect(cl) * o : 0.0;
     y = el + fma(Ae, carry - er, Be);
   }
-#pragma unroll 4
+#pragma unroll
   for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
-    if (!c.valid(t)) break;
-    if (f < 0 || t < f) { sink(k, -1ll, y); continue; }
-    y = st.step(t - f, y, in(t, k));
-    sink(k, t - f, y);
+    const int t = g0 + k;
+    if (c.valid(t)) {
+      if (f < 0 || t < f) sink(k, -1, y);
+      else {
+        y = st.step(t - f, y, xin[k]);
+        sink(k, t - f, y);
+      }
+    }
   }
   return round_tail(c, y);
 }
@@ -191,13 +208,13 @@ __host__ __device__ inline void talib_ema_coeffs(int p, double& beta, double& k)
 // EMA(p): talib08:5546-5627 TA_EMA; leading NaNs skipped (BatchFused.cu:34-41).
 // fp[0] = beta, fp[1] = k (host-precomputed TA-Lib coefficients).
 template <int K>
-__device__ void ema_round(const Ctx<K>& c, const Job& j, Carry& cy) {
+__device__ __forceinline__ void ema_round(const Ctx<K>& c, const Job& j, Carry& cy) {
   const int pl = j.in[0];
-  const long long f = resolve_start(c, cy, pl);
+  const int f = resolve_start(c, cy, pl);
   const EmaStage st{j.ip[0], 0, j.fp[0], j.fp[1], 1.0 / j.ip[0]};
   cy.v[0] = stage_round(
-      c, f, st, cy.v[0], [&](long long t, int) { return (double)c.x(pl, t); },
-      [&](int k, long long cnt, double v) { c.put(0, k, (cnt >= 0 && st.ready(cnt)) ? (float)v : qnan()); });
+      c, f, st, cy.v[0], [&](int t, int) { return (double)c.x(pl, t); },
+      [&](int k, int cnt, double v) { c.put(0, k, (cnt >= 0 && st.ready(cnt)) ? (float)v : qnan()); });
   cy.f = f;
   c.flush(0, (float*)j.out[0]);
 }
@@ -209,9 +226,9 @@ __device__ void ema_round(const Ctx<K>& c, const Job& j, Carry& cy) {
 // Scratch lines: 0 = running stage value, 1.. = stage values kept for the
 // combination (DEMA: e1; TEMA: e1 e2; T3: e3 e4 e5).
 template <int K>
-__device__ void cascade_round(const Ctx<K>& c, const Job& j, Carry& cy, int stages) {
+__device__ __forceinline__ void cascade_round(const Ctx<K>& c, const Job& j, Carry& cy, int stages) {
   const int pl = j.in[0];
-  const long long f = resolve_start(c, cy, pl);
+  const int f = resolve_start(c, cy, pl);
   const int p = j.ip[0];
   const double beta = j.fp[0], kk = j.fp[1];
   double c1 = 0, c2 = 0, c3 = 0, c4 = 0;
@@ -232,8 +249,8 @@ __device__ void cascade_round(const Ctx<K>& c, const Job& j, Carry& cy, int stag
     if (stages == 6 && s >= 2 && s <= 4) keep = s - 1;
     cy.v[s] = stage_round(
         c, f, st, cy.v[s],
-        [&](long long t, int k) { return s == 0 ? (double)c.x(pl, t) : c.line(0, k); },
-        [&](int k, long long cnt, double v) {
+        [&](int t, int k) { return s == 0 ? (double)c.x(pl, t) : c.line(0, k); },
+        [&](int k, int cnt, double v) {
           c.line(0, k) = v;
           if (keep >= 0) c.line(keep, k) = v;
           if (last) {
@@ -260,49 +277,52 @@ __device__ void cascade_round(const Ctx<K>& c, const Job& j, Carry& cy, int stag
 // same multiply by 1/p; 100*g/(g+l), 50 when both are zero. A NaN change makes
 // the row NaN from there on (StreamStates.h:663). Leading NaNs skipped.
 template <int K>
-__device__ void rsi_round(const Ctx<K>& c, const Job& j, Carry& cy) {
+__device__ __forceinline__ void rsi_round(const Ctx<K>& c, const Job& j, Carry& cy) {
   const int pl = j.in[0];
-  const long long f = resolve_start(c, cy, pl);
+  const int f = resolve_start(c, cy, pl);
   const int p = j.ip[0];
   const double inv = 1.0 / (double)p, pm1 = (double)(p - 1);
   const double steady = pm1 * inv;
   double A = 1.0, B[2] = {0.0, 0.0};
-  const long long g0 = c.gb0();
-  auto change = [&](long long t, double& g, double& l) {
-    const double d = (double)c.x(pl, t) - (double)c.x(pl, t - 1);
-    if (isnan(d)) { g = l = d; return; }
-    g = d > 0.0 ? d : 0.0;
-    l = g - d;
-  };
+  const int g0 = c.gb0();
+  double gk[K], lk[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int t = g0 + k;
+    gk[k] = lk[k] = 0.0;
+    if (f >= 0 && c.valid(t) && t - f > 0) {
+      const double d = (double)c.x(pl, t) - (double)c.x(pl, t - 1);
+      if (isnan(d)) { gk[k] = lk[k] = d; }
+      else { gk[k] = d > 0.0 ? d : 0.0; lk[k] = gk[k] - d; }
+    }
+  }
   if (f >= 0) {
-#pragma unroll 4
+#pragma unroll
     for (int k = 0; k < K; ++k) {
-      const long long t = g0 + k;
-      if (!c.valid(t)) break;
-      const long long cnt = t - f;
-      if (cnt <= 0) continue;
-      double g, l, a;
-      change(t, g, l);
-      if (cnt < p) a = 1.0;
-      else if (cnt == p) { a = inv; g *= inv; l *= inv; }
-      else { a = steady; g *= inv; l *= inv; }
-      B[0] = fma(a, B[0], g);
-      B[1] = fma(a, B[1], l);
-      A *= a;
+      const int t = g0 + k;
+      const int cnt = t - f;
+      if (c.valid(t) && cnt > 0) {
+        double g = gk[k], l = lk[k], a;
+        if (cnt < p) a = 1.0;
+        else if (cnt == p) { a = inv; g *= inv; l *= inv; }
+        else { a = steady; g *= inv; l *= inv; }
+        B[0] = fma(a, B[0], g);
+        B[1] = fma(a, B[1], l);
+        A *= a;
+      }
     }
   }
   warp_scan_affine_shared<2>(A, B, c.lane);
   const double Ae = shfl_excl(A, 1.0, c.lane);
   double gain = fma(Ae, cy.v[0], shfl_excl(B[0], 0.0, c.lane));
   double loss = fma(Ae, cy.v[1], shfl_excl(B[1], 0.0, c.lane));
-#pragma unroll 4
+#pragma unroll
   for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
-    if (!c.valid(t)) break;
-    const long long cnt = f < 0 ? -1 : t - f;
+    const int t = g0 + k;
+    if (!c.valid(t)) continue;
+    const int cnt = f < 0 ? -1 : t - f;
     if (cnt > 0) {
-      double g, l;
-      change(t, g, l);
+      const double g = gk[k], l = lk[k];
       if (isnan(g)) { gain = loss = g; }
       else if (cnt < p) { gain += g; loss += l; }
       else if (cnt == p) { gain = (gain + g) * inv; loss = (loss + l) * inv; }
@@ -330,21 +350,21 @@ __device__ void rsi_round(const Ctx<K>& c, const Job& j, Carry& cy) {
 // mean at `ready`, then fma(gb, y, gk*m); signal period 1 copies.
 struct SigStage {
   int sig;
-  long long start, ready;
+  int start, ready;
   double gb, gk, inv;
-  __device__ __forceinline__ void coef(long long cnt, double& a, double& w) const {
+  __device__ __forceinline__ void coef(int cnt, double& a, double& w) const {
     if (cnt < start) { a = 1.0; w = 0.0; }
     else if (cnt < ready) { a = 1.0; w = 1.0; }
     else if (cnt == ready) { a = inv; w = inv; }
     else if (sig == 1) { a = 0.0; w = 1.0; }
     else { a = gb; w = gk; }
   }
-  __device__ __forceinline__ double expect(long long cnt) const {
+  __device__ __forceinline__ double expect(int cnt) const {
     if (cnt < start) return 0.0;
     if (cnt < ready) return (double)(cnt - start + 1);
     return 1.0;
   }
-  __device__ __forceinline__ double step(long long cnt, double y, double m) const {
+  __device__ __forceinline__ double step(int cnt, double y, double m) const {
     if (cnt < start) return y;
     if (cnt < ready) return y + m;
     if (cnt == ready) return (y + m) / sig;
@@ -360,24 +380,24 @@ struct SigStage {
 // beta, slow k]. Leading NaNs skipped. Scratch line 0 carries the slow line,
 // then the MACD line.
 template <int K>
-__device__ void macd_round(const Ctx<K>& c, const Job& j, Carry& cy) {
+__device__ __forceinline__ void macd_round(const Ctx<K>& c, const Job& j, Carry& cy) {
   const int pl = j.in[0];
-  const long long f = resolve_start(c, cy, pl);
+  const int f = resolve_start(c, cy, pl);
   const int fast = j.ip[0], slow = j.ip[1], sig = j.ip[2];
   const EmaStage slowSt{slow, 0, j.fp[2], j.fp[3], 1.0 / slow};
   const EmaStage fastSt{fast, slow - fast, j.fp[0], j.fp[1], 1.0 / fast};
   double gb, gk;
   talib_ema_coeffs(sig, gb, gk);
-  const long long start = slow - 1, ready = start + sig - 1;
-  auto px = [&](long long t, int) { return (double)c.x(pl, t); };
-  cy.v[1] = stage_round(c, f, slowSt, cy.v[1], px, [&](int k, long long, double y) { c.line(0, k) = y; });
-  cy.v[0] = stage_round(c, f, fastSt, cy.v[0], px, [&](int k, long long cnt, double y) {
+  const int start = slow - 1, ready = start + sig - 1;
+  auto px = [&](int t, int) { return (double)c.x(pl, t); };
+  cy.v[1] = stage_round(c, f, slowSt, cy.v[1], px, [&](int k, int, double y) { c.line(0, k) = y; });
+  cy.v[0] = stage_round(c, f, fastSt, cy.v[0], px, [&](int k, int cnt, double y) {
     c.line(0, k) = cnt >= start ? y - c.line(0, k) : 0.0;
   });
   const SigStage sst{sig, start, ready, gb, gk, 1.0 / sig};
   cy.v[2] = stage_round(
-      c, f, sst, cy.v[2], [&](long long, int k) { return c.line(0, k); },
-      [&](int k, long long cnt, double s) {
+      c, f, sst, cy.v[2], [&](int, int k) { return c.line(0, k); },
+      [&](int k, int cnt, double s) {
         const bool ok = cnt >= ready;
         const double m = c.line(0, k);
         c.put(0, k, ok ? (float)m : qnan());
@@ -397,17 +417,17 @@ __device__ void macd_round(const Ctx<K>& c, const Job& j, Carry& cy) {
 struct AtrStage {
   int p;
   double wb, wa, inv;
-  __device__ __forceinline__ void coef(long long t, double& a, double& w) const {
+  __device__ __forceinline__ void coef(int t, double& a, double& w) const {
     if (t < 1) { a = 1.0; w = 0.0; }
     else if (t < p) { a = 1.0; w = 1.0; }
     else if (t == p) { a = inv; w = inv; }
     else { a = wb; w = wa; }
   }
-  __device__ __forceinline__ double expect(long long t) const {
+  __device__ __forceinline__ double expect(int t) const {
     if (t < 1) return 0.0;
     return t < p ? (double)t : 1.0;
   }
-  __device__ __forceinline__ double step(long long t, double y, double r) const {
+  __device__ __forceinline__ double step(int t, double y, double r) const {
     if (t < 1) return y;
     if (t < p) return y + r;
     if (t == p) return (y + r) / p;
@@ -420,15 +440,15 @@ struct AtrStage {
 // 0 for a zero close; period 1 keeps the unnormalised true range. TRANGE:
 // true range from bar 1 (talib08:17625-17690). mode: 0 ATR, 1 NATR, 2 TRANGE.
 template <int K>
-__device__ void atr_round(const Ctx<K>& c, const Job& j, Carry& cy, int mode) {
+__device__ __forceinline__ void atr_round(const Ctx<K>& c, const Job& j, Carry& cy, int mode) {
   const int ph = j.in[0], plo = j.in[1], pc = j.in[2];
-  auto tr = [&](long long t, int) {
+  auto tr = [&](int t, int) {
     return t < 1 ? 0.0 : true_range((double)c.x(ph, t), (double)c.x(plo, t), (double)c.x(pc, t - 1));
   };
-  const long long g0 = c.gb0();
+  const int g0 = c.gb0();
   if (mode == 2) {
     for (int k = 0; k < K; ++k) {
-      const long long t = g0 + k;
+      const int t = g0 + k;
       if (!c.valid(t)) break;
       c.put(0, k, t >= 1 ? (float)tr(t, k) : qnan());
     }
@@ -437,7 +457,7 @@ __device__ void atr_round(const Ctx<K>& c, const Job& j, Carry& cy, int mode) {
   }
   const int p = j.ip[0];
   const AtrStage st{p, j.fp[0], j.fp[1], 1.0 / p};
-  cy.v[0] = stage_round(c, 0, st, cy.v[0], tr, [&](int k, long long t, double y) {
+  cy.v[0] = stage_round(c, 0, st, cy.v[0], tr, [&](int k, int t, double y) {
     float o = qnan();
     if (t >= p) {
       if (mode == 0 || p == 1) o = (float)y;
@@ -460,11 +480,11 @@ __device__ void atr_round(const Ctx<K>& c, const Job& j, Carry& cy, int mode) {
 // sum is 0); ADX is the mean of DX over bars p..2p-1, then a*ADX + DX/p.
 // The reference keeps DI/DX in float; this path keeps them in FP64.
 template <int K>
-__device__ void adx_round(const Ctx<K>& c, const Job& j, Carry& cy, bool adx) {
+__device__ __forceinline__ void adx_round(const Ctx<K>& c, const Job& j, Carry& cy, bool adx) {
   const int ph = j.in[0], plo = j.in[1], pc = j.in[2];
   const int p = j.ip[0];
   const double a = ((double)p - 1.0) / (double)p;
-  auto moves = [&](long long t, double& r, double& pl, double& mi) {
+  auto moves = [&](int t, double& r, double& pl, double& mi) {
     if (t == 0) {
       r = (double)c.x(ph, 0) - (double)c.x(plo, 0);
       pl = mi = 0.0;
@@ -476,31 +496,40 @@ __device__ void adx_round(const Ctx<K>& c, const Job& j, Carry& cy, bool adx) {
     const double hh = c.x(ph, t), ll = c.x(plo, t), yc = c.x(pc, t - 1);
     r = fmax(hh - ll, fmax(fabs(hh - yc), fabs(ll - yc)));
   };
-  const long long g0 = c.gb0();
-  double A = 1.0, B[3] = {0.0, 0.0, 0.0};
-#pragma unroll 2
+  const int g0 = c.gb0();
+  double rk[K];
+  float pk[K], mk[K];
+#pragma unroll
   for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
-    if (!c.valid(t)) break;
-    double r, pl, mi;
-    moves(t, r, pl, mi);
-    const double m = t < p ? 1.0 : a;
-    B[0] = fma(m, B[0], r);
-    B[1] = fma(m, B[1], pl);
-    B[2] = fma(m, B[2], mi);
-    A *= m;
+    rk[k] = 0.0; pk[k] = mk[k] = 0.0f;
+    if (c.valid(g0 + k)) {
+      double pl, mi;
+      moves(g0 + k, rk[k], pl, mi);
+      pk[k] = (float)pl; mk[k] = (float)mi;
+    }
+  }
+  double A = 1.0, B[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int t = g0 + k;
+    if (c.valid(t)) {
+      const double m = t < p ? 1.0 : a;
+      B[0] = fma(m, B[0], rk[k]);
+      B[1] = fma(m, B[1], (double)pk[k]);
+      B[2] = fma(m, B[2], (double)mk[k]);
+      A *= m;
+    }
   }
   warp_scan_affine_shared<3>(A, B, c.lane);
   const double Ae = shfl_excl(A, 1.0, c.lane);
   double tr = fma(Ae, cy.v[0], shfl_excl(B[0], 0.0, c.lane));
   double pd = fma(Ae, cy.v[1], shfl_excl(B[1], 0.0, c.lane));
   double md = fma(Ae, cy.v[2], shfl_excl(B[2], 0.0, c.lane));
-#pragma unroll 2
+#pragma unroll
   for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
-    if (!c.valid(t)) break;
-    double r, pl, mi;
-    moves(t, r, pl, mi);
+    const int t = g0 + k;
+    if (!c.valid(t)) continue;
+    const double r = rk[k], pl = pk[k], mi = mk[k];
     double dx = 0.0;
     if (t < p) { tr += r; pd += pl; md += mi; }
     else {
@@ -521,17 +550,17 @@ __device__ void adx_round(const Ctx<K>& c, const Job& j, Carry& cy, bool adx) {
   if (adx) {
     struct AdxStage {
       int p; double a, inv;
-      __device__ __forceinline__ void coef(long long t, double& m, double& w) const {
+      __device__ __forceinline__ void coef(int t, double& m, double& w) const {
         if (t < p) { m = 1.0; w = 0.0; }
         else if (t < 2 * p - 1) { m = 1.0; w = 1.0; }
         else if (t == 2 * p - 1) { m = inv; w = inv; }
         else { m = a; w = inv; }
       }
-      __device__ __forceinline__ double expect(long long t) const {
+      __device__ __forceinline__ double expect(int t) const {
         if (t < p) return 0.0;
         return t < 2 * p - 1 ? (double)(t - p + 1) : 1.0;
       }
-      __device__ __forceinline__ double step(long long t, double y, double dx) const {
+      __device__ __forceinline__ double step(int t, double y, double dx) const {
         if (t < p) return y;
         if (t < 2 * p - 1) return y + dx;
         if (t == 2 * p - 1) return (y + dx) / p;
@@ -539,8 +568,8 @@ __device__ void adx_round(const Ctx<K>& c, const Job& j, Carry& cy, bool adx) {
       }
     } st{p, a, 1.0 / p};
     cy.v[3] = stage_round(
-        c, 0, st, cy.v[3], [&](long long, int k) { return c.line(0, k); },
-        [&](int k, long long t, double y) { c.put(0, k, t >= 2 * p - 1 ? (float)y : qnan()); });
+        c, 0, st, cy.v[3], [&](int, int k) { return c.line(0, k); },
+        [&](int k, int t, double y) { c.put(0, k, t >= 2 * p - 1 ? (float)y : qnan()); });
   }
   c.flush(0, (float*)j.out[0]);
 }
@@ -554,9 +583,9 @@ __device__ void adx_round(const Ctx<K>& c, const Job& j, Carry& cy, bool adx) {
 // both seeded with AD[0], k = 2/(n+1), warm-up max(fast, slow)-1.
 // mode: 0 OBV (in: close, volume), 1 AD, 2 ADOSC (in: h, l, c, v).
 template <int K>
-__device__ void volume_round(const Ctx<K>& c, const Job& j, Carry& cy, int mode) {
-  const long long g0 = c.gb0();
-  auto term = [&](long long t) -> double {
+__device__ __forceinline__ void volume_round(const Ctx<K>& c, const Job& j, Carry& cy, int mode) {
+  const int g0 = c.gb0();
+  auto term = [&](int t) -> double {
     if (mode == 0) {
       const int pc = j.in[0], pv = j.in[1];
       const double v = c.x(pv, t);
@@ -572,12 +601,12 @@ __device__ void volume_round(const Ctx<K>& c, const Job& j, Carry& cy, int mode)
     }
     return 0.0;
   };
+  double tm[K];
   double B = 0.0;
-#pragma unroll 4
+#pragma unroll
   for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
-    if (!c.valid(t)) break;
-    B += term(t);
+    tm[k] = c.valid(g0 + k) ? term(g0 + k) : 0.0;
+    B += tm[k];
   }
   // prefix sum (all multipliers are 1)
 #pragma unroll
@@ -586,11 +615,10 @@ __device__ void volume_round(const Ctx<K>& c, const Job& j, Carry& cy, int mode)
     if (c.lane >= d) B += u;
   }
   double acc = cy.v[0] + shfl_excl(B, 0.0, c.lane);
-#pragma unroll 4
+#pragma unroll
   for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
-    if (!c.valid(t)) break;
-    acc += term(t);
+    if (!c.valid(g0 + k)) continue;
+    acc += tm[k];
     if (mode < 2) c.put(0, k, (float)acc);
     else c.line(0, k) = acc;
   }
@@ -600,19 +628,19 @@ __device__ void volume_round(const Ctx<K>& c, const Job& j, Carry& cy, int mode)
     const int warm = (fp_ > sp_ ? fp_ : sp_) - 1;
     struct Osc {
       double kk;
-      __device__ __forceinline__ void coef(long long t, double& a, double& w) const {
+      __device__ __forceinline__ void coef(int t, double& a, double& w) const {
         if (t == 0) { a = 0.0; w = 1.0; } else { a = 1.0 - kk; w = kk; }
       }
-      __device__ __forceinline__ double expect(long long) const { return 1.0; }
-      __device__ __forceinline__ double step(long long t, double y, double ad) const {
+      __device__ __forceinline__ double expect(int) const { return 1.0; }
+      __device__ __forceinline__ double step(int t, double y, double ad) const {
         return t == 0 ? ad : kk * ad + (1.0 - kk) * y;
       }
     };
     const Osc fs{2.0 / (fp_ + 1.0)}, ss{2.0 / (sp_ + 1.0)};
-    cy.v[1] = stage_round(c, 0, fs, cy.v[1], [&](long long, int k) { return c.line(0, k); },
-                          [&](int k, long long, double y) { c.line(1, k) = y; });
-    cy.v[2] = stage_round(c, 0, ss, cy.v[2], [&](long long, int k) { return c.line(0, k); },
-                          [&](int k, long long t, double y) {
+    cy.v[1] = stage_round(c, 0, fs, cy.v[1], [&](int, int k) { return c.line(0, k); },
+                          [&](int k, int, double y) { c.line(1, k) = y; });
+    cy.v[2] = stage_round(c, 0, ss, cy.v[2], [&](int, int k) { return c.line(0, k); },
+                          [&](int k, int t, double y) {
                             c.put(0, k, t >= warm ? (float)(c.line(1, k) - y) : qnan());
                           });
   }
@@ -630,10 +658,10 @@ __device__ void volume_round(const Ctx<K>& c, const Job& j, Carry& cy, int mode)
 // (talib08:19171-19277, weights 1..p over the divider p(p+1)/2).
 // mode: 0 SMA, 1 SUM, 2 WMA.
 template <int K>
-__device__ void sum_window_round(const Ctx<K>& c, const Job& j, int mode) {
+__device__ __forceinline__ void sum_window_round(const Ctx<K>& c, const Job& j, int mode) {
   const int pl = j.in[0], p = j.ip[0];
-  const long long g0 = c.gb0();
-  const long long tf = g0 > p - 1 ? g0 : (long long)(p - 1);
+  const int g0 = c.gb0();
+  const int tf = g0 > p - 1 ? g0 : (int)(p - 1);
   double s = 0.0, w = 0.0;
   int nn = 0;
   if (tf < g0 + K && c.valid(tf)) {
@@ -645,7 +673,7 @@ __device__ void sum_window_round(const Ctx<K>& c, const Job& j, int mode) {
   }
   const double divider = (double)p * (p + 1) / 2.0;
   for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
+    const int t = g0 + k;
     if (!c.valid(t)) break;
     float o = qnan();
     if (t >= tf) {
@@ -674,10 +702,10 @@ __device__ void sum_window_round(const Ctx<K>& c, const Job& j, int mode) {
 // The middle band is the exact window sum divided by p, as TA-Lib's.
 // mode: 0 BBANDS, 1 STDDEV, 2 VAR.
 template <int K>
-__device__ void moment_window_round(const Ctx<K>& c, const Job& j, int mode) {
+__device__ __forceinline__ void moment_window_round(const Ctx<K>& c, const Job& j, int mode) {
   const int pl = j.in[0], p = j.ip[0];
-  const long long g0 = c.gb0();
-  const long long tf = g0 > p - 1 ? g0 : (long long)(p - 1);
+  const int g0 = c.gb0();
+  const int tf = g0 > p - 1 ? g0 : (int)(p - 1);
   double raw = 0.0, s2 = 0.0, o = 0.0;
   int nn = 0;
   if (tf < g0 + K && c.valid(tf)) {
@@ -692,7 +720,7 @@ __device__ void moment_window_round(const Ctx<K>& c, const Job& j, int mode) {
   const double inv = 1.0 / (double)p, po = (double)p * o;
   const double up = j.fp[0], dn = j.fp[1];
   for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
+    const int t = g0 + k;
     if (!c.valid(t)) break;
     float o0 = qnan(), o1 = qnan(), o2 = qnan();
     if (t >= tf) {
@@ -732,10 +760,10 @@ __device__ void moment_window_round(const Ctx<K>& c, const Job& j, int mode) {
 // lane-local origin o (LINEARREG(o + d) = o + LINEARREG(d)) and slide as
 // TA-Lib's: SumXY += SumY - p*y_out, SumY += y_in - y_out.
 template <int K>
-__device__ void linreg_round(const Ctx<K>& c, const Job& j) {
+__device__ __forceinline__ void linreg_round(const Ctx<K>& c, const Job& j) {
   const int pl = j.in[0], p = j.ip[0];
-  const long long g0 = c.gb0();
-  const long long tf = g0 > p - 1 ? g0 : (long long)(p - 1);
+  const int g0 = c.gb0();
+  const int tf = g0 > p - 1 ? g0 : (int)(p - 1);
   const double sumX = (double)p * (p - 1) * 0.5;
   const double sumXSqr = (double)p * (p - 1) * (2 * p - 1) / 6.0;
   const double divisor = sumX * sumX - p * sumXSqr;
@@ -751,7 +779,7 @@ __device__ void linreg_round(const Ctx<K>& c, const Job& j) {
     }
   }
   for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
+    const int t = g0 + k;
     if (!c.valid(t)) break;
     float out = qnan();
     if (t >= tf) {
@@ -776,13 +804,13 @@ __device__ void linreg_round(const Ctx<K>& c, const Job& j) {
 
 // Window extrema over [t-p+1, t] of a float plane; fmaxf/fminf ignore NaN.
 template <int K>
-__device__ __forceinline__ float win_max(const Ctx<K>& c, int pl, long long t, int p) {
+__device__ __forceinline__ float win_max(const Ctx<K>& c, int pl, int t, int p) {
   float v = c.x(pl, t - p + 1);
   for (int i = 1; i < p; ++i) v = fmaxf(v, c.x(pl, t - p + 1 + i));
   return v;
 }
 template <int K>
-__device__ __forceinline__ float win_min(const Ctx<K>& c, int pl, long long t, int p) {
+__device__ __forceinline__ float win_min(const Ctx<K>& c, int pl, int t, int p) {
   float v = c.x(pl, t - p + 1);
   for (int i = 1; i < p; ++i) v = fminf(v, c.x(pl, t - p + 1 + i));
   return v;
@@ -791,12 +819,12 @@ __device__ __forceinline__ float win_min(const Ctx<K>& c, int pl, long long t, i
 // MIN(p) / MAX(p): BatchFused.cu:110-119 (float extrema; a window reaching
 // into the row's leading NaN run stays NaN, LeadingNaN.cuh:21-27).
 template <int K>
-__device__ void minmax_round(const Ctx<K>& c, const Job& j, Carry& cy, bool is_max) {
+__device__ __forceinline__ void minmax_round(const Ctx<K>& c, const Job& j, Carry& cy, bool is_max) {
   const int pl = j.in[0], p = j.ip[0];
-  const long long f = resolve_start(c, cy, pl);
-  const long long g0 = c.gb0();
+  const int f = resolve_start(c, cy, pl);
+  const int g0 = c.gb0();
   for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
+    const int t = g0 + k;
     if (!c.valid(t)) break;
     float o = qnan();
     if (t >= p - 1) {
@@ -813,11 +841,11 @@ __device__ void minmax_round(const Ctx<K>& c, const Job& j, Carry& cy, bool is_m
 // comparisons seeded with the current bar), ((HH - C)/(HH - LL)) * -100 in
 // FP64, clamped to [-100, 0]; 0 for a zero range.
 template <int K>
-__device__ void willr_round(const Ctx<K>& c, const Job& j) {
+__device__ __forceinline__ void willr_round(const Ctx<K>& c, const Job& j) {
   const int ph = j.in[0], plo = j.in[1], pc = j.in[2], p = j.ip[0];
-  const long long g0 = c.gb0();
+  const int g0 = c.gb0();
   for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
+    const int t = g0 + k;
     if (!c.valid(t)) break;
     float o = qnan();
     if (t >= p - 1) {
@@ -841,12 +869,12 @@ __device__ void willr_round(const Ctx<K>& c, const Job& j) {
 // slowD = SMA_d(slowK), both from bar k-1+2(d-1). fastK of the round and of the
 // 2(d-1) bars before it goes to scratch line 0, then each bar averages it.
 template <int K>
-__device__ void stoch_round(const Ctx<K>& c, const Job& j) {
+__device__ __forceinline__ void stoch_round(const Ctx<K>& c, const Job& j) {
   const int ph = j.in[0], plo = j.in[1], pc = j.in[2];
   const int p = j.ip[0], q = j.ip[1];
-  const long long lb = (long long)p - 1 + 2ll * (q - 1);
+  const int lb = (int)p - 1 + 2ll * (q - 1);
   const int ext = 2 * (q - 1);
-  auto fastk = [&](long long t) -> double {
+  auto fastk = [&](int t) -> double {
     if (t < p - 1) return 0.0;
     double lo = c.x(plo, t - p + 1), hi = c.x(ph, t - p + 1);
     for (int i = 1; i < p; ++i) {
@@ -857,9 +885,9 @@ __device__ void stoch_round(const Ctx<K>& c, const Job& j) {
     const double range = hi - lo;
     return fabs(range) <= 1e-14 * (fabs(hi) + fabs(lo)) ? 0.0 : ((double)c.x(pc, t) - lo) / range * 100.0;
   };
-  const long long g0 = c.gb0();
+  const int g0 = c.gb0();
   for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
+    const int t = g0 + k;
     if (!c.valid(t)) break;
     c.line(0, k) = fastk(t);
   }
@@ -867,7 +895,7 @@ __device__ void stoch_round(const Ctx<K>& c, const Job& j) {
   __syncwarp();
   const double invq = 1.0 / (double)q;
   for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
+    const int t = g0 + k;
     if (!c.valid(t)) break;
     float o0 = qnan(), o1 = qnan();
     if (t >= lb) {
@@ -894,11 +922,11 @@ __device__ void stoch_round(const Ctx<K>& c, const Job& j) {
 // window mean and mean absolute deviation; (tp - sma)/(0.015*md), 0 unless both
 // the numerator and md are nonzero.
 template <int K>
-__device__ void cci_round(const Ctx<K>& c, const Job& j) {
+__device__ __forceinline__ void cci_round(const Ctx<K>& c, const Job& j) {
   const int p = j.ip[0];
-  const long long g0 = c.gb0();
+  const int g0 = c.gb0();
   for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
+    const int t = g0 + k;
     if (!c.valid(t)) break;
     float o = qnan();
     if (t >= p - 1) {
@@ -921,10 +949,10 @@ __device__ void cci_round(const Ctx<K>& c, const Job& j) {
 // negative sums over the last p flows, 100*pos/(pos+neg), 0 when the total is
 // below 1; output from bar p.
 template <int K>
-__device__ void mfi_round(const Ctx<K>& c, const Job& j) {
+__device__ __forceinline__ void mfi_round(const Ctx<K>& c, const Job& j) {
   const int pv = j.in[3], p = j.ip[0];
-  const long long g0 = c.gb0();
-  auto flow = [&](long long t, double& pos, double& neg) {
+  const int g0 = c.gb0();
+  auto flow = [&](int t, double& pos, double& neg) {
     pos = neg = 0.0;
     if (t < 1) return;
     const double pr = c.typ(t), pp = c.typ(t - 1);
@@ -934,7 +962,7 @@ __device__ void mfi_round(const Ctx<K>& c, const Job& j) {
       else if (pr < pp) neg = fl;
     }
   };
-  const long long tf = g0 > p ? g0 : (long long)p;
+  const int tf = g0 > p ? g0 : (int)p;
   double ps = 0.0, ns = 0.0;
   if (tf < g0 + K && c.valid(tf)) {
     for (int i = p - 1; i >= 0; --i) {
@@ -944,7 +972,7 @@ __device__ void mfi_round(const Ctx<K>& c, const Job& j) {
     }
   }
   for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
+    const int t = g0 + k;
     if (!c.valid(t)) break;
     float o = qnan();
     if (t >= tf) {
@@ -972,22 +1000,22 @@ __device__ void mfi_round(const Ctx<K>& c, const Job& j) {
 // product (<= 1e-14) vanishes; 0 from the first non-finite bar of the row on
 // (findInvalidSuffix, Correl.cu:14-21). Carry.f holds that first bar (-1 none).
 template <int K>
-__device__ void correl_round(const Ctx<K>& c, const Job& j, Carry& cy) {
+__device__ __forceinline__ void correl_round(const Ctx<K>& c, const Job& j, Carry& cy) {
   const int px = j.in[0], py = j.in[1], p = j.ip[0];
-  const long long g0 = c.gb0();
-  long long bad = cy.f;
+  const int g0 = c.gb0();
+  int bad = cy.f;
   if (bad < 0) {
-    long long first = 0x7fffffffffffffffll;
+    int first = 0x7fffffff;
     for (int k = 0; k < K; ++k) {
-      const long long t = g0 + k;
+      const int t = g0 + k;
       if (!c.valid(t)) break;
       if (!isfinite(c.x(px, t)) || !isfinite(c.x(py, t))) { first = t; break; }
     }
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) first = min(first, __shfl_xor_sync(kFull, first, d));
-    bad = first == 0x7fffffffffffffffll ? -1 : first;
+    bad = first == 0x7fffffff ? -1 : first;
   }
-  const long long tf = g0 > p - 1 ? g0 : (long long)(p - 1);
+  const int tf = g0 > p - 1 ? g0 : (int)(p - 1);
   double sx = 0, sy = 0, sxx = 0, syy = 0, sxy = 0, ox = 0, oy = 0;
   if (tf < g0 + K && c.valid(tf)) {
     ox = c.x(px, tf - p + 1);
@@ -1001,7 +1029,7 @@ __device__ void correl_round(const Ctx<K>& c, const Job& j, Carry& cy) {
   }
   const double pp = (double)p;
   for (int k = 0; k < K; ++k) {
-    const long long t = g0 + k;
+    const int t = g0 + k;
     if (!c.valid(t)) break;
     float o = qnan();
     if (t >= tf) {

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <mutex>
 #include <vector>
 
@@ -38,8 +39,8 @@ void load_cache_locked() {
   ShapeKey k{};
   SchedulePlan p{};
   unsigned long long jobs = 0;
-  while (std::fscanf(f, "%d %d %d %llx %d %d %d", &k.S_bucket, &k.T_bucket, &k.Tmax_bucket, &jobs, &p.k,
-                     &p.warps_per_block, &p.max_blocks) == 7) {
+  while (std::fscanf(f, "%d %d %d %llx %d %d %d %d %d", &k.S_bucket, &k.T_bucket, &k.Tmax_bucket, &jobs, &p.mode,
+                     &p.groups, &p.k, &p.warps_per_block, &p.max_blocks) == 9) {
     k.jobs = jobs;
     g_tuned.emplace_back(k, p);
   }
@@ -75,6 +76,15 @@ SchedulePlan plan_for(const Launch& L, long long total_bars, long long max_len) 
   else if (mean <= 512) p.k = 8;
   else p.k = 16;
   p.warps_per_block = 8;
+  // Many series: one thread per series walking it in TA-Lib order (no scans).
+  // Few or very long series: a warp per series splitting time across lanes.
+  p.mode = (L.S >= 512 && max_len <= (1ll << 22)) ? 1 : 0;
+  if (const char* e = std::getenv("TACUDA_B200_MODE")) {
+    if (std::strcmp(e, "sp") == 0) p.mode = 1;
+    if (std::strcmp(e, "ws") == 0) p.mode = 0;
+  }
+  for (int j = 0; j < L.njobs; ++j)
+    if (L.jobs[j].family == F_CDL) p.mode = 1;  // candles run on the series-parallel engine
   // TACUDA_B200_BARS_PER_LANE=4|8|16 pins the round width (read on every call):
   // results of a row are then bit-independent of its length as well as of the
   // other rows, batch size and order.
@@ -93,8 +103,9 @@ void remember_plan(const ShapeKey& key, const SchedulePlan& plan) {
   g_tuned.emplace_back(key, plan);
   if (const char* path = std::getenv("TACUDA_B200_TUNE_CACHE")) {
     if (FILE* f = std::fopen(path, "a")) {
-      std::fprintf(f, "%d %d %d %llx %d %d %d\n", key.S_bucket, key.T_bucket, key.Tmax_bucket,
-                   (unsigned long long)key.jobs, plan.k, plan.warps_per_block, plan.max_blocks);
+      std::fprintf(f, "%d %d %d %llx %d %d %d %d %d\n", key.S_bucket, key.T_bucket, key.Tmax_bucket,
+                   (unsigned long long)key.jobs, plan.mode, plan.groups, plan.k, plan.warps_per_block,
+                   plan.max_blocks);
       std::fclose(f);
     }
   }

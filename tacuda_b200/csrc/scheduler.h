@@ -11,6 +11,8 @@
 namespace tb {
 
 struct SchedulePlan {
+  int mode = 0;            // 0: warp per series (time-parallel lanes), 1: thread per series
+  int groups = 0;          // series-parallel: 32-series groups per CTA (0 = auto)
   int k = 8;               // bars per lane; a round covers 32*k bars
   int warps_per_block = 8;
   int max_blocks = 0;      // 0 = as many as fit

@@ -1,0 +1,578 @@
+// Candlestick engine (series-parallel): the 61 TA-Lib CDL patterns (plus the
+// reference's legacy bullish/bearish engulfing split) for every bar.
+//
+// TA-Lib's candle settings average one of three ranges (real body |c-o|,
+// high-low, upper+lower shadows) over the 10 or 5 bars before an anchor bar
+// (include/utils/CandleUtils.h:37-63, 1466-1495). Per chunk, the first candle
+// warp of a group writes the four distinct trailing sums (body/10, high-low/10,
+// shadows/10, high-low/5) for the anchors r-4 .. C-1 of its 32 rows into a
+// shared table, sliding them in FP64: the ranges of float32 bars are exact in
+// FP64 and so are their sums, so the table equals the reference's per-call
+// re-summing bit for bit. Every candle warp of the group then evaluates its own
+// subset of patterns bar by bar from the staged bars and the table and writes
+// each pattern through a transpose buffer as coalesced rows (int32 or float).
+#pragma once
+
+#include "sp_families.cuh"
+
+namespace tb {
+namespace sp {
+
+enum CdlRange { CR_BODY = 0, CR_HL = 1, CR_SHADOW = 2 };
+enum CdlSet {
+  BODY_LONG = 0, BODY_VERY_LONG, BODY_SHORT, BODY_DOJI, SHADOW_LONG, SHADOW_VERY_LONG, SHADOW_SHORT,
+  SHADOW_VERY_SHORT, NEAR, FAR, EQUAL
+};
+// table slot of each setting (-1: uses the bar itself), factor, divisor, period
+__device__ __constant__ const int kSetSlot[11] = {0, 0, 0, 1, -1, -1, 2, 1, 3, 3, 3};
+__device__ __constant__ const float kSetFactor[11] = {1.0f, 3.0f, 1.0f, 0.1f, 1.0f, 2.0f, 1.0f, 0.1f, 0.2f, 0.6f, 0.05f};
+__device__ __constant__ const int kSlotPeriod[4] = {10, 10, 10, 5};
+
+constexpr int kCdlBack = 5;  // anchors r-5 .. r (HIKKAKEMOD reads NEAR at r-5)
+
+// Shared table of trailing sums: [slot 0..3][row 0..31][anchor r + kCdlBack]
+// (anchor a holds the sum of the slot's range over bars a-period .. a-1)
+struct CdlTable {
+  double* p;
+  int W;  // C + kCdlBack
+  __device__ __forceinline__ double& at(int slot, int row, int r) const {
+    return p[((size_t)slot * 32 + row) * W + r + kCdlBack];
+  }
+};
+
+__device__ __forceinline__ double cdl_range(int type, float o, float h, float l, float c) {
+  const double od = o, hd = h, ld = l, cd = c;
+  if (type == CR_BODY) return fabs(cd - od);
+  if (type == CR_HL) return hd - ld;
+  return (hd - fmax(od, cd)) + (fmin(od, cd) - ld);
+}
+
+// View of one row at bar r for the pattern decisions.
+struct Bars {
+  const CdlTable* tb;
+  int lane, r;
+  long long t;
+  const float *Op, *Hp, *Lp, *Cp;
+  __device__ __forceinline__ float O(int d) const { return Op[r - d]; }
+  __device__ __forceinline__ float H(int d) const { return Hp[r - d]; }
+  __device__ __forceinline__ float L(int d) const { return Lp[r - d]; }
+  __device__ __forceinline__ float C(int d) const { return Cp[r - d]; }
+  __device__ __forceinline__ double RB(int d) const { return fabs((double)C(d) - (double)O(d)); }
+  __device__ __forceinline__ double US(int d) const { return (double)H(d) - fmax((double)O(d), (double)C(d)); }
+  __device__ __forceinline__ double LS(int d) const { return fmin((double)O(d), (double)C(d)) - (double)L(d); }
+  __device__ __forceinline__ int COL(int d) const { return C(d) >= O(d) ? 1 : -1; }
+  __device__ __forceinline__ float TOP(int d) const { return fmaxf(O(d), C(d)); }
+  __device__ __forceinline__ float BOT(int d) const { return fminf(O(d), C(d)); }
+  __device__ __forceinline__ bool BGAP_UP(int a, int b) const { return fminf(O(a), C(a)) > fmaxf(O(b), C(b)); }
+  __device__ __forceinline__ bool BGAP_DN(int a, int b) const { return fmaxf(O(a), C(a)) < fminf(O(b), C(b)); }
+  __device__ __forceinline__ bool RGAP_UP(int a, int b) const { return L(a) > H(b); }
+  __device__ __forceinline__ bool RGAP_DN(int a, int b) const { return H(a) < L(b); }
+  // TA-Lib candle average of setting s anchored at bar r-d
+  __device__ __forceinline__ double AVG(int s, int d) const {
+    const int slot = kSetSlot[s];
+    const double factor = (double)kSetFactor[s];
+    const double div = slot == 2 ? 2.0 : 1.0;
+    const long long a = t - d;
+    if (slot < 0) return factor * RB(d) / div;
+    const int per = kSlotPeriod[slot];
+    const long long cnt = a < per ? a : per;
+    if (cnt <= 0) {
+      const int type = slot == 0 ? CR_BODY : (slot == 2 ? CR_SHADOW : CR_HL);
+      return factor * cdl_range(type, O(d), H(d), L(d), C(d)) / div;
+    }
+    return factor * (tb->at(slot, lane, r - d) / (double)cnt) / div;
+  }
+};
+
+#define CDL_FN(name) __device__ __forceinline__ int name(const Bars& b)
+
+CDL_FN(c_two_crows) {
+  return (b.COL(2) == 1 && b.RB(2) > b.AVG(BODY_LONG, 2) && b.COL(1) == -1 && b.BGAP_UP(1, 2) && b.COL(0) == -1 &&
+          b.O(0) < b.O(1) && b.O(0) > b.C(1) && b.C(0) > b.O(2) && b.C(0) < b.C(2)) ? -100 : 0;
+}
+CDL_FN(c_three_black_crows) {
+  return (b.COL(3) == 1 && b.COL(2) == -1 && b.LS(2) < b.AVG(SHADOW_VERY_SHORT, 2) && b.COL(1) == -1 &&
+          b.LS(1) < b.AVG(SHADOW_VERY_SHORT, 1) && b.COL(0) == -1 && b.LS(0) < b.AVG(SHADOW_VERY_SHORT, 0) &&
+          b.O(1) < b.O(2) && b.O(1) > b.C(2) && b.O(0) < b.O(1) && b.O(0) > b.C(1) && b.H(3) > b.C(2) &&
+          b.C(2) > b.C(1) && b.C(1) > b.C(0)) ? -100 : 0;
+}
+CDL_FN(c_three_inside) {
+  if (b.RB(2) > b.AVG(BODY_LONG, 2) && b.RB(1) <= b.AVG(BODY_SHORT, 1) &&
+      fmaxf(b.C(1), b.O(1)) < fmaxf(b.C(2), b.O(2)) && fminf(b.C(1), b.O(1)) > fminf(b.C(2), b.O(2)) &&
+      ((b.COL(2) == 1 && b.COL(0) == -1 && b.C(0) < b.O(2)) || (b.COL(2) == -1 && b.COL(0) == 1 && b.C(0) > b.O(2))))
+    return -b.COL(2) * 100;
+  return 0;
+}
+CDL_FN(c_three_line_strike) {
+  if (b.COL(3) == b.COL(2) && b.COL(2) == b.COL(1) && b.COL(0) == -b.COL(1) &&
+      (double)b.O(2) >= (double)b.BOT(3) - b.AVG(NEAR, 3) && (double)b.O(2) <= (double)b.TOP(3) + b.AVG(NEAR, 3) &&
+      (double)b.O(1) >= (double)b.BOT(2) - b.AVG(NEAR, 2) && (double)b.O(1) <= (double)b.TOP(2) + b.AVG(NEAR, 2) &&
+      ((b.COL(1) == 1 && b.C(1) > b.C(2) && b.C(2) > b.C(3) && b.O(0) > b.C(1) && b.C(0) < b.O(3)) ||
+       (b.COL(1) == -1 && b.C(1) < b.C(2) && b.C(2) < b.C(3) && b.O(0) < b.C(1) && b.C(0) > b.O(3))))
+    return b.COL(1) * 100;
+  return 0;
+}
+CDL_FN(c_three_outside) {
+  if ((b.COL(1) == 1 && b.COL(2) == -1 && b.C(1) > b.O(2) && b.O(1) < b.C(2) && b.C(0) > b.C(1)) ||
+      (b.COL(1) == -1 && b.COL(2) == 1 && b.O(1) > b.C(2) && b.C(1) < b.O(2) && b.C(0) < b.C(1)))
+    return b.COL(1) * 100;
+  return 0;
+}
+CDL_FN(c_three_stars_in_south) {
+  return (b.COL(2) == -1 && b.COL(1) == -1 && b.COL(0) == -1 && b.RB(2) > b.AVG(BODY_LONG, 2) &&
+          b.LS(2) > b.AVG(SHADOW_LONG, 2) && b.RB(1) < b.RB(2) && b.O(1) > b.C(2) && b.O(1) <= b.H(2) &&
+          b.L(1) < b.C(2) && b.L(1) >= b.L(2) && b.LS(1) > b.AVG(SHADOW_VERY_SHORT, 1) &&
+          b.RB(0) < b.AVG(BODY_SHORT, 0) && b.LS(0) < b.AVG(SHADOW_VERY_SHORT, 0) &&
+          b.US(0) < b.AVG(SHADOW_VERY_SHORT, 0) && b.L(0) > b.L(1) && b.H(0) < b.H(1)) ? 100 : 0;
+}
+CDL_FN(c_three_white_soldiers) {
+  return (b.COL(2) == 1 && b.US(2) < b.AVG(SHADOW_VERY_SHORT, 2) && b.COL(1) == 1 &&
+          b.US(1) < b.AVG(SHADOW_VERY_SHORT, 1) && b.COL(0) == 1 && b.US(0) < b.AVG(SHADOW_VERY_SHORT, 0) &&
+          b.C(0) > b.C(1) && b.C(1) > b.C(2) && b.O(1) > b.O(2) &&
+          (double)b.O(1) <= (double)b.C(2) + b.AVG(NEAR, 2) && b.O(0) > b.O(1) &&
+          (double)b.O(0) <= (double)b.C(1) + b.AVG(NEAR, 1) && b.RB(1) > b.RB(2) - b.AVG(FAR, 2) &&
+          b.RB(0) > b.RB(1) - b.AVG(FAR, 1) && b.RB(0) > b.AVG(BODY_SHORT, 0)) ? 100 : 0;
+}
+CDL_FN(c_abandoned_baby) {
+  const double pen = 0.3;
+  if (b.RB(2) > b.AVG(BODY_LONG, 2) && b.RB(1) <= b.AVG(BODY_DOJI, 1) && b.RB(0) > b.AVG(BODY_SHORT, 0) &&
+      ((b.COL(2) == 1 && b.COL(0) == -1 && b.C(0) < b.C(2) - b.RB(2) * pen && b.RGAP_UP(1, 2) && b.RGAP_DN(0, 1)) ||
+       (b.COL(2) == -1 && b.COL(0) == 1 && b.C(0) > b.C(2) + b.RB(2) * pen && b.RGAP_DN(1, 2) && b.RGAP_UP(0, 1))))
+    return b.COL(0) * 100;
+  return 0;
+}
+CDL_FN(c_advance_block) {
+  if (b.COL(2) == 1 && b.COL(1) == 1 && b.COL(0) == 1 && b.C(0) > b.C(1) && b.C(1) > b.C(2) && b.O(1) > b.O(2) &&
+      b.O(1) <= b.C(2) + b.AVG(NEAR, 2) && b.O(0) > b.O(1) && b.O(0) <= b.C(1) + b.AVG(NEAR, 1) &&
+      b.RB(2) > b.AVG(BODY_LONG, 2) && b.US(2) < b.AVG(SHADOW_SHORT, 2) &&
+      ((b.RB(1) < b.RB(2) - b.AVG(FAR, 2) && b.RB(0) < b.RB(1) + b.AVG(NEAR, 1)) ||
+       (b.RB(0) < b.RB(1) - b.AVG(FAR, 1)) ||
+       (b.RB(0) < b.RB(1) && b.RB(1) < b.RB(2) &&
+        (b.US(0) > b.AVG(SHADOW_SHORT, 0) || b.US(1) > b.AVG(SHADOW_SHORT, 1))) ||
+       (b.RB(0) < b.RB(1) && b.US(0) > b.AVG(SHADOW_LONG, 0))))
+    return -100;
+  return 0;
+}
+CDL_FN(c_belt_hold) {
+  if (b.RB(0) > b.AVG(BODY_LONG, 0) && ((b.COL(0) == 1 && b.LS(0) < b.AVG(SHADOW_VERY_SHORT, 0)) ||
+                                         (b.COL(0) == -1 && b.US(0) < b.AVG(SHADOW_VERY_SHORT, 0))))
+    return b.COL(0) * 100;
+  return 0;
+}
+CDL_FN(c_breakaway) {
+  if (b.RB(4) > b.AVG(BODY_LONG, 4) && b.COL(4) == b.COL(3) && b.COL(3) == b.COL(1) && b.COL(1) == -b.COL(0) &&
+      ((b.COL(4) == -1 && b.BGAP_DN(3, 4) && b.H(2) < b.H(3) && b.L(2) < b.L(3) && b.H(1) < b.H(2) &&
+        b.L(1) < b.L(2) && b.C(0) > b.O(3) && b.C(0) < b.C(4)) ||
+       (b.COL(4) == 1 && b.BGAP_UP(3, 4) && b.H(2) > b.H(3) && b.L(2) > b.L(3) && b.H(1) > b.H(2) &&
+        b.L(1) > b.L(2) && b.C(0) < b.O(3) && b.C(0) > b.C(4))))
+    return b.COL(0) * 100;
+  return 0;
+}
+CDL_FN(c_closing_marubozu) {
+  if (b.RB(0) > b.AVG(BODY_LONG, 0) && ((b.COL(0) == 1 && b.US(0) < b.AVG(SHADOW_VERY_SHORT, 0)) ||
+                                         (b.COL(0) == -1 && b.LS(0) < b.AVG(SHADOW_VERY_SHORT, 0))))
+    return b.COL(0) * 100;
+  return 0;
+}
+CDL_FN(c_conceal_baby_swallow) {
+  return (b.COL(3) == -1 && b.COL(2) == -1 && b.COL(1) == -1 && b.COL(0) == -1 &&
+          b.LS(3) < b.AVG(SHADOW_VERY_SHORT, 3) && b.US(3) < b.AVG(SHADOW_VERY_SHORT, 3) &&
+          b.LS(2) < b.AVG(SHADOW_VERY_SHORT, 2) && b.US(2) < b.AVG(SHADOW_VERY_SHORT, 2) && b.BGAP_DN(1, 2) &&
+          b.US(1) > b.AVG(SHADOW_VERY_SHORT, 1) && b.H(1) > b.C(2) && b.H(0) > b.H(1) && b.L(0) < b.L(1)) ? 100 : 0;
+}
+CDL_FN(c_counterattack) {
+  if (b.COL(1) == -b.COL(0) && b.RB(1) > b.AVG(BODY_LONG, 1) && b.RB(0) > b.AVG(BODY_LONG, 0) &&
+      b.C(0) <= b.C(1) + b.AVG(EQUAL, 1) && b.C(0) >= b.C(1) - b.AVG(EQUAL, 1))
+    return b.COL(0) * 100;
+  return 0;
+}
+CDL_FN(c_dark_cloud_cover) {
+  return (b.COL(1) == 1 && b.RB(1) > b.AVG(BODY_LONG, 1) && b.COL(0) == -1 && b.O(0) > b.H(1) && b.C(0) > b.O(1) &&
+          (double)b.C(0) < (double)b.C(1) - b.RB(1) * 0.5) ? -100 : 0;
+}
+CDL_FN(c_doji) { return b.RB(0) <= b.AVG(BODY_DOJI, 0) ? 100 : 0; }
+CDL_FN(c_doji_star) {
+  if (b.RB(1) > b.AVG(BODY_LONG, 1) && b.RB(0) <= b.AVG(BODY_DOJI, 0) &&
+      ((b.COL(1) == 1 && b.BGAP_UP(0, 1)) || (b.COL(1) == -1 && b.BGAP_DN(0, 1))))
+    return -b.COL(1) * 100;
+  return 0;
+}
+CDL_FN(c_dragonfly_doji) {
+  return (b.RB(0) <= b.AVG(BODY_DOJI, 0) && b.US(0) < b.AVG(SHADOW_VERY_SHORT, 0) &&
+          b.LS(0) > b.AVG(SHADOW_VERY_SHORT, 0)) ? 100 : 0;
+}
+CDL_FN(c_engulfing) {
+  const bool white = b.COL(0) == 1 && b.COL(1) == -1 &&
+                     ((b.C(0) >= b.O(1) && b.O(0) < b.C(1)) || (b.C(0) > b.O(1) && b.O(0) <= b.C(1)));
+  const bool black = b.COL(0) == -1 && b.COL(1) == 1 &&
+                     ((b.O(0) >= b.C(1) && b.C(0) < b.O(1)) || (b.O(0) > b.C(1) && b.C(0) <= b.O(1)));
+  if (white || black) return (b.O(0) != b.C(1) && b.C(0) != b.O(1)) ? b.COL(0) * 100 : b.COL(0) * 80;
+  return 0;
+}
+__device__ __forceinline__ bool star_shape(const Bars& b, bool doji_middle, bool bull) {
+  const double pen = 0.3;
+  const bool mid = doji_middle ? b.RB(1) <= b.AVG(BODY_DOJI, 1) : b.RB(1) <= b.AVG(BODY_SHORT, 1);
+  if (bull)
+    return b.RB(2) > b.AVG(BODY_LONG, 2) && b.COL(2) == -1 && mid && b.BGAP_DN(1, 2) &&
+           b.RB(0) > b.AVG(BODY_SHORT, 0) && b.COL(0) == 1 && (double)b.C(0) > (double)b.C(2) + b.RB(2) * pen;
+  return b.RB(2) > b.AVG(BODY_LONG, 2) && b.COL(2) == 1 && mid && b.BGAP_UP(1, 2) &&
+         b.RB(0) > b.AVG(BODY_SHORT, 0) && b.COL(0) == -1 && (double)b.C(0) < (double)b.C(2) - b.RB(2) * pen;
+}
+CDL_FN(c_evening_doji_star) { return star_shape(b, true, false) ? -100 : 0; }
+CDL_FN(c_evening_star) { return star_shape(b, false, false) ? -100 : 0; }
+CDL_FN(c_morning_doji_star) { return star_shape(b, true, true) ? 100 : 0; }
+CDL_FN(c_morning_star) { return star_shape(b, false, true) ? 100 : 0; }
+CDL_FN(c_gap_side_side_white) {
+  if (((b.BGAP_UP(1, 2) && b.BGAP_UP(0, 2)) || (b.BGAP_DN(1, 2) && b.BGAP_DN(0, 2))) && b.COL(1) == 1 &&
+      b.COL(0) == 1 && b.RB(0) >= b.RB(1) - b.AVG(NEAR, 1) && b.RB(0) <= b.RB(1) + b.AVG(NEAR, 1) &&
+      b.O(0) >= b.O(1) - b.AVG(EQUAL, 1) && b.O(0) <= b.O(1) + b.AVG(EQUAL, 1))
+    return b.BGAP_UP(1, 2) ? 100 : -100;
+  return 0;
+}
+CDL_FN(c_gravestone_doji) {
+  return (b.RB(0) <= b.AVG(BODY_DOJI, 0) && b.LS(0) < b.AVG(SHADOW_VERY_SHORT, 0) &&
+          b.US(0) > b.AVG(SHADOW_VERY_SHORT, 0)) ? 100 : 0;
+}
+__device__ __forceinline__ bool hammer_shape(const Bars& b) {
+  return b.RB(0) < b.AVG(BODY_SHORT, 0) && b.LS(0) > b.AVG(SHADOW_LONG, 0) && b.US(0) < b.AVG(SHADOW_VERY_SHORT, 0);
+}
+CDL_FN(c_hammer) {
+  return (hammer_shape(b) && (double)fminf(b.C(0), b.O(0)) <= (double)b.L(1) + b.AVG(NEAR, 1)) ? 100 : 0;
+}
+CDL_FN(c_hanging_man) {
+  return (hammer_shape(b) && (double)fminf(b.C(0), b.O(0)) >= (double)b.H(1) - b.AVG(NEAR, 1)) ? -100 : 0;
+}
+__device__ __forceinline__ int harami_common(const Bars& b, bool cross) {
+  const bool small = cross ? b.RB(0) <= b.AVG(BODY_DOJI, 0) : b.RB(0) <= b.AVG(BODY_SHORT, 0);
+  if (b.RB(1) > b.AVG(BODY_LONG, 1) && small) {
+    const float hi2 = fmaxf(b.C(0), b.O(0)), lo2 = fminf(b.C(0), b.O(0));
+    const float hi1 = fmaxf(b.C(1), b.O(1)), lo1 = fminf(b.C(1), b.O(1));
+    if (hi2 < hi1 && lo2 > lo1) return -b.COL(1) * 100;
+    if (hi2 <= hi1 && lo2 >= lo1) return -b.COL(1) * 80;
+  }
+  return 0;
+}
+CDL_FN(c_harami) { return harami_common(b, false); }
+CDL_FN(c_harami_cross) { return harami_common(b, true); }
+CDL_FN(c_high_wave) {
+  return (b.RB(0) < b.AVG(BODY_SHORT, 0) && b.US(0) > b.AVG(SHADOW_VERY_LONG, 0) &&
+          b.LS(0) > b.AVG(SHADOW_VERY_LONG, 0)) ? b.COL(0) * 100 : 0;
+}
+// HIKKAKE / HIKKAKEMOD: the pattern bar, or its confirmation within three bars
+// (first confirming close only), CandleUtils.h:1849-1895.
+__device__ __forceinline__ int hikkake_at(const Bars& b, int d) {
+  if (b.H(d + 1) < b.H(d + 2) && b.L(d + 1) > b.L(d + 2) &&
+      ((b.H(d) < b.H(d + 1) && b.L(d) < b.L(d + 1)) || (b.H(d) > b.H(d + 1) && b.L(d) > b.L(d + 1))))
+    return b.H(d) < b.H(d + 1) ? 100 : -100;
+  return 0;
+}
+__device__ __forceinline__ int hikkake_mod_at(const Bars& b, int d) {
+  if (b.H(d + 2) < b.H(d + 3) && b.L(d + 2) > b.L(d + 3) && b.H(d + 1) < b.H(d + 2) && b.L(d + 1) > b.L(d + 2) &&
+      ((b.H(d) < b.H(d + 1) && b.L(d) < b.L(d + 1) && b.C(d + 2) <= b.L(d + 2) + b.AVG(NEAR, d + 2)) ||
+       (b.H(d) > b.H(d + 1) && b.L(d) > b.L(d + 1) && b.C(d + 2) >= b.H(d + 2) - b.AVG(NEAR, d + 2))))
+    return b.H(d) < b.H(d + 1) ? 100 : -100;
+  return 0;
+}
+__device__ __forceinline__ int hikkake_confirm(const Bars& b, bool modified) {
+  const int pat = modified ? hikkake_mod_at(b, 0) : hikkake_at(b, 0);
+  if (pat != 0) return pat;
+  const long long lowest = modified ? 3 : 2;
+  for (int d = 1; d <= 3 && b.t - d >= lowest; ++d) {
+    const int pj = modified ? hikkake_mod_at(b, d) : hikkake_at(b, d);
+    if (pj == 0) continue;
+    for (int m = d - 1; m >= 0; --m) {
+      const bool conf = (pj > 0 && b.C(m) > b.H(d + 1)) || (pj < 0 && b.C(m) < b.L(d + 1));
+      if (conf) return m == 0 ? pj + (pj > 0 ? 100 : -100) : 0;
+    }
+    return 0;
+  }
+  return 0;
+}
+CDL_FN(c_hikkake) { return hikkake_confirm(b, false); }
+CDL_FN(c_hikkake_mod) { return hikkake_confirm(b, true); }
+CDL_FN(c_homing_pigeon) {
+  return (b.COL(1) == -1 && b.COL(0) == -1 && b.RB(1) > b.AVG(BODY_LONG, 1) && b.RB(0) <= b.AVG(BODY_SHORT, 0) &&
+          b.O(0) < b.O(1) && b.C(0) > b.C(1)) ? 100 : 0;
+}
+CDL_FN(c_identical_three_crows) {
+  return (b.COL(2) == -1 && b.LS(2) < b.AVG(SHADOW_VERY_SHORT, 2) && b.COL(1) == -1 &&
+          b.LS(1) < b.AVG(SHADOW_VERY_SHORT, 1) && b.COL(0) == -1 && b.LS(0) < b.AVG(SHADOW_VERY_SHORT, 0) &&
+          b.C(2) > b.C(1) && b.C(1) > b.C(0) && (double)b.O(1) <= (double)b.C(2) + b.AVG(EQUAL, 2) &&
+          (double)b.O(1) >= (double)b.C(2) - b.AVG(EQUAL, 2) && (double)b.O(0) <= (double)b.C(1) + b.AVG(EQUAL, 1) &&
+          (double)b.O(0) >= (double)b.C(1) - b.AVG(EQUAL, 1)) ? -100 : 0;
+}
+CDL_FN(c_in_neck) {
+  return (b.COL(1) == -1 && b.RB(1) > b.AVG(BODY_LONG, 1) && b.COL(0) == 1 && b.O(0) < b.L(1) &&
+          (double)b.C(0) <= (double)b.C(1) + b.AVG(EQUAL, 1) && b.C(0) >= b.C(1)) ? -100 : 0;
+}
+CDL_FN(c_inverted_hammer) {
+  return (b.RB(0) < b.AVG(BODY_SHORT, 0) && b.US(0) > b.AVG(SHADOW_LONG, 0) &&
+          b.LS(0) < b.AVG(SHADOW_VERY_SHORT, 0) && b.BGAP_DN(0, 1)) ? 100 : 0;
+}
+__device__ __forceinline__ bool kicking_common(const Bars& b) {
+  return b.COL(1) == -b.COL(0) && b.RB(1) > b.AVG(BODY_LONG, 1) && b.US(1) < b.AVG(SHADOW_VERY_SHORT, 1) &&
+         b.LS(1) < b.AVG(SHADOW_VERY_SHORT, 1) && b.RB(0) > b.AVG(BODY_LONG, 0) &&
+         b.US(0) < b.AVG(SHADOW_VERY_SHORT, 0) && b.LS(0) < b.AVG(SHADOW_VERY_SHORT, 0) &&
+         ((b.COL(1) == -1 && b.RGAP_UP(0, 1)) || (b.COL(1) == 1 && b.RGAP_DN(0, 1)));
+}
+CDL_FN(c_kicking) { return kicking_common(b) ? b.COL(0) * 100 : 0; }
+CDL_FN(c_kicking_by_length) {
+  if (!kicking_common(b)) return 0;
+  return (b.RB(0) > b.RB(1) ? b.COL(0) : b.COL(1)) * 100;
+}
+CDL_FN(c_ladder_bottom) {
+  return (b.COL(4) == -1 && b.COL(3) == -1 && b.COL(2) == -1 && b.O(4) > b.O(3) && b.O(3) > b.O(2) &&
+          b.C(4) > b.C(3) && b.C(3) > b.C(2) && b.COL(1) == -1 && b.US(1) > b.AVG(SHADOW_VERY_SHORT, 1) &&
+          b.COL(0) == 1 && b.O(0) > b.O(1) && b.C(0) > b.H(1)) ? 100 : 0;
+}
+CDL_FN(c_long_legged_doji) {
+  return (b.RB(0) <= b.AVG(BODY_DOJI, 0) &&
+          (b.LS(0) > b.AVG(SHADOW_LONG, 0) || b.US(0) > b.AVG(SHADOW_LONG, 0))) ? 100 : 0;
+}
+CDL_FN(c_long_line) {
+  return (b.RB(0) > b.AVG(BODY_LONG, 0) && b.US(0) < b.AVG(SHADOW_SHORT, 0) && b.LS(0) < b.AVG(SHADOW_SHORT, 0))
+             ? b.COL(0) * 100 : 0;
+}
+CDL_FN(c_marubozu) {
+  return (b.RB(0) > b.AVG(BODY_LONG, 0) && b.US(0) < b.AVG(SHADOW_VERY_SHORT, 0) &&
+          b.LS(0) < b.AVG(SHADOW_VERY_SHORT, 0)) ? b.COL(0) * 100 : 0;
+}
+CDL_FN(c_matching_low) {
+  return (b.COL(1) == -1 && b.COL(0) == -1 && b.C(0) <= b.C(1) + b.AVG(EQUAL, 1) &&
+          b.C(0) >= b.C(1) - b.AVG(EQUAL, 1)) ? 100 : 0;
+}
+CDL_FN(c_mat_hold) {
+  const double pen = 0.5;
+  return (b.RB(4) > b.AVG(BODY_LONG, 4) && b.RB(3) < b.AVG(BODY_SHORT, 3) && b.RB(2) < b.AVG(BODY_SHORT, 2) &&
+          b.RB(1) < b.AVG(BODY_SHORT, 1) && b.COL(4) == 1 && b.COL(3) == -1 && b.COL(0) == 1 && b.BGAP_UP(3, 4) &&
+          b.BOT(2) < b.C(4) && b.BOT(1) < b.C(4) && b.BOT(2) > b.C(4) - b.RB(4) * pen &&
+          b.BOT(1) > b.C(4) - b.RB(4) * pen && fmaxf(b.C(2), b.O(2)) < b.O(3) &&
+          fmaxf(b.C(1), b.O(1)) < fmaxf(b.C(2), b.O(2)) && b.O(0) > b.C(1) &&
+          b.C(0) > fmaxf(fmaxf(b.H(3), b.H(2)), b.H(1))) ? 100 : 0;
+}
+CDL_FN(c_on_neck) {
+  return (b.COL(1) == -1 && b.RB(1) > b.AVG(BODY_LONG, 1) && b.COL(0) == 1 && b.O(0) < b.L(1) &&
+          b.C(0) <= b.L(1) + b.AVG(EQUAL, 1) && b.C(0) >= b.L(1) - b.AVG(EQUAL, 1)) ? -100 : 0;
+}
+CDL_FN(c_piercing) {
+  return (b.COL(1) == -1 && b.RB(1) > b.AVG(BODY_LONG, 1) && b.COL(0) == 1 && b.RB(0) > b.AVG(BODY_LONG, 0) &&
+          b.O(0) < b.L(1) && b.C(0) < b.O(1) && (double)b.C(0) > (double)b.C(1) + b.RB(1) * 0.5) ? 100 : 0;
+}
+CDL_FN(c_rickshaw_man) {
+  const double mid = (double)b.L(0) + ((double)b.H(0) - (double)b.L(0)) / 2.0;
+  return (b.RB(0) <= b.AVG(BODY_DOJI, 0) && b.LS(0) > b.AVG(SHADOW_LONG, 0) && b.US(0) > b.AVG(SHADOW_LONG, 0) &&
+          (double)b.BOT(0) <= mid + b.AVG(NEAR, 0) && (double)b.TOP(0) >= mid - b.AVG(NEAR, 0)) ? 100 : 0;
+}
+CDL_FN(c_rise_fall3_methods) {
+  const int c4 = b.COL(4);
+  return (b.RB(4) > b.AVG(BODY_LONG, 4) && b.RB(3) < b.AVG(BODY_SHORT, 3) && b.RB(2) < b.AVG(BODY_SHORT, 2) &&
+          b.RB(1) < b.AVG(BODY_SHORT, 1) && b.RB(0) > b.AVG(BODY_LONG, 0) && c4 == -b.COL(3) &&
+          b.COL(3) == b.COL(2) && b.COL(2) == b.COL(1) && b.COL(1) == -b.COL(0) && b.BOT(3) < b.H(4) &&
+          b.TOP(3) > b.L(4) && b.BOT(2) < b.H(4) && b.TOP(2) > b.L(4) && b.BOT(1) < b.H(4) && b.TOP(1) > b.L(4) &&
+          b.C(2) * c4 < b.C(3) * c4 && b.C(1) * c4 < b.C(2) * c4 && b.O(0) * c4 > b.C(1) * c4 &&
+          b.C(0) * c4 > b.C(4) * c4) ? 100 * c4 : 0;
+}
+CDL_FN(c_separating_lines) {
+  if (b.COL(1) == -b.COL(0) && b.O(0) <= b.O(1) + b.AVG(EQUAL, 1) && b.O(0) >= b.O(1) - b.AVG(EQUAL, 1) &&
+      b.RB(0) > b.AVG(BODY_LONG, 0) &&
+      ((b.COL(0) == 1 && b.LS(0) < b.AVG(SHADOW_VERY_SHORT, 0)) ||
+       (b.COL(0) == -1 && b.US(0) < b.AVG(SHADOW_VERY_SHORT, 0))))
+    return b.COL(0) * 100;
+  return 0;
+}
+CDL_FN(c_shooting_star) {
+  return (b.RB(0) < b.AVG(BODY_SHORT, 0) && b.US(0) > b.AVG(SHADOW_LONG, 0) &&
+          b.LS(0) < b.AVG(SHADOW_VERY_SHORT, 0) && b.BGAP_UP(0, 1)) ? -100 : 0;
+}
+CDL_FN(c_short_line) {
+  return (b.RB(0) < b.AVG(BODY_SHORT, 0) && b.US(0) < b.AVG(SHADOW_SHORT, 0) && b.LS(0) < b.AVG(SHADOW_SHORT, 0))
+             ? b.COL(0) * 100 : 0;
+}
+CDL_FN(c_spinning_top) {
+  return (b.RB(0) < b.AVG(BODY_SHORT, 0) && b.US(0) > b.RB(0) && b.LS(0) > b.RB(0)) ? b.COL(0) * 100 : 0;
+}
+CDL_FN(c_stalled_pattern) {
+  return (b.COL(2) == 1 && b.COL(1) == 1 && b.COL(0) == 1 && b.C(0) > b.C(1) && b.C(1) > b.C(2) &&
+          b.RB(2) > b.AVG(BODY_LONG, 2) && b.RB(1) > b.AVG(BODY_LONG, 1) && b.US(1) < b.AVG(SHADOW_VERY_SHORT, 1) &&
+          b.O(1) > b.O(2) && b.O(1) <= b.C(2) + b.AVG(NEAR, 2) && b.RB(0) < b.AVG(BODY_SHORT, 0) &&
+          b.O(0) >= b.C(1) - b.RB(0) - b.AVG(NEAR, 1)) ? -100 : 0;
+}
+CDL_FN(c_stick_sandwich) {
+  return (b.COL(2) == -1 && b.COL(1) == 1 && b.COL(0) == -1 && b.L(1) > b.C(2) &&
+          (double)b.C(0) <= (double)b.C(2) + b.AVG(EQUAL, 2) &&
+          (double)b.C(0) >= (double)b.C(2) - b.AVG(EQUAL, 2)) ? 100 : 0;
+}
+CDL_FN(c_takuri) {
+  return (b.RB(0) <= b.AVG(BODY_DOJI, 0) && b.US(0) < b.AVG(SHADOW_VERY_SHORT, 0) &&
+          b.LS(0) > b.AVG(SHADOW_VERY_LONG, 0)) ? 100 : 0;
+}
+CDL_FN(c_tasuki_gap) {
+  if ((b.BGAP_UP(1, 2) && b.COL(1) == 1 && b.COL(0) == -1 && b.O(0) < b.C(1) && b.O(0) > b.O(1) &&
+       b.C(0) < b.O(1) && b.C(0) > fmaxf(b.C(2), b.O(2)) && fabs(b.RB(1) - b.RB(0)) < b.AVG(NEAR, 1)) ||
+      (b.BGAP_DN(1, 2) && b.COL(1) == -1 && b.COL(0) == 1 && b.O(0) < b.O(1) && b.O(0) > b.C(1) &&
+       b.C(0) > b.O(1) && b.C(0) < fminf(b.C(2), b.O(2)) && fabs(b.RB(1) - b.RB(0)) < b.AVG(NEAR, 1)))
+    return b.COL(1) * 100;
+  return 0;
+}
+CDL_FN(c_thrusting) {
+  return (b.COL(1) == -1 && b.RB(1) > b.AVG(BODY_LONG, 1) && b.COL(0) == 1 && b.O(0) < b.L(1) &&
+          b.C(0) > b.C(1) + b.AVG(EQUAL, 1) && (double)b.C(0) <= (double)b.C(1) + b.RB(1) * 0.5) ? -100 : 0;
+}
+// TA-Lib keeps the doji average anchored at the first candle for all three.
+CDL_FN(c_tristar) {
+  const double d = b.AVG(BODY_DOJI, 2);
+  if (b.RB(2) <= d && b.RB(1) <= d && b.RB(0) <= d) {
+    int out = 0;
+    if (b.BGAP_UP(1, 2) && fmaxf(b.O(0), b.C(0)) < fmaxf(b.O(1), b.C(1))) out = -100;
+    if (b.BGAP_DN(1, 2) && fminf(b.O(0), b.C(0)) > fminf(b.O(1), b.C(1))) out = 100;
+    return out;
+  }
+  return 0;
+}
+CDL_FN(c_unique_3_river) {
+  return (b.RB(2) > b.AVG(BODY_LONG, 2) && b.COL(2) == -1 && b.COL(1) == -1 && b.C(1) > b.C(2) && b.O(1) <= b.O(2) &&
+          b.L(1) < b.L(2) && b.RB(0) < b.AVG(BODY_SHORT, 0) && b.COL(0) == 1 && b.O(0) > b.L(1)) ? 100 : 0;
+}
+CDL_FN(c_upside_gap_2_crows) {
+  return (b.COL(2) == 1 && b.RB(2) > b.AVG(BODY_LONG, 2) && b.COL(1) == -1 && b.RB(1) <= b.AVG(BODY_SHORT, 1) &&
+          b.BGAP_UP(1, 2) && b.COL(0) == -1 && b.O(0) > b.O(1) && b.C(0) < b.C(1) && b.C(0) > b.C(2)) ? -100 : 0;
+}
+CDL_FN(c_xside_gap_3_methods) {
+  if (b.COL(2) == b.COL(1) && b.COL(1) == -b.COL(0) && b.O(0) < fmaxf(b.C(1), b.O(1)) &&
+      b.O(0) > fminf(b.C(1), b.O(1)) && b.C(0) < fmaxf(b.C(2), b.O(2)) && b.C(0) > fminf(b.C(2), b.O(2)) &&
+      ((b.COL(2) == 1 && b.BGAP_UP(1, 2)) || (b.COL(2) == -1 && b.BGAP_DN(1, 2))))
+    return b.COL(2) * 100;
+  return 0;
+}
+#undef CDL_FN
+
+// Pattern k in the order of the ct_cdl_*_batch_d declarations.
+__device__ __forceinline__ int cdl_eval(int k, const Bars& b) {
+  switch (k) {
+    case 0: return c_doji(b);
+    case 1: return c_hammer(b);
+    case 2: return c_inverted_hammer(b);
+    case 3: case 4: return c_engulfing(b);  // legacy bullish / bearish split
+    case 5: return c_three_white_soldiers(b);
+    case 6: return c_abandoned_baby(b);
+    case 7: return c_advance_block(b);
+    case 8: return c_belt_hold(b);
+    case 9: return c_breakaway(b);
+    case 10: return c_two_crows(b);
+    case 11: return c_three_black_crows(b);
+    case 12: return c_three_inside(b);
+    case 13: return c_three_outside(b);
+    case 14: return c_three_line_strike(b);
+    case 15: return c_three_stars_in_south(b);
+    case 16: return c_closing_marubozu(b);
+    case 17: return c_conceal_baby_swallow(b);
+    case 18: return c_counterattack(b);
+    case 19: return c_dark_cloud_cover(b);
+    case 20: return c_doji_star(b);
+    case 21: return c_dragonfly_doji(b);
+    case 22: return c_engulfing(b);
+    case 23: return c_evening_doji_star(b);
+    case 24: return c_evening_star(b);
+    case 25: return c_gap_side_side_white(b);
+    case 26: return c_gravestone_doji(b);
+    case 27: return c_hanging_man(b);
+    case 28: return c_harami(b);
+    case 29: return c_harami_cross(b);
+    case 30: return c_high_wave(b);
+    case 31: return c_hikkake(b);
+    case 32: return c_hikkake_mod(b);
+    case 33: return c_homing_pigeon(b);
+    case 34: return c_identical_three_crows(b);
+    case 35: return c_in_neck(b);
+    case 36: return c_kicking(b);
+    case 37: return c_kicking_by_length(b);
+    case 38: return c_ladder_bottom(b);
+    case 39: return c_long_legged_doji(b);
+    case 40: return c_long_line(b);
+    case 41: return c_marubozu(b);
+    case 42: return c_matching_low(b);
+    case 43: return c_mat_hold(b);
+    case 44: return c_morning_doji_star(b);
+    case 45: return c_morning_star(b);
+    case 46: return c_on_neck(b);
+    case 47: return c_piercing(b);
+    case 48: return c_rickshaw_man(b);
+    case 49: return c_rise_fall3_methods(b);
+    case 50: return c_separating_lines(b);
+    case 51: return c_shooting_star(b);
+    case 52: return c_short_line(b);
+    case 53: return c_spinning_top(b);
+    case 54: return c_stalled_pattern(b);
+    case 55: return c_stick_sandwich(b);
+    case 56: return c_takuri(b);
+    case 57: return c_tasuki_gap(b);
+    case 58: return c_thrusting(b);
+    case 59: return c_tristar(b);
+    case 60: return c_unique_3_river(b);
+    case 61: return c_upside_gap_2_crows(b);
+    case 62: return c_xside_gap_3_methods(b);
+  }
+  return 0;
+}
+
+// Warm-up lengths (bars before them are 0), order as above.
+__device__ __constant__ const unsigned char kCdlLookbackDev[63] = {
+    10, 11, 11, 1, 1, 12, 12, 12, 10, 14, 12, 13, 12, 3, 8, 12, 10, 13, 11, 11, 11, 10, 2, 12, 12, 7, 10, 11, 11, 11,
+    10, 5, 10, 11, 12, 11, 11, 11, 14, 10, 10, 10, 6, 14, 12, 12, 11, 11, 10, 14, 11, 11, 10, 10, 12, 7, 10, 7, 11, 12,
+    12, 12, 2};
+
+// Candle job: pattern subset `cdl_mask` of one group. `writer` fills the
+// group's trailing-sum table; `bar_id`/`nthreads` name the barrier shared by
+// the group's candle warps.
+__device__ void sp_cdl_job(Driver& drv, const Job& j, const Stage& st, int lane, const CdlTable& tbl, bool writer,
+                           int bar_id, int nthreads) {
+  const int po = j.in[0], ph = j.in[1], pl = j.in[2], pc = j.in[3];
+  for (int c = 0; c < drv.nchunks; ++c) {
+    drv.begin(c);
+    const Row rw = drv.row(c);
+    const float* Op = drv.pptr(c, po);
+    const float* Hp = drv.pptr(c, ph);
+    const float* Lp = drv.pptr(c, pl);
+    const float* Cp = drv.pptr(c, pc);
+    const int lim = (int)min((long long)C, rw.n - rw.t0);
+    if (writer) {
+      for (int slot = 0; slot < 4; ++slot) {
+        const int per = kSlotPeriod[slot];
+        const int type = slot == 0 ? CR_BODY : (slot == 2 ? CR_SHADOW : CR_HL);
+        auto rg = [&](int r) { return cdl_range(type, Op[r], Hp[r], Lp[r], Cp[r]); };
+        const int a0 = -kCdlBack;
+        double s = 0.0;
+        for (int i = 1; i <= per; ++i) s += rg(a0 - i);
+        for (int a = a0; a < lim; ++a) {
+          tbl.at(slot, lane, a) = s;
+          s += rg(a) - rg(a - per);
+        }
+      }
+    }
+    asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
+    Bars b;
+    b.tb = &tbl;
+    b.lane = lane;
+    b.Op = Op; b.Hp = Hp; b.Lp = Lp; b.Cp = Cp;
+    int* ibuf = reinterpret_cast<int*>(st.buf);
+    uint64_t mask = j.cdl_mask;
+    while (mask) {
+      const int k = __ffsll((long long)mask) - 1;
+      mask &= mask - 1;
+      const int lb = kCdlLookbackDev[k];
+      for (int r = 0; r < lim; ++r) {
+        b.r = r;
+        b.t = rw.t0 + r;
+        const int v = b.t >= lb ? cdl_eval(k, b) : 0;
+        if (j.cdl_int32) ibuf[lane * (C + 1) + r] = v;
+        else st.buf[lane * (C + 1) + r] = (float)v;
+      }
+      if (j.cdl_int32) st.flush_int(0, (int*)j.out[0] + (long long)k * j.cdl_stride, drv.my_base, drv.my_n, rw.t0, lane);
+      else st.flush(0, (float*)j.out[0] + (long long)k * j.cdl_stride, drv.my_base, drv.my_n, rw.t0, lane);
+    }
+    drv.end(c);
+  }
+}
+
+}  // namespace sp
+}  // namespace tb

@@ -78,3 +78,14 @@ def call_batch_d(name: str, dplanes: dict, params: dict, stream=0, outs=None):
 def to_np(ts):
     torch.cuda.synchronize()
     return [t.cpu().numpy() for t in ts]
+
+
+def call_cdl(k: int, dplanes: dict, name: str, stream=0):
+    """ct_cdl_<name>_batch_d for pattern k (float signal plane)."""
+    S, T = dplanes["open"].shape
+    out = torch.full((S, T), 12345.0, device=dplanes["open"].device)
+    sym = f"ct_cdl_{name}_batch_d"
+    args = [ct.c_void_p(dplanes[p].data_ptr()) for p in ("open", "high", "low", "close")]
+    args += [ct.c_void_p(out.data_ptr()), ct.c_int(T), ct.c_int(S), ct.c_int(0), ct.c_void_p(stream)]
+    tb.call_status(getattr(tb.get_lib(), sym)(*args), sym)
+    return out

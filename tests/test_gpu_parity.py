@@ -37,9 +37,17 @@ def run_case(name, params, shape, seed=6):
     return stats
 
 
+@pytest.fixture(params=["sp", "ws"])
+def mode(request):
+    """Both engines: series-parallel (thread per series) and warp-per-series."""
+    os.environ["TACUDA_B200_MODE"] = request.param
+    yield request.param
+    del os.environ["TACUDA_B200_MODE"]
+
+
 @pytest.mark.parametrize("name", sorted(SPECS))
 @pytest.mark.parametrize("shape", SHAPES)
-def test_family_matches_oracle(name, shape):
+def test_family_matches_oracle(name, shape, mode):
     run_case(name, DEFAULTS[name], shape)
 
 
@@ -72,11 +80,11 @@ VARIANTS = {
 
 
 @pytest.mark.parametrize("name,params", [(n, p) for n, ps in VARIANTS.items() for p in ps])
-def test_parameter_corpus(name, params):
+def test_parameter_corpus(name, params, mode):
     run_case(name, params, (7, 1300), seed=17)
 
 
-def test_fused_pass_matches_oracle_and_single_calls():
+def test_fused_pass_matches_oracle_and_single_calls(mode):
     S, T = 67, 700
     d = synthetic.ohlcv(S, T, seed=8)
     dp = device_planes(d)
@@ -137,7 +145,7 @@ def test_row_independence(name):
         del os.environ["TACUDA_B200_BARS_PER_LANE"]
 
 
-def test_known_answers_on_gpu():
+def test_known_answers_on_gpu(mode):
     flat = {k: np.full((3, 129), 100.0 if k != "volume" else 1000.0, np.float32)
             for k in ("open", "high", "low", "close", "volume")}
     dp = device_planes(flat)
@@ -159,7 +167,7 @@ def test_known_answers_on_gpu():
     np.testing.assert_array_equal(out[:, 2:], -25.0)
 
 
-def test_leading_nan_and_interior_nan_semantics():
+def test_leading_nan_and_interior_nan_semantics(mode):
     d = synthetic.ohlcv(5, 600, seed=12)
     for v in d.values():
         v[1, :37] = np.nan
@@ -173,7 +181,7 @@ def test_leading_nan_and_interior_nan_semantics():
             compare(g, r, f"nan {name}[{i}]")
 
 
-def test_ragged_plan_matches_oracle():
+def test_ragged_plan_matches_oracle(mode):
     lengths = synthetic.ragged_lengths(300, 1, 5000, seed=3)
     lengths[:5] = [0, 1, 2, 1024, 4097]
     planes, off = synthetic.ragged_ohlcv(lengths, seed=4)
@@ -197,7 +205,7 @@ def test_ragged_plan_matches_oracle():
     plan.close()
 
 
-def test_graph_capture_replay_equals_eager():
+def test_graph_capture_replay_equals_eager(mode):
     S, T = 67, 234
     d = synthetic.ohlcv(S, T, seed=6)
     dp = device_planes(d)
