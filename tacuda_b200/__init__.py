@@ -72,7 +72,7 @@ def _load() -> ct.CDLL:
     lib.ct_b200_plan_create.argtypes = [ct.POINTER(ctB200Job), _I, _P, _I, ct.c_int64, ct.POINTER(_P)]
     lib.ct_b200_plan_execute.argtypes = [_P, ct.POINTER(ctB200Series), ct.POINTER(ctB200Job), _I, _P]
     lib.ct_b200_plan_autotune.argtypes = [_P, ct.POINTER(ctB200Series), ct.POINTER(ctB200Job), _I, _P]
-    lib.ct_b200_plan_describe.argtypes = [_P, ct.POINTER(_I), ct.POINTER(_I), ct.POINTER(_I)]
+    lib.ct_b200_plan_describe.argtypes = [_P, ct.POINTER(_I), ct.POINTER(_I), ct.POINTER(_I), ct.POINTER(_I)]
     lib.ct_b200_plan_destroy.argtypes = [_P]
     lib.ct_b200_cdl_batch_d.argtypes = [_P, _P, _P, _P, _P, _I, _I, ct.c_uint64, _P]
     return lib
@@ -275,10 +275,10 @@ class Plan:
                     "ct_b200_plan_autotune")
 
     def describe(self) -> dict:
-        k, w, b = _I(), _I(), _I()
-        call_status(get_lib().ct_b200_plan_describe(self.handle, ct.byref(k), ct.byref(w), ct.byref(b)),
-                    "ct_b200_plan_describe")
-        return {"bars_per_lane": k.value, "warps_per_block": w.value, "max_blocks": b.value}
+        m, k, w, b = _I(), _I(), _I(), _I()
+        call_status(get_lib().ct_b200_plan_describe(self.handle, ct.byref(m), ct.byref(k), ct.byref(w),
+                                                    ct.byref(b)), "ct_b200_plan_describe")
+        return {"mode": m.value, "bars_per_lane": k.value, "warps_per_block": w.value, "max_blocks": b.value}
 
     def close(self) -> None:
         if self.handle:

@@ -173,7 +173,7 @@ ctStatus_t finish(cudaStream_t stream, const char* who) {
 ctStatus_t launch(Launch& L, long long total, long long maxlen, const tb::SchedulePlan* forced, cudaStream_t stream,
                   const char* who, tb::LaunchStats* stats = nullptr) {
   const tb::SchedulePlan plan = forced ? *forced : tb::plan_for(L, total, maxlen);
-  const cudaError_t e = tb::launch_batch(L, plan, stream, stats);
+  const cudaError_t e = tb::launch_batch(L, plan, total, stream, stats);
   if (e != cudaSuccess) return cuda_fail(CT_STATUS_KERNEL_FAILED, who, e);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return CT_STATUS_SUCCESS;
@@ -764,12 +764,34 @@ ctStatus_t ct_b200_plan_autotune(ctB200Plan* plan, const ctB200Series* series, c
   cudaEventCreate(&e1);
   float best = 1e30f;
   tb::SchedulePlan bestPlan = plan->sched;
-  for (int ki : ks) {
-    if (ki == 4 && plan->maxlen > 4096) continue;
-    for (int wi : ws) {
-      tb::SchedulePlan cand;
-      cand.k = ki;
-      cand.warps_per_block = wi;
+  // candidates: warp-per-series and look-back engines over round widths and
+  // block sizes (candles excepted), the series-parallel engine over group counts
+  bool cdl = false;
+  for (int j = 0; j < plan->njobs; ++j) cdl = cdl || plan->jobs[j].family == tb::F_CDL;
+  std::vector<tb::SchedulePlan> cands;
+  if (!cdl)
+    for (int mode : {0, 2})
+      for (int ki : ks) {
+        if (ki == 4 && plan->maxlen > 4096) continue;
+        if (mode == 2 && plan->maxlen < 4ll * 32 * ki) continue;
+        for (int wi : ws) {
+          tb::SchedulePlan cand;
+          cand.mode = mode;
+          cand.k = ki;
+          cand.warps_per_block = wi;
+          cands.push_back(cand);
+        }
+      }
+  for (int g : {1, 2, 4, 8}) {
+    if (g * plan->njobs > tb::kMaxJobs) continue;
+    tb::SchedulePlan cand;
+    cand.mode = 1;
+    cand.groups = g;
+    cands.push_back(cand);
+  }
+  (void)ws;
+  for (const tb::SchedulePlan& cand : cands) {
+    {
       ctStatus_t st = plan_launch(plan, series, jobs, numJobs, cand, stream, who, nullptr);  // warm-up
       if (st != CT_STATUS_SUCCESS) continue;
       cudaEventRecord(e0, stream);
@@ -794,9 +816,11 @@ ctStatus_t ct_b200_plan_autotune(ctB200Plan* plan, const ctB200Series* series, c
   return CT_STATUS_SUCCESS;
 }
 
-ctStatus_t ct_b200_plan_describe(const ctB200Plan* plan, int* barsPerLane, int* warpsPerBlock, int* blocks) {
+ctStatus_t ct_b200_plan_describe(const ctB200Plan* plan, int* engine, int* barsPerLane, int* warpsPerBlock,
+                                 int* blocks) {
   clear_error();
   if (!plan) return fail(CT_STATUS_INVALID_ARGUMENT, "ct_b200_plan_describe: null plan");
+  if (engine) *engine = plan->sched.mode;
   if (barsPerLane) *barsPerLane = plan->sched.k;
   if (warpsPerBlock) *warpsPerBlock = plan->sched.warps_per_block;
   if (blocks) *blocks = plan->sched.max_blocks;

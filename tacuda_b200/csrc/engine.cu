@@ -100,6 +100,80 @@ __global__ void __launch_bounds__(256) batch_kernel(const __grid_constant__ Laun
   const int W = gridDim.x * lay.warps;
   const int gw = blockIdx.x * lay.warps + warp;
   const int span = L.halo + TILE;
+  auto stage_round_inputs = [&](int t0) {
+    c.t0 = t0;
+    c.L = min(TILE, c.n - t0);
+    // stage the input planes with asynchronous copies, all in flight at once
+    // (bars outside the row read as 0; no family reads them for an output)
+    const int tlo = t0 - L.halo;
+    for (int p = 0; p < P_COUNT; ++p) {
+      if (!(L.plane_mask & (1u << p))) continue;
+      const float* src = L.plane[p] + c.base;
+      float* dst = planes + lay.plane_slot[p] * lay.plane_len;
+      for (int i = lane; i < span; i += 32) {
+        const int t = tlo + i;
+        const bool ok = t >= 0 && t < c.n;
+        cp_async4(dst + pad(i), ok ? src + t : src, ok);
+      }
+    }
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+    __syncwarp();
+    if (L.need_tp) {
+      const float* hp = c.plane(P_HIGH);
+      const float* lp = c.plane(P_LOW);
+      const float* cp = c.plane(P_CLOSE);
+      double* tpp = reinterpret_cast<double*>(c.sm + lay.off_tp);
+      for (int i = lane; i < span; i += 32)
+        tpp[i + (i >> 4)] = ((double)hp[pad(i)] + (double)lp[pad(i)] + (double)cp[pad(i)]) / 3.0;
+    }
+    __syncwarp();
+  };
+  if (L.lb) {
+    // Look-back mode: tiles of one round taken in order from a global counter;
+    // the carries between tiles come from the descriptors, not shared memory.
+    c.lb = true;
+    c.lbs = L.lb_nslots;
+    c.err = L.err;
+    const long long tps = L.lb_tile_start ? 0 : (L.T + TILE - 1) / TILE;
+    const long long ntiles = L.lb_tile_start ? L.lb_tile_start[L.S] : L.lb_tiles;
+    for (;;) {
+      unsigned long long g = 0;
+      if (lane == 0) g = atomicAdd(L.lb_counter, 1ull);
+      g = __shfl_sync(kFull, g, 0);
+      if ((long long)g >= ntiles) break;
+      long long s, first;
+      if (L.lb_tile_start) {
+        long long lo = 0, hi = L.S;  // largest s with tile_start[s] <= g
+        while (lo < hi) {
+          const long long mid = (lo + hi + 1) >> 1;
+          if (L.lb_tile_start[mid] <= (long long)g) lo = mid;
+          else hi = mid - 1;
+        }
+        s = lo;
+        first = L.lb_tile_start[s];
+        c.base = L.offsets[s];
+        c.n = (int)(L.offsets[s + 1] - c.base);
+      } else {
+        s = (long long)g / tps;
+        first = s * tps;
+        c.base = s * L.T;
+        c.n = (int)L.T;
+      }
+      c.tile = (int)((long long)g - first);
+      c.lbd = L.lb_desc + first * L.lb_nslots;
+      stage_round_inputs(c.tile * TILE);
+      for (int j = 0; j < L.njobs; ++j) {
+        Carry cy;
+        cy.f = -1;
+#pragma unroll
+        for (int v = 0; v < 10; ++v) cy.v[v] = 0.0;
+        run_job<K>(c, L.jobs[j], cy);
+        __syncwarp();
+      }
+    }
+    return;
+  }
+  c.lb = false;
   for (int pass = 0;; ++pass) {
     const long long idx = (long long)pass * W + ((pass & 1) ? (W - 1 - gw) : gw);
     if (idx >= L.S) break;
@@ -119,32 +193,7 @@ __global__ void __launch_bounds__(256) batch_kernel(const __grid_constant__ Laun
     }
     __syncwarp();
     for (int t0 = 0; t0 < c.n; t0 += TILE) {
-      c.t0 = t0;
-      c.L = min(TILE, c.n - t0);
-      // stage the input planes with asynchronous copies, all in flight at once
-      // (bars outside the row read as 0; no family reads them for an output)
-      const int tlo = t0 - L.halo;
-      for (int p = 0; p < P_COUNT; ++p) {
-        if (!(L.plane_mask & (1u << p))) continue;
-        const float* src = L.plane[p] + c.base;
-        float* dst = planes + lay.plane_slot[p] * lay.plane_len;
-        for (int i = lane; i < span; i += 32) {
-          const int t = tlo + i;
-          const bool ok = t >= 0 && t < c.n;
-          cp_async4(dst + pad(i), ok ? src + t : src, ok);
-        }
-      }
-      asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
-      __syncwarp();
-      if (L.need_tp) {
-        const float* hp = c.plane(P_HIGH);
-        const float* lp = c.plane(P_LOW);
-        const float* cp = c.plane(P_CLOSE);
-        double* tpp = reinterpret_cast<double*>(c.sm + lay.off_tp);
-        for (int i = lane; i < span; i += 32)
-          tpp[i + (i >> 4)] = ((double)hp[pad(i)] + (double)lp[pad(i)] + (double)cp[pad(i)]) / 3.0;
-      }
-      __syncwarp();
+      stage_round_inputs(t0);
       for (int j = 0; j < L.njobs; ++j) {
         Carry cy = carry[j];
         run_job<K>(c, L.jobs[j], cy);
@@ -245,9 +294,58 @@ __global__ void __launch_bounds__(768) sp_kernel(const __grid_constant__ Launch 
   }
 }
 
+// First look-back tile of every ragged series: tile_start[s] = sum over
+// earlier series of ceil(n / tile), tile_start[S] = total. One block.
+__global__ void __launch_bounds__(1024) lb_tile_start_kernel(const long long* offsets, int S, int tile,
+                                                             long long* tile_start) {
+  __shared__ long long part[1024];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const long long per = ((long long)S + nt - 1) / nt;
+  const long long lo = min((long long)S, (long long)tid * per), hi = min((long long)S, lo + per);
+  long long sum = 0;
+  for (long long s = lo; s < hi; ++s) sum += (offsets[s + 1] - offsets[s] + tile - 1) / tile;
+  part[tid] = sum;
+  __syncthreads();
+  if (tid == 0) {
+    long long acc = 0;
+    for (int i = 0; i < nt; ++i) {
+      const long long v = part[i];
+      part[i] = acc;
+      acc += v;
+    }
+    tile_start[S] = acc;
+  }
+  __syncthreads();
+  long long acc = part[tid];
+  for (long long s = lo; s < hi; ++s) {
+    tile_start[s] = acc;
+    acc += (offsets[s + 1] - offsets[s] + tile - 1) / tile;
+  }
+}
+
 // ------------------------------------------------------------------ host side
 
 namespace {
+
+// Look-back descriptor slots of a job: one per first-index carry and one per
+// recurrence stage, in the order the round functions address them.
+int lb_slots(const Job& j) {
+  switch (j.family) {
+    case F_EMA: return 2;
+    case F_DEMA: return 3;
+    case F_TEMA: return 4;
+    case F_T3: return 7;
+    case F_RSI: return 2;
+    case F_MACD: return 4;
+    case F_ATR: case F_NATR: return 1;
+    case F_ADX: return 2;
+    case F_DX: return 1;
+    case F_OBV: case F_AD: return 1;
+    case F_ADOSC: return 3;
+    case F_MIN: case F_MAX: case F_CORREL: return 1;
+    default: return 0;
+  }
+}
 
 int job_halo(const Job& j) {
   switch (j.family) {
@@ -378,7 +476,9 @@ cudaError_t launch_k(Launch& L, const SchedulePlan& plan, cudaStream_t stream, L
     }
   }
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
-  long long want = (L.S + warps - 1) / warps;
+  long long units = L.S;
+  if (L.lb) units = L.lb_tiles;
+  long long want = (units + warps - 1) / warps;
   long long cap = (long long)per_sm * di.sms;
   if (plan.max_blocks > 0) cap = std::min<long long>(cap, plan.max_blocks);
   const int blocks = (int)std::max<long long>(1, std::min(want, cap));
@@ -487,7 +587,52 @@ int max_lookback_halo(const Launch& L) {
   return h;
 }
 
-cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, cudaStream_t stream, LaunchStats* stats) {
+template <int K>
+cudaError_t launch_lookback(Launch& L, const SchedulePlan& plan, long long total_bars, cudaStream_t stream,
+                            LaunchStats* stats) {
+  constexpr int TILE = 32 * K;
+  int nslots = 0;
+  for (int j = 0; j < L.njobs; ++j) {
+    L.jobs[j].lb_slot = nslots;
+    nslots += lb_slots(L.jobs[j]);
+  }
+  if (nslots == 0) nslots = 1;
+  // bound on the tile count (exact for uniform rows)
+  const long long ntiles = L.offsets ? total_bars / TILE + L.S : (long long)L.S * ((L.T + TILE - 1) / TILE);
+  const size_t head = 256;
+  const size_t ts_bytes = L.offsets ? (((size_t)(L.S + 1) * 8 + 255) & ~(size_t)255) : 0;
+  const size_t desc_bytes = (size_t)ntiles * nslots * sizeof(LbDesc);
+  unsigned char* scratch = nullptr;
+  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&scratch), head + ts_bytes + desc_bytes, stream);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(scratch, 0, head + ts_bytes + desc_bytes, stream);
+  if (e == cudaSuccess) {
+    L.lb = 1;
+    L.lb_counter = reinterpret_cast<unsigned long long*>(scratch);
+    L.err = reinterpret_cast<int*>(scratch + 8);
+    L.lb_tile_start = L.offsets ? reinterpret_cast<long long*>(scratch + head) : nullptr;
+    L.lb_desc = reinterpret_cast<LbDesc*>(scratch + head + ts_bytes);
+    L.lb_nslots = nslots;
+    L.lb_tiles = ntiles;
+    if (L.offsets) {
+      lb_tile_start_kernel<<<1, 1024, 0, stream>>>(L.offsets, L.S, TILE, L.lb_tile_start);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = launch_k<K>(L, plan, stream, stats);
+    if (e == cudaSuccess && stream == 0) {
+      // synchronous calls report a look-back wait that ran out
+      int herr = 0;
+      e = cudaMemcpyAsync(&herr, L.err, sizeof(int), cudaMemcpyDeviceToHost, stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+      if (e == cudaSuccess && herr != 0) e = cudaErrorLaunchTimeout;
+    }
+  }
+  const cudaError_t ef = cudaFreeAsync(scratch, stream);
+  return e != cudaSuccess ? e : ef;
+}
+
+cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, long long total_bars, cudaStream_t stream,
+                         LaunchStats* stats) {
   unsigned mask = 0;
   int need_tp = 0;
   for (int j = 0; j < L.njobs; ++j) {
@@ -500,6 +645,14 @@ cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, cudaStream_t strea
   const int h = max_lookback_halo(L);
   L.halo = ((h + 31) / 32) * 32;
   if (plan.mode == 1) return launch_sp(L, plan, stream, stats);
+  L.lb = 0;
+  if (plan.mode == 2) {
+    switch (plan.k) {
+      case 4: return launch_lookback<4>(L, plan, total_bars, stream, stats);
+      case 16: return launch_lookback<16>(L, plan, total_bars, stream, stats);
+      default: return launch_lookback<8>(L, plan, total_bars, stream, stats);
+    }
+  }
   switch (plan.k) {
     case 4: return launch_k<4>(L, plan, stream, stats);
     case 16: return launch_k<16>(L, plan, stream, stats);

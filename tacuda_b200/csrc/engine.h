@@ -35,7 +35,10 @@ struct Job {
   long long cdl_stride;
   int cdl_int32;
   int halo;         // bars of history this job reads before a round
+  int lb_slot;      // first look-back descriptor slot of this job (look-back mode)
 };
+
+struct LbDesc;
 
 struct Launch {
   const float* plane[P_COUNT];
@@ -50,6 +53,13 @@ struct Launch {
   int* sched;                // [0] series counter, [1] finished warps (self-resetting)
   int total_warps;
   int* err;                  // device error word (0 = ok)
+  // look-back mode: series split into one-round tiles taken in order
+  int lb;
+  unsigned long long* lb_counter;  // next tile (zeroed before the launch)
+  long long lb_tiles;        // total tiles
+  long long* lb_tile_start;  // ragged: first tile of each series (S+1), else nullptr
+  LbDesc* lb_desc;           // lb_tiles * lb_nslots descriptors (zeroed)
+  int lb_nslots;
   Job jobs[kMaxJobs];
 };
 

@@ -14,6 +14,7 @@
 
 #include "common.cuh"
 #include "engine.h"
+#include "lookback.cuh"
 
 namespace tb {
 
@@ -40,6 +41,12 @@ struct Ctx {
   int off_planes, plane_len, off_tp, off_dscr, off_stage, stage_len;
   unsigned slots;  // 4-bit staged slot of each plane
   bool has_tp;
+  // look-back mode: this round is tile `tile` of a series split across warps
+  bool lb;
+  int tile;
+  LbDesc* lbd;       // descriptors of this series' tile 0 (slot 0)
+  long long lbs;     // descriptors per tile
+  int* err;
 
   __device__ __forceinline__ const float* plane(int p) const {
     return reinterpret_cast<const float*>(sm + off_planes) + (int)((slots >> (4 * p)) & 15u) * plane_len;
@@ -76,8 +83,8 @@ struct Ctx {
 // of the row (src/api/BatchFused.cu:34-41 skips a leading NaN run). Resolved
 // once per series; warp-uniform. -1 while the row is all NaN so far.
 template <int K>
-__device__ __forceinline__ int resolve_start(const Ctx<K>& c, const Carry& cy, int plane) {
-  if (cy.f >= 0) return cy.f;
+__device__ __forceinline__ int resolve_start(const Ctx<K>& c, const Carry& cy, int plane, int slot = -1) {
+  if (!c.lb && cy.f >= 0) return cy.f;
   int first = 0x7fffffff;
   for (int k = 0; k < K; ++k) {
     const int t = c.gb0() + k;
@@ -85,7 +92,9 @@ __device__ __forceinline__ int resolve_start(const Ctx<K>& c, const Carry& cy, i
   }
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) first = min(first, __shfl_xor_sync(kFull, first, d));
-  return first == 0x7fffffff ? -1 : first;
+  const int local = first == 0x7fffffff ? -1 : first;
+  if (c.lb) return lb_first_index(c.lbd + slot, c.lbs, c.tile, local, c.err, c.lane);
+  return local;
 }
 
 // Value held after the last valid bar of the round (exact replay state).
@@ -134,6 +143,8 @@ struct EmaStage {
     return fma(beta, y, k * x);
   }
   __device__ __forceinline__ bool ready(int cnt) const { return cnt >= start + p - 1; }
+  // first count whose map is the constant steady one
+  __device__ __forceinline__ int steady_from() const { return p == 1 ? 0 : start + p; }
 };
 
 // Scan one stage over the round. in(t, k) gives the FP64 input of the lane's
@@ -141,7 +152,7 @@ struct EmaStage {
 // series starts). Returns the state after the round.
 template <int K, class Stage, class In, class Sink>
 __device__ __forceinline__ double stage_round(const Ctx<K>& c, int f, const Stage& st,
-                                              double carry, In in, Sink sink) {
+                                              double carry, In in, Sink sink, int slot = -1) {
   const int g0 = c.gb0();
   // inputs of the lane's bars, evaluated once and kept in registers
   double xin[K];
@@ -176,6 +187,17 @@ __device__ __forceinline__ double stage_round(const Ctx<K>& c, int f, const Stag
   }
   warp_scan_affine(A, B, c.lane);
   const double Ae = shfl_excl(A, 1.0, c.lane), Be = shfl_excl(B, 0.0, c.lane);
+  if (c.lb && slot >= 0) {
+    // aggregate of the tile in absolute coordinates (meaningful when the tile
+    // starts past warm-up, where E = 1 before and after every bar)
+    const double tA[1] = {__shfl_sync(kFull, A, 31)};
+    const double tB[1] = {__shfl_sync(kFull, B, 31) + o * (1.0 - tA[0])};
+    const double init[1] = {carry};
+    double Y[1];
+    lb_resolve<1>(c.lbd + slot, c.lbs, c.tile, tA, tB, init, lb_first_steady(f, st.steady_from(), Ctx<K>::TILE), Y,
+                  c.err, c.lane);
+    carry = Y[0];
+  }
   double y = carry;
   if (f >= 0) {
     const int cr = c.t0 - 1 - f, cl = g0 - 1 - f;
@@ -194,7 +216,12 @@ __device__ __forceinline__ double stage_round(const Ctx<K>& c, int f, const Stag
       }
     }
   }
-  return round_tail(c, y);
+  const double tail = round_tail(c, y);
+  if (c.lb && slot >= 0) {
+    const double Y[1] = {tail};
+    lb_publish<1>(c.lbd + slot, c.lbs, c.tile, Y, c.lane);
+  }
+  return tail;
 }
 
 __host__ __device__ inline void talib_ema_coeffs(int p, double& beta, double& k) {
@@ -210,11 +237,12 @@ __host__ __device__ inline void talib_ema_coeffs(int p, double& beta, double& k)
 template <int K>
 __device__ __forceinline__ void ema_round(const Ctx<K>& c, const Job& j, Carry& cy) {
   const int pl = j.in[0];
-  const int f = resolve_start(c, cy, pl);
+  const int f = resolve_start(c, cy, pl, j.lb_slot);
   const EmaStage st{j.ip[0], 0, j.fp[0], j.fp[1], 1.0 / j.ip[0]};
   cy.v[0] = stage_round(
       c, f, st, cy.v[0], [&](int t, int) { return (double)c.x(pl, t); },
-      [&](int k, int cnt, double v) { c.put(0, k, (cnt >= 0 && st.ready(cnt)) ? (float)v : qnan()); });
+      [&](int k, int cnt, double v) { c.put(0, k, (cnt >= 0 && st.ready(cnt)) ? (float)v : qnan()); },
+      j.lb_slot + 1);
   cy.f = f;
   c.flush(0, (float*)j.out[0]);
 }
@@ -228,7 +256,7 @@ __device__ __forceinline__ void ema_round(const Ctx<K>& c, const Job& j, Carry& 
 template <int K>
 __device__ __forceinline__ void cascade_round(const Ctx<K>& c, const Job& j, Carry& cy, int stages) {
   const int pl = j.in[0];
-  const int f = resolve_start(c, cy, pl);
+  const int f = resolve_start(c, cy, pl, j.lb_slot);
   const int p = j.ip[0];
   const double beta = j.fp[0], kk = j.fp[1];
   double c1 = 0, c2 = 0, c3 = 0, c4 = 0;
@@ -263,7 +291,8 @@ __device__ __forceinline__ void cascade_round(const Ctx<K>& c, const Job& j, Car
             }
             c.put(0, k, o);
           }
-        });
+        },
+        j.lb_slot + 1 + s);
     __syncwarp();
   }
   cy.f = f;
@@ -279,7 +308,7 @@ __device__ __forceinline__ void cascade_round(const Ctx<K>& c, const Job& j, Car
 template <int K>
 __device__ __forceinline__ void rsi_round(const Ctx<K>& c, const Job& j, Carry& cy) {
   const int pl = j.in[0];
-  const int f = resolve_start(c, cy, pl);
+  const int f = resolve_start(c, cy, pl, j.lb_slot);
   const int p = j.ip[0];
   const double inv = 1.0 / (double)p, pm1 = (double)(p - 1);
   const double steady = pm1 * inv;
@@ -314,8 +343,20 @@ __device__ __forceinline__ void rsi_round(const Ctx<K>& c, const Job& j, Carry& 
   }
   warp_scan_affine_shared<2>(A, B, c.lane);
   const double Ae = shfl_excl(A, 1.0, c.lane);
-  double gain = fma(Ae, cy.v[0], shfl_excl(B[0], 0.0, c.lane));
-  double loss = fma(Ae, cy.v[1], shfl_excl(B[1], 0.0, c.lane));
+  const double Be0 = shfl_excl(B[0], 0.0, c.lane), Be1 = shfl_excl(B[1], 0.0, c.lane);
+  if (c.lb) {
+    const double a31 = __shfl_sync(kFull, A, 31);
+    const double tA[2] = {a31, a31};
+    const double tB[2] = {__shfl_sync(kFull, B[0], 31), __shfl_sync(kFull, B[1], 31)};
+    const double init[2] = {cy.v[0], cy.v[1]};
+    double Y[2];
+    lb_resolve<2>(c.lbd + j.lb_slot + 1, c.lbs, c.tile, tA, tB, init, lb_first_steady(f, p + 1, Ctx<K>::TILE), Y,
+                  c.err, c.lane);
+    cy.v[0] = Y[0];
+    cy.v[1] = Y[1];
+  }
+  double gain = fma(Ae, cy.v[0], Be0);
+  double loss = fma(Ae, cy.v[1], Be1);
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const int t = g0 + k;
@@ -340,6 +381,10 @@ __device__ __forceinline__ void rsi_round(const Ctx<K>& c, const Job& j, Carry& 
   }
   cy.v[0] = round_tail(c, gain);
   cy.v[1] = round_tail(c, loss);
+  if (c.lb) {
+    const double Y[2] = {cy.v[0], cy.v[1]};
+    lb_publish<2>(c.lbd + j.lb_slot + 1, c.lbs, c.tile, Y, c.lane);
+  }
   cy.f = f;
   c.flush(0, (float*)j.out[0]);
 }
@@ -364,6 +409,7 @@ struct SigStage {
     if (cnt < ready) return (double)(cnt - start + 1);
     return 1.0;
   }
+  __device__ __forceinline__ int steady_from() const { return (int)ready + 1; }
   __device__ __forceinline__ double step(int cnt, double y, double m) const {
     if (cnt < start) return y;
     if (cnt < ready) return y + m;
@@ -382,7 +428,7 @@ struct SigStage {
 template <int K>
 __device__ __forceinline__ void macd_round(const Ctx<K>& c, const Job& j, Carry& cy) {
   const int pl = j.in[0];
-  const int f = resolve_start(c, cy, pl);
+  const int f = resolve_start(c, cy, pl, j.lb_slot);
   const int fast = j.ip[0], slow = j.ip[1], sig = j.ip[2];
   const EmaStage slowSt{slow, 0, j.fp[2], j.fp[3], 1.0 / slow};
   const EmaStage fastSt{fast, slow - fast, j.fp[0], j.fp[1], 1.0 / fast};
@@ -390,10 +436,10 @@ __device__ __forceinline__ void macd_round(const Ctx<K>& c, const Job& j, Carry&
   talib_ema_coeffs(sig, gb, gk);
   const int start = slow - 1, ready = start + sig - 1;
   auto px = [&](int t, int) { return (double)c.x(pl, t); };
-  cy.v[1] = stage_round(c, f, slowSt, cy.v[1], px, [&](int k, int, double y) { c.line(0, k) = y; });
+  cy.v[1] = stage_round(c, f, slowSt, cy.v[1], px, [&](int k, int, double y) { c.line(0, k) = y; }, j.lb_slot + 1);
   cy.v[0] = stage_round(c, f, fastSt, cy.v[0], px, [&](int k, int cnt, double y) {
     c.line(0, k) = cnt >= start ? y - c.line(0, k) : 0.0;
-  });
+  }, j.lb_slot + 2);
   const SigStage sst{sig, start, ready, gb, gk, 1.0 / sig};
   cy.v[2] = stage_round(
       c, f, sst, cy.v[2], [&](int, int k) { return c.line(0, k); },
@@ -403,7 +449,8 @@ __device__ __forceinline__ void macd_round(const Ctx<K>& c, const Job& j, Carry&
         c.put(0, k, ok ? (float)m : qnan());
         c.put(1, k, ok ? (float)s : qnan());
         c.put(2, k, ok ? (float)(m - s) : qnan());
-      });
+      },
+      j.lb_slot + 3);
   cy.f = f;
   c.flush(0, (float*)j.out[0]);
   c.flush(1, (float*)j.out[1]);
@@ -427,6 +474,7 @@ struct AtrStage {
     if (t < 1) return 0.0;
     return t < p ? (double)t : 1.0;
   }
+  __device__ __forceinline__ int steady_from() const { return p + 1; }
   __device__ __forceinline__ double step(int t, double y, double r) const {
     if (t < 1) return y;
     if (t < p) return y + r;
@@ -467,7 +515,7 @@ __device__ __forceinline__ void atr_round(const Ctx<K>& c, const Job& j, Carry& 
       }
     }
     c.put(0, k, o);
-  });
+  }, j.lb_slot);
   c.flush(0, (float*)j.out[0]);
 }
 
@@ -522,9 +570,21 @@ __device__ __forceinline__ void adx_round(const Ctx<K>& c, const Job& j, Carry& 
   }
   warp_scan_affine_shared<3>(A, B, c.lane);
   const double Ae = shfl_excl(A, 1.0, c.lane);
-  double tr = fma(Ae, cy.v[0], shfl_excl(B[0], 0.0, c.lane));
-  double pd = fma(Ae, cy.v[1], shfl_excl(B[1], 0.0, c.lane));
-  double md = fma(Ae, cy.v[2], shfl_excl(B[2], 0.0, c.lane));
+  const double Be0 = shfl_excl(B[0], 0.0, c.lane), Be1 = shfl_excl(B[1], 0.0, c.lane),
+               Be2 = shfl_excl(B[2], 0.0, c.lane);
+  if (c.lb) {
+    const double a31 = __shfl_sync(kFull, A, 31);
+    const double tA[3] = {a31, a31, a31};
+    const double tB[3] = {__shfl_sync(kFull, B[0], 31), __shfl_sync(kFull, B[1], 31), __shfl_sync(kFull, B[2], 31)};
+    const double init[3] = {cy.v[0], cy.v[1], cy.v[2]};
+    double Y[3];
+    lb_resolve<3>(c.lbd + j.lb_slot, c.lbs, c.tile, tA, tB, init, lb_first_steady(0, p, Ctx<K>::TILE), Y, c.err,
+                  c.lane);
+    cy.v[0] = Y[0]; cy.v[1] = Y[1]; cy.v[2] = Y[2];
+  }
+  double tr = fma(Ae, cy.v[0], Be0);
+  double pd = fma(Ae, cy.v[1], Be1);
+  double md = fma(Ae, cy.v[2], Be2);
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const int t = g0 + k;
@@ -547,6 +607,10 @@ __device__ __forceinline__ void adx_round(const Ctx<K>& c, const Job& j, Carry& 
   cy.v[0] = round_tail(c, tr);
   cy.v[1] = round_tail(c, pd);
   cy.v[2] = round_tail(c, md);
+  if (c.lb) {
+    const double Y[3] = {cy.v[0], cy.v[1], cy.v[2]};
+    lb_publish<3>(c.lbd + j.lb_slot, c.lbs, c.tile, Y, c.lane);
+  }
   if (adx) {
     struct AdxStage {
       int p; double a, inv;
@@ -560,6 +624,7 @@ __device__ __forceinline__ void adx_round(const Ctx<K>& c, const Job& j, Carry& 
         if (t < p) return 0.0;
         return t < 2 * p - 1 ? (double)(t - p + 1) : 1.0;
       }
+      __device__ __forceinline__ int steady_from() const { return 2 * p; }
       __device__ __forceinline__ double step(int t, double y, double dx) const {
         if (t < p) return y;
         if (t < 2 * p - 1) return y + dx;
@@ -569,7 +634,7 @@ __device__ __forceinline__ void adx_round(const Ctx<K>& c, const Job& j, Carry& 
     } st{p, a, 1.0 / p};
     cy.v[3] = stage_round(
         c, 0, st, cy.v[3], [&](int, int k) { return c.line(0, k); },
-        [&](int k, int t, double y) { c.put(0, k, t >= 2 * p - 1 ? (float)y : qnan()); });
+        [&](int k, int t, double y) { c.put(0, k, t >= 2 * p - 1 ? (float)y : qnan()); }, j.lb_slot + 1);
   }
   c.flush(0, (float*)j.out[0]);
 }
@@ -614,6 +679,14 @@ __device__ __forceinline__ void volume_round(const Ctx<K>& c, const Job& j, Carr
     const double u = __shfl_up_sync(kFull, B, d);
     if (c.lane >= d) B += u;
   }
+  if (c.lb) {
+    const double tA[1] = {1.0};
+    const double tB[1] = {__shfl_sync(kFull, B, 31)};
+    const double init[1] = {cy.v[0]};
+    double Y[1];
+    lb_resolve<1>(c.lbd + j.lb_slot, c.lbs, c.tile, tA, tB, init, 0, Y, c.err, c.lane);
+    cy.v[0] = Y[0];
+  }
   double acc = cy.v[0] + shfl_excl(B, 0.0, c.lane);
 #pragma unroll
   for (int k = 0; k < K; ++k) {
@@ -623,6 +696,10 @@ __device__ __forceinline__ void volume_round(const Ctx<K>& c, const Job& j, Carr
     else c.line(0, k) = acc;
   }
   cy.v[0] = round_tail(c, acc);
+  if (c.lb) {
+    const double Y[1] = {cy.v[0]};
+    lb_publish<1>(c.lbd + j.lb_slot, c.lbs, c.tile, Y, c.lane);
+  }
   if (mode == 2) {
     const int fp_ = j.ip[0], sp_ = j.ip[1];
     const int warm = (fp_ > sp_ ? fp_ : sp_) - 1;
@@ -632,17 +709,19 @@ __device__ __forceinline__ void volume_round(const Ctx<K>& c, const Job& j, Carr
         if (t == 0) { a = 0.0; w = 1.0; } else { a = 1.0 - kk; w = kk; }
       }
       __device__ __forceinline__ double expect(int) const { return 1.0; }
+      __device__ __forceinline__ int steady_from() const { return 1; }
       __device__ __forceinline__ double step(int t, double y, double ad) const {
         return t == 0 ? ad : kk * ad + (1.0 - kk) * y;
       }
     };
     const Osc fs{2.0 / (fp_ + 1.0)}, ss{2.0 / (sp_ + 1.0)};
     cy.v[1] = stage_round(c, 0, fs, cy.v[1], [&](int, int k) { return c.line(0, k); },
-                          [&](int k, int, double y) { c.line(1, k) = y; });
+                          [&](int k, int, double y) { c.line(1, k) = y; }, j.lb_slot + 1);
     cy.v[2] = stage_round(c, 0, ss, cy.v[2], [&](int, int k) { return c.line(0, k); },
                           [&](int k, int t, double y) {
                             c.put(0, k, t >= warm ? (float)(c.line(1, k) - y) : qnan());
-                          });
+                          },
+                          j.lb_slot + 2);
   }
   c.flush(0, (float*)j.out[0]);
 }
@@ -821,7 +900,7 @@ __device__ __forceinline__ float win_min(const Ctx<K>& c, int pl, int t, int p) 
 template <int K>
 __device__ __forceinline__ void minmax_round(const Ctx<K>& c, const Job& j, Carry& cy, bool is_max) {
   const int pl = j.in[0], p = j.ip[0];
-  const int f = resolve_start(c, cy, pl);
+  const int f = resolve_start(c, cy, pl, j.lb_slot);
   const int g0 = c.gb0();
   for (int k = 0; k < K; ++k) {
     const int t = g0 + k;
@@ -1014,6 +1093,7 @@ __device__ __forceinline__ void correl_round(const Ctx<K>& c, const Job& j, Carr
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) first = min(first, __shfl_xor_sync(kFull, first, d));
     bad = first == 0x7fffffff ? -1 : first;
+    if (c.lb) bad = lb_first_index(c.lbd + j.lb_slot, c.lbs, c.tile, bad, c.err, c.lane);
   }
   const int tf = g0 > p - 1 ? g0 : (int)(p - 1);
   double sx = 0, sy = 0, sxx = 0, syy = 0, sxy = 0, ox = 0, oy = 0;

@@ -3,6 +3,7 @@
 // The heuristic picks the round width from the batch shape: short rows use
 // K = 4 or 8 bars per lane (a 128/256-bar round covers a whole row with few
 // idle lanes), long rows K = 16 (fewer halo re-reads and scan steps per bar).
+// Candle jobs run on the series-parallel engine (a thread per series).
 // Measured plans (ct_b200_autotune) override it; they are keyed by a coarse
 // shape histogram (log2 of the series count, mean and max length) plus a hash
 // of the job set, kept in memory and optionally in the file named by
@@ -76,12 +77,15 @@ SchedulePlan plan_for(const Launch& L, long long total_bars, long long max_len) 
   else if (mean <= 512) p.k = 8;
   else p.k = 16;
   p.warps_per_block = 8;
-  // Many series: one thread per series walking it in TA-Lib order (no scans).
-  // Few or very long series: a warp per series splitting time across lanes.
-  p.mode = (L.S >= 512 && max_len <= (1ll << 22)) ? 1 : 0;
+  // A warp per series splitting each round across its lanes; when there are
+  // too few series to fill the GPU and they span many rounds, rounds of one
+  // series go to different warps chained by decoupled look-back.
+  p.mode = 0;
+  if (L.S < 1024 && max_len >= 8ll * 32 * p.k) p.mode = 2;
   if (const char* e = std::getenv("TACUDA_B200_MODE")) {
     if (std::strcmp(e, "sp") == 0) p.mode = 1;
     if (std::strcmp(e, "ws") == 0) p.mode = 0;
+    if (std::strcmp(e, "lb") == 0) p.mode = 2;
   }
   for (int j = 0; j < L.njobs; ++j)
     if (L.jobs[j].family == F_CDL) p.mode = 1;  // candles run on the series-parallel engine

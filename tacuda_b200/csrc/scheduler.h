@@ -11,7 +11,8 @@
 namespace tb {
 
 struct SchedulePlan {
-  int mode = 0;            // 0: warp per series (time-parallel lanes), 1: thread per series
+  int mode = 0;            // 0: warp per series (time-parallel lanes), 1: thread per series,
+                           // 2: warp per tile with decoupled look-back between tiles
   int groups = 0;          // series-parallel: 32-series groups per CTA (0 = auto)
   int k = 8;               // bars per lane; a round covers 32*k bars
   int warps_per_block = 8;
@@ -37,7 +38,8 @@ ShapeKey shape_key(const Launch& L, long long total_bars, long long max_len);
 SchedulePlan plan_for(const Launch& L, long long total_bars, long long max_len);
 void remember_plan(const ShapeKey& key, const SchedulePlan& plan);
 
-cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, cudaStream_t stream, LaunchStats* stats);
+cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, long long total_bars, cudaStream_t stream,
+                         LaunchStats* stats);
 int max_lookback_halo(const Launch& L);
 
 }  // namespace tb

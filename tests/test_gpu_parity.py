@@ -37,9 +37,10 @@ def run_case(name, params, shape, seed=6):
     return stats
 
 
-@pytest.fixture(params=["sp", "ws"])
+@pytest.fixture(params=["sp", "ws", "lb"])
 def mode(request):
-    """Both engines: series-parallel (thread per series) and warp-per-series."""
+    """Every engine: series-parallel (thread per series), warp per series, and
+    warp per tile chained by decoupled look-back."""
     os.environ["TACUDA_B200_MODE"] = request.param
     yield request.param
     del os.environ["TACUDA_B200_MODE"]
@@ -231,3 +232,57 @@ def test_graph_capture_replay_equals_eager(mode):
         for k in outs:
             assert torch.equal(outs[k].view(torch.int32), eager[k].view(torch.int32)), k
     del g
+
+
+LOOKBACK_FAMILIES = ["ema", "dema", "tema", "t3", "rsi", "macd", "atr", "natr", "adx", "dx", "obv", "ad", "adosc",
+                     "min", "max", "correl", "sma", "stoch", "mfi"]
+SINGLE_INPUT = {"ema", "dema", "tema", "t3", "rsi", "macd", "min", "max", "sma"}
+
+
+@pytest.mark.parametrize("bars", ["4", "16"])
+@pytest.mark.parametrize("name", LOOKBACK_FAMILIES)
+def test_lookback_long_rows(name, bars):
+    """Rows of hundreds of tiles chained by look-back (checkpoints every 32
+    tiles, warm-up spanning tiles, a leading NaN run ending inside a later
+    tile) match the oracle, and repeated launches are bit-identical."""
+    os.environ["TACUDA_B200_MODE"] = "lb"
+    os.environ["TACUDA_B200_BARS_PER_LANE"] = bars
+    try:
+        d = oracle_data(synthetic.ohlcv(3, 30000, seed=21))
+        if name in SINGLE_INPUT:
+            d["close"][1, :1500] = np.nan
+        if name == "correl":
+            d["x"][2, 20000] = np.inf
+        p = dict(DEFAULTS[name])
+        if name in ("ema", "rsi", "dema"):
+            p["period"] = 300
+        dp = device_planes(d)
+        got = to_np(call_batch_d(name, dp, p))
+        again = to_np(call_batch_d(name, dp, p))
+        ref = O.run(name, d, **p)
+        for i, (g, a, r) in enumerate(zip(got, again, ref)):
+            compare(g, r, f"lookback {name}[{i}] bars/lane {bars}")
+            np.testing.assert_array_equal(g.view(np.uint32), a.view(np.uint32))
+    finally:
+        del os.environ["TACUDA_B200_MODE"]
+        del os.environ["TACUDA_B200_BARS_PER_LANE"]
+
+
+def test_lookback_fused_pass_on_long_rows():
+    """The 13-indicator fused pass over three 60000-bar rows in look-back mode
+    (the default plan for few long rows) matches the oracle."""
+    S, T = 3, 60000
+    d = synthetic.ohlcv(S, T, seed=23)
+    dp = device_planes(d)
+    outs = {n: torch.full((S, T), 777.0, device="cuda") for n in workloads.PASS13_OUTPUTS}
+    jobs = [tb.make_job(fam, p, fp, [outs[o].data_ptr() for o in on]) for _, fam, p, fp, on in workloads.PASS13]
+    series = tb.make_series({k: v.data_ptr() for k, v in dp.items() if k in tb.PLANE_ID}, S, T)
+    plan = tb.Plan(jobs, S, T)
+    assert plan.describe()["mode"] == 2
+    plan.execute(series, jobs, 0)
+    torch.cuda.synchronize()
+    for _, fam, p, fp, onames in workloads.PASS13:
+        ref = O.run(fam, d, **workloads.ORACLE_PARAMS[fam](p, fp))
+        for name, r in zip(onames, ref):
+            compare(outs[name].cpu().numpy(), r, f"lookback fused {name}")
+    plan.close()
