@@ -765,12 +765,9 @@ ctStatus_t ct_b200_plan_autotune(ctB200Plan* plan, const ctB200Series* series, c
   float best = 1e30f;
   tb::SchedulePlan bestPlan = plan->sched;
   // candidates: warp-per-series and look-back engines over round widths and
-  // block sizes (candles excepted), the series-parallel engine over group counts
-  bool cdl = false;
-  for (int j = 0; j < plan->njobs; ++j) cdl = cdl || plan->jobs[j].family == tb::F_CDL;
+  // block sizes, the series-parallel engine over group counts
   std::vector<tb::SchedulePlan> cands;
-  if (!cdl)
-    for (int mode : {0, 2})
+  for (int mode : {0, 2})
       for (int ki : ks) {
         if (ki == 4 && plan->maxlen > 4096) continue;
         if (mode == 2 && plan->maxlen < 4ll * 32 * ki) continue;

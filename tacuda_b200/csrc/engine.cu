@@ -63,7 +63,6 @@ __device__ __forceinline__ void run_job(const Ctx<K>& c, const Job& j, Carry& cy
     case F_CCI: cci_round(c, j); break;
     case F_MFI: mfi_round(c, j); break;
     case F_CORREL: correl_round(c, j, cy); break;
-    case F_CDL: cdl_round(c, j); break;
     default: break;
   }
 }
@@ -426,6 +425,7 @@ struct DeviceInfo {
   int smem_optin = 0;
   bool attr_set[3] = {false, false, false};
   bool sp_attr = false;
+  int cdl_per_sm = 0;
   std::vector<OccEntry> occ;
 };
 
@@ -587,6 +587,40 @@ int max_lookback_halo(const Launch& L) {
   return h;
 }
 
+// Candle jobs run on the bar-parallel tile kernel; consecutive jobs reading
+// the same planes share one launch.
+cudaError_t launch_candles(const Launch& L, const Job* jobs, int n, cudaStream_t stream) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  DeviceInfo& di = device_info(dev);
+  {
+    std::lock_guard<std::mutex> lk(g_mutex);
+    if (di.cdl_per_sm == 0) {
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&di.cdl_per_sm, cdl::tile_kernel, cdl::kTileBars, 0);
+      if (e != cudaSuccess) return e;
+      if (di.cdl_per_sm < 1) return cudaErrorInvalidConfiguration;
+    }
+  }
+  for (int a = 0; a < n;) {
+    cdl::TileArgs A;
+    std::memset(&A, 0, sizeof(A));
+    for (int i = 0; i < 4; ++i) A.plane[i] = L.plane[jobs[a].in[i]];
+    A.offsets = L.offsets;
+    A.order = L.order;
+    A.T = L.T;
+    A.S = L.S;
+    int b = a;
+    while (b < n && std::memcmp(jobs[b].in, jobs[a].in, sizeof(jobs[a].in)) == 0) A.jobs[A.njobs++] = jobs[b++];
+    const long long blocks = std::min<long long>(L.S, (long long)di.cdl_per_sm * di.sms);
+    cdl::tile_kernel<<<(int)std::max<long long>(1, blocks), cdl::kTileBars, 0, stream>>>(A);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    a = b;
+  }
+  return cudaSuccess;
+}
+
 template <int K>
 cudaError_t launch_lookback(Launch& L, const SchedulePlan& plan, long long total_bars, cudaStream_t stream,
                             LaunchStats* stats) {
@@ -645,6 +679,21 @@ cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, long long total_ba
   const int h = max_lookback_halo(L);
   L.halo = ((h + 31) / 32) * 32;
   if (plan.mode == 1) return launch_sp(L, plan, stream, stats);
+  // candle jobs go to the bar-parallel tile kernel, the rest to the engine
+  int ncdl = 0;
+  Job cdl_jobs[kMaxJobs];
+  for (int j = 0, k = 0; j < L.njobs; ++j) {
+    if (L.jobs[j].family == F_CDL) cdl_jobs[ncdl++] = L.jobs[j];
+    else L.jobs[k++] = L.jobs[j];
+  }
+  L.njobs -= ncdl;
+  if (ncdl > 0) {
+    if (L.njobs > 0) {
+      const cudaError_t e = launch_batch(L, plan, total_bars, stream, stats);
+      if (e != cudaSuccess) return e;
+    }
+    return launch_candles(L, cdl_jobs, ncdl, stream);
+  }
   L.lb = 0;
   if (plan.mode == 2) {
     switch (plan.k) {

@@ -3,7 +3,8 @@
 // The heuristic picks the round width from the batch shape: short rows use
 // K = 4 or 8 bars per lane (a 128/256-bar round covers a whole row with few
 // idle lanes), long rows K = 16 (fewer halo re-reads and scan steps per bar).
-// Candle jobs run on the series-parallel engine (a thread per series).
+// Candle jobs run on their own bar-parallel kernel unless the series-parallel
+// engine is forced (it evaluates them in the same pass).
 // Measured plans (ct_b200_autotune) override it; they are keyed by a coarse
 // shape histogram (log2 of the series count, mean and max length) plus a hash
 // of the job set, kept in memory and optionally in the file named by
@@ -87,8 +88,6 @@ SchedulePlan plan_for(const Launch& L, long long total_bars, long long max_len) 
     if (std::strcmp(e, "ws") == 0) p.mode = 0;
     if (std::strcmp(e, "lb") == 0) p.mode = 2;
   }
-  for (int j = 0; j < L.njobs; ++j)
-    if (L.jobs[j].family == F_CDL) p.mode = 1;  // candles run on the series-parallel engine
   // TACUDA_B200_BARS_PER_LANE=4|8|16 pins the round width (read on every call):
   // results of a row are then bit-independent of its length as well as of the
   // other rows, batch size and order.

@@ -84,7 +84,7 @@ struct Bars {
   }
 };
 
-#define CDL_FN(name) __device__ __forceinline__ int name(const Bars& b)
+#define CDL_FN(name) template <class B> __device__ __forceinline__ int name(const B& b)
 
 CDL_FN(c_two_crows) {
   return (b.COL(2) == 1 && b.RB(2) > b.AVG(BODY_LONG, 2) && b.COL(1) == -1 && b.BGAP_UP(1, 2) && b.COL(0) == -1 &&
@@ -209,7 +209,8 @@ CDL_FN(c_engulfing) {
   if (white || black) return (b.O(0) != b.C(1) && b.C(0) != b.O(1)) ? b.COL(0) * 100 : b.COL(0) * 80;
   return 0;
 }
-__device__ __forceinline__ bool star_shape(const Bars& b, bool doji_middle, bool bull) {
+template <class B>
+__device__ __forceinline__ bool star_shape(const B& b, bool doji_middle, bool bull) {
   const double pen = 0.3;
   const bool mid = doji_middle ? b.RB(1) <= b.AVG(BODY_DOJI, 1) : b.RB(1) <= b.AVG(BODY_SHORT, 1);
   if (bull)
@@ -233,7 +234,8 @@ CDL_FN(c_gravestone_doji) {
   return (b.RB(0) <= b.AVG(BODY_DOJI, 0) && b.LS(0) < b.AVG(SHADOW_VERY_SHORT, 0) &&
           b.US(0) > b.AVG(SHADOW_VERY_SHORT, 0)) ? 100 : 0;
 }
-__device__ __forceinline__ bool hammer_shape(const Bars& b) {
+template <class B>
+__device__ __forceinline__ bool hammer_shape(const B& b) {
   return b.RB(0) < b.AVG(BODY_SHORT, 0) && b.LS(0) > b.AVG(SHADOW_LONG, 0) && b.US(0) < b.AVG(SHADOW_VERY_SHORT, 0);
 }
 CDL_FN(c_hammer) {
@@ -242,7 +244,8 @@ CDL_FN(c_hammer) {
 CDL_FN(c_hanging_man) {
   return (hammer_shape(b) && (double)fminf(b.C(0), b.O(0)) >= (double)b.H(1) - b.AVG(NEAR, 1)) ? -100 : 0;
 }
-__device__ __forceinline__ int harami_common(const Bars& b, bool cross) {
+template <class B>
+__device__ __forceinline__ int harami_common(const B& b, bool cross) {
   const bool small = cross ? b.RB(0) <= b.AVG(BODY_DOJI, 0) : b.RB(0) <= b.AVG(BODY_SHORT, 0);
   if (b.RB(1) > b.AVG(BODY_LONG, 1) && small) {
     const float hi2 = fmaxf(b.C(0), b.O(0)), lo2 = fminf(b.C(0), b.O(0));
@@ -260,20 +263,23 @@ CDL_FN(c_high_wave) {
 }
 // HIKKAKE / HIKKAKEMOD: the pattern bar, or its confirmation within three bars
 // (first confirming close only), CandleUtils.h:1849-1895.
-__device__ __forceinline__ int hikkake_at(const Bars& b, int d) {
+template <class B>
+__device__ __forceinline__ int hikkake_at(const B& b, int d) {
   if (b.H(d + 1) < b.H(d + 2) && b.L(d + 1) > b.L(d + 2) &&
       ((b.H(d) < b.H(d + 1) && b.L(d) < b.L(d + 1)) || (b.H(d) > b.H(d + 1) && b.L(d) > b.L(d + 1))))
     return b.H(d) < b.H(d + 1) ? 100 : -100;
   return 0;
 }
-__device__ __forceinline__ int hikkake_mod_at(const Bars& b, int d) {
+template <class B>
+__device__ __forceinline__ int hikkake_mod_at(const B& b, int d) {
   if (b.H(d + 2) < b.H(d + 3) && b.L(d + 2) > b.L(d + 3) && b.H(d + 1) < b.H(d + 2) && b.L(d + 1) > b.L(d + 2) &&
       ((b.H(d) < b.H(d + 1) && b.L(d) < b.L(d + 1) && b.C(d + 2) <= b.L(d + 2) + b.AVG(NEAR, d + 2)) ||
        (b.H(d) > b.H(d + 1) && b.L(d) > b.L(d + 1) && b.C(d + 2) >= b.H(d + 2) - b.AVG(NEAR, d + 2))))
     return b.H(d) < b.H(d + 1) ? 100 : -100;
   return 0;
 }
-__device__ __forceinline__ int hikkake_confirm(const Bars& b, bool modified) {
+template <class B>
+__device__ __forceinline__ int hikkake_confirm(const B& b, bool modified) {
   const int pat = modified ? hikkake_mod_at(b, 0) : hikkake_at(b, 0);
   if (pat != 0) return pat;
   const long long lowest = modified ? 3 : 2;
@@ -309,7 +315,8 @@ CDL_FN(c_inverted_hammer) {
   return (b.RB(0) < b.AVG(BODY_SHORT, 0) && b.US(0) > b.AVG(SHADOW_LONG, 0) &&
           b.LS(0) < b.AVG(SHADOW_VERY_SHORT, 0) && b.BGAP_DN(0, 1)) ? 100 : 0;
 }
-__device__ __forceinline__ bool kicking_common(const Bars& b) {
+template <class B>
+__device__ __forceinline__ bool kicking_common(const B& b) {
   return b.COL(1) == -b.COL(0) && b.RB(1) > b.AVG(BODY_LONG, 1) && b.US(1) < b.AVG(SHADOW_VERY_SHORT, 1) &&
          b.LS(1) < b.AVG(SHADOW_VERY_SHORT, 1) && b.RB(0) > b.AVG(BODY_LONG, 0) &&
          b.US(0) < b.AVG(SHADOW_VERY_SHORT, 0) && b.LS(0) < b.AVG(SHADOW_VERY_SHORT, 0) &&
@@ -447,7 +454,8 @@ CDL_FN(c_xside_gap_3_methods) {
 #undef CDL_FN
 
 // Pattern k in the order of the ct_cdl_*_batch_d declarations.
-__device__ __forceinline__ int cdl_eval(int k, const Bars& b) {
+template <class B>
+__device__ __forceinline__ int cdl_eval(int k, const B& b) {
   switch (k) {
     case 0: return c_doji(b);
     case 1: return c_hammer(b);
