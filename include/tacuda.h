@@ -337,6 +337,18 @@ CTAPI_EXPORT int ct_b200_cdl_count(void);
 CTAPI_EXPORT const char* ct_b200_cdl_name(int pattern);
 CTAPI_EXPORT int ct_b200_cdl_lookback(int pattern);
 
+/* Allocation-free look-back launch (no counterpart in the reference): the jobs
+ * of a uniform batch (no candle jobs) on the look-back engine, with its scratch
+ * in a static 8 MiB device array per device instead of the stream-ordered pool.
+ * The batch must need at most 8 MiB of scratch: 256 B plus 96 B per
+ * (round of a row, recurrence stage); larger batches fail with
+ * CT_STATUS_INVALID_ARGUMENT. The first call on a device looks up the array's
+ * address and must come before any stream capture. Each call zeroes the
+ * scratch on its stream before the launch; calls that overlap in time (other
+ * streams or threads) race on the one array and must be serialised. */
+CTAPI_EXPORT ctStatus_t ct_b200_fused_lookback_static_d(const ctB200Series* series, const ctB200Job* jobs,
+                                                        int numJobs, cudaStream_t stream);
+
 /* Number of kernel launches this library issued from the calling process
  * (diagnostics; the batch entry points issue one each). */
 CTAPI_EXPORT unsigned long long ct_b200_launch_count(void);

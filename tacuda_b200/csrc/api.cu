@@ -593,6 +593,32 @@ ctStatus_t ct_b200_fused_batch_d(const ctB200Series* series, const ctB200Job* jo
   return finish(stream, who);
 }
 
+ctStatus_t ct_b200_fused_lookback_static_d(const ctB200Series* series, const ctB200Job* jobs, int numJobs,
+                                           cudaStream_t stream) {
+  clear_error();
+  const char* who = "ct_b200_fused_lookback_static_d";
+  Launch L;
+  ctStatus_t st = build_launch(series, jobs, numJobs, L, who);
+  if (st != CT_STATUS_SUCCESS) return st;
+  if (L.offsets) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": uniform rows only");
+  for (int j = 0; j < L.njobs; ++j)
+    if (L.jobs[j].family == tb::F_CDL)
+      return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": candle jobs are not supported");
+  tb::SchedulePlan plan = tb::plan_for(L, L.T * (long long)L.S, L.T);
+  plan.mode = 2;
+  size_t need = 0;
+  const cudaError_t e = tb::launch_lookback_static(L, plan, stream, &need);
+  if (e == cudaErrorInvalidValue && need > tb::kStaticLookbackBytes) {
+    char msg[256];
+    std::snprintf(msg, sizeof msg, "%s: batch needs %zu bytes of look-back scratch, more than the static %zu bytes",
+                  who, need, (size_t)tb::kStaticLookbackBytes);
+    return fail(CT_STATUS_INVALID_ARGUMENT, msg);
+  }
+  if (e != cudaSuccess) return cuda_fail(CT_STATUS_KERNEL_FAILED, who, e);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return finish(stream, who);
+}
+
 ctStatus_t ct_b200_fused_batch(const ctB200Series* hs, const ctB200Job* hjobs, int numJobs, cudaStream_t stream) {
   clear_error();
   const char* who = "ct_b200_fused_batch";

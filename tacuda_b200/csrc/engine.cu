@@ -665,6 +665,88 @@ cudaError_t launch_lookback(Launch& L, const SchedulePlan& plan, long long total
   return e != cudaSuccess ? e : ef;
 }
 
+// Look-back scratch of the allocation-free entry point: a file-scope device
+// array (one copy per device, created when the module loads there). Its
+// address is taken once per device with cudaGetSymbolAddress while that device
+// is current. Every launch zeroes the part it uses (tile counter, error word,
+// descriptor flags) on its stream first, so calls must not overlap in time.
+__device__ __align__(256) unsigned char g_static_lb_scratch[kStaticLookbackBytes];
+
+namespace {
+std::mutex g_static_mutex;
+std::vector<unsigned char*> g_static_ptr;  // per device
+
+cudaError_t static_scratch(unsigned char** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(g_static_mutex);
+  if ((int)g_static_ptr.size() <= dev) g_static_ptr.resize(dev + 1, nullptr);
+  if (!g_static_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_static_lb_scratch);
+    if (e != cudaSuccess) return e;
+    g_static_ptr[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = g_static_ptr[dev];
+  return cudaSuccess;
+}
+
+template <int K>
+cudaError_t launch_lookback_static_k(Launch& L, const SchedulePlan& plan, cudaStream_t stream, size_t* need) {
+  constexpr int TILE = 32 * K;
+  int nslots = 0;
+  for (int j = 0; j < L.njobs; ++j) {
+    L.jobs[j].lb_slot = nslots;
+    nslots += lb_slots(L.jobs[j]);
+  }
+  if (nslots == 0) nslots = 1;
+  const long long ntiles = (long long)L.S * ((L.T + TILE - 1) / TILE);
+  const size_t head = 256;
+  const size_t bytes = head + (size_t)ntiles * nslots * sizeof(LbDesc);
+  *need = bytes;
+  if (bytes > kStaticLookbackBytes) return cudaErrorInvalidValue;
+  unsigned char* scratch = nullptr;
+  cudaError_t e = static_scratch(&scratch);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(scratch, 0, bytes, stream);
+  if (e != cudaSuccess) return e;
+  L.lb = 1;
+  L.lb_counter = reinterpret_cast<unsigned long long*>(scratch);
+  L.err = reinterpret_cast<int*>(scratch + 8);
+  L.lb_tile_start = nullptr;
+  L.lb_desc = reinterpret_cast<LbDesc*>(scratch + head);
+  L.lb_nslots = nslots;
+  L.lb_tiles = ntiles;
+  e = launch_k<K>(L, plan, stream, nullptr);
+  if (e == cudaSuccess && stream == 0) {
+    int herr = 0;
+    e = cudaMemcpyAsync(&herr, L.err, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess && herr != 0) e = cudaErrorLaunchTimeout;
+  }
+  return e;
+}
+}  // namespace
+
+cudaError_t launch_lookback_static(Launch& L, const SchedulePlan& plan, cudaStream_t stream, size_t* need) {
+  unsigned mask = 0;
+  int need_tp = 0;
+  for (int j = 0; j < L.njobs; ++j) {
+    mask |= job_planes(L.jobs[j]);
+    if (L.jobs[j].family == F_CCI || L.jobs[j].family == F_MFI) need_tp = 1;
+  }
+  if (need_tp) mask |= (1u << P_HIGH) | (1u << P_LOW) | (1u << P_CLOSE);
+  L.plane_mask = mask;
+  L.need_tp = need_tp;
+  L.halo = ((max_lookback_halo(L) + 31) / 32) * 32;
+  switch (plan.k) {
+    case 4: return launch_lookback_static_k<4>(L, plan, stream, need);
+    case 16: return launch_lookback_static_k<16>(L, plan, stream, need);
+    default: return launch_lookback_static_k<8>(L, plan, stream, need);
+  }
+}
+
 cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, long long total_bars, cudaStream_t stream,
                          LaunchStats* stats) {
   unsigned mask = 0;

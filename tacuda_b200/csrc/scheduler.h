@@ -42,4 +42,11 @@ cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, long long total_ba
                          LaunchStats* stats);
 int max_lookback_halo(const Launch& L);
 
+// Look-back launch with its scratch in a static device array of
+// kStaticLookbackBytes per device (allocation-free). Uniform rows, no candle
+// jobs. Returns cudaErrorInvalidValue when the scratch it needs (*need bytes)
+// exceeds the array. Calls must not overlap in time.
+constexpr size_t kStaticLookbackBytes = 8u << 20;
+cudaError_t launch_lookback_static(Launch& L, const SchedulePlan& plan, cudaStream_t stream, size_t* need);
+
 }  // namespace tb
