@@ -73,7 +73,7 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src, bool val
 }
 
 template <int K>
-__global__ void __launch_bounds__(256) batch_kernel(const __grid_constant__ Launch L, const SmemLayout lay) {
+__global__ void __launch_bounds__(256, (K <= 8 ? 2 : 1)) batch_kernel(const __grid_constant__ Launch L, const SmemLayout lay) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int TILE = 32 * K;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
