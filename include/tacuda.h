@@ -349,6 +349,34 @@ CTAPI_EXPORT int ct_b200_cdl_lookback(int pattern);
 CTAPI_EXPORT ctStatus_t ct_b200_fused_lookback_static_d(const ctB200Series* series, const ctB200Job* jobs,
                                                         int numJobs, cudaStream_t stream);
 
+/* Differentiable EMA / MACD / RSI with a continuous smoothing coefficient per
+ * series (no counterpart in the reference). Periods fix each indicator's
+ * lookback and seed as in TA-Lib; alpha replaces the recurrence coefficient of
+ * the EMA, of MACD's fast line and of RSI's Wilder smoothing (alpha = 2/(p+1),
+ * resp. 1/p, gives TA-Lib's values within float tolerance). MACD's slow and
+ * signal lines keep TA-Lib's 2/(n+1). Inputs must be finite; alpha in (0, 1).
+ * The forward pass writes, per series, the recurrence state entering every
+ * 256-bar segment into d_checkpoints (ct_b200_alpha_checkpoint_doubles(T)
+ * doubles per series); the backward pass reads them instead of per-bar state.
+ * Backward: gradients of L = sum(w_ema*EMA + w_macd*MACD + w_signal*SIGNAL +
+ * w_hist*HIST + w_rsi*RSI) over the non-warm-up bars with respect to the
+ * closes (d_dclose, numSeries x seriesLen) and alpha (d_dalpha, numSeries).
+ * Null weight planes count as zero; null forward outputs are skipped. */
+typedef struct ctB200AlphaParams {
+  int emaPeriod, fastPeriod, slowPeriod, signalPeriod, rsiPeriod;
+} ctB200AlphaParams;
+CTAPI_EXPORT long long ct_b200_alpha_checkpoint_doubles(int seriesLen);
+CTAPI_EXPORT ctStatus_t ct_b200_alpha_forward_d(const float* d_close, const float* d_alpha, int seriesLen,
+                                                int numSeries, const ctB200AlphaParams* params, float* d_ema,
+                                                float* d_macd, float* d_signal, float* d_hist, float* d_rsi,
+                                                double* d_checkpoints, cudaStream_t stream);
+CTAPI_EXPORT ctStatus_t ct_b200_alpha_backward_d(const float* d_close, const float* d_alpha, int seriesLen,
+                                                 int numSeries, const ctB200AlphaParams* params,
+                                                 const double* d_checkpoints, const float* d_w_ema,
+                                                 const float* d_w_macd, const float* d_w_signal,
+                                                 const float* d_w_hist, const float* d_w_rsi, float* d_dclose,
+                                                 float* d_dalpha, cudaStream_t stream);
+
 /* Number of kernel launches this library issued from the calling process
  * (diagnostics; the batch entry points issue one each). */
 CTAPI_EXPORT unsigned long long ct_b200_launch_count(void);

@@ -55,6 +55,11 @@ class ctB200Job(ct.Structure):
                 ("cdl_int32", _I)]
 
 
+class ctB200AlphaParams(ct.Structure):
+    _fields_ = [("emaPeriod", _I), ("fastPeriod", _I), ("slowPeriod", _I), ("signalPeriod", _I),
+                ("rsiPeriod", _I)]
+
+
 def _load() -> ct.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(f"tacuda_b200 native library missing: {LIB_PATH} "
@@ -75,6 +80,10 @@ def _load() -> ct.CDLL:
     lib.ct_b200_plan_describe.argtypes = [_P, ct.POINTER(_I), ct.POINTER(_I), ct.POINTER(_I), ct.POINTER(_I)]
     lib.ct_b200_plan_destroy.argtypes = [_P]
     lib.ct_b200_cdl_batch_d.argtypes = [_P, _P, _P, _P, _P, _I, _I, ct.c_uint64, _P]
+    lib.ct_b200_alpha_checkpoint_doubles.argtypes = [_I]
+    lib.ct_b200_alpha_checkpoint_doubles.restype = ct.c_longlong
+    lib.ct_b200_alpha_forward_d.argtypes = [_P, _P, _I, _I, ct.POINTER(ctB200AlphaParams)] + [_P] * 7
+    lib.ct_b200_alpha_backward_d.argtypes = [_P, _P, _I, _I, ct.POINTER(ctB200AlphaParams)] + [_P] * 9
     return lib
 
 

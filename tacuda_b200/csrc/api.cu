@@ -5,6 +5,7 @@
 // engine (engine.cu) with one or more jobs.
 #include <tacuda.h>
 
+#include "adjoint.h"
 #include "engine.h"
 #include "families.cuh"
 #include "scheduler.h"
@@ -614,6 +615,64 @@ ctStatus_t ct_b200_fused_lookback_static_d(const ctB200Series* series, const ctB
                   who, need, (size_t)tb::kStaticLookbackBytes);
     return fail(CT_STATUS_INVALID_ARGUMENT, msg);
   }
+  if (e != cudaSuccess) return cuda_fail(CT_STATUS_KERNEL_FAILED, who, e);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return finish(stream, who);
+}
+
+// ------------------------------------------------------------ alpha API
+
+long long ct_b200_alpha_checkpoint_doubles(int seriesLen) {
+  if (seriesLen <= 0) return 0;
+  return (long long)((seriesLen + tb::kAlphaSegment - 1) / tb::kAlphaSegment) * tb::kAlphaStates;
+}
+
+static ctStatus_t alpha_params(const ctB200AlphaParams* p, tb::AlphaParams& out, const char* who) {
+  if (!p) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": null parameters");
+  out = tb::AlphaParams{p->emaPeriod, p->fastPeriod, p->slowPeriod, p->signalPeriod, p->rsiPeriod};
+  if (out.ema_period < 2 || out.fast < 2 || out.slow < out.fast || out.signal < 1 || out.rsi_period < 2 ||
+      out.ema_period > kMaxWindow || out.slow > kMaxWindow || out.signal > kMaxWindow || out.rsi_period > kMaxWindow)
+    return fail(CT_STATUS_INVALID_ARGUMENT,
+                std::string(who) + ": invalid periods (need ema>=2, 2<=fast<=slow, signal>=1, rsi>=2)");
+  return CT_STATUS_SUCCESS;
+}
+
+ctStatus_t ct_b200_alpha_forward_d(const float* d_close, const float* d_alpha, int seriesLen, int numSeries,
+                                   const ctB200AlphaParams* params, float* d_ema, float* d_macd, float* d_signal,
+                                   float* d_hist, float* d_rsi, double* d_checkpoints, cudaStream_t stream) {
+  clear_error();
+  const char* who = "ct_b200_alpha_forward_d";
+  if (!d_close || !d_alpha || !d_checkpoints || seriesLen <= 0 || numSeries <= 0)
+    return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": null pointer or invalid size");
+  tb::AlphaLaunch L{};
+  ctStatus_t st = alpha_params(params, L.P, who);
+  if (st != CT_STATUS_SUCCESS) return st;
+  L.x = d_close; L.alpha = d_alpha; L.T = seriesLen; L.S = numSeries;
+  L.ema = d_ema; L.macd = d_macd; L.sig = d_signal; L.hist = d_hist; L.rsi = d_rsi;
+  L.ckpt = d_checkpoints;
+  const cudaError_t e = tb::alpha_forward(L, stream);
+  if (e != cudaSuccess) return cuda_fail(CT_STATUS_KERNEL_FAILED, who, e);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return finish(stream, who);
+}
+
+ctStatus_t ct_b200_alpha_backward_d(const float* d_close, const float* d_alpha, int seriesLen, int numSeries,
+                                    const ctB200AlphaParams* params, const double* d_checkpoints,
+                                    const float* d_w_ema, const float* d_w_macd, const float* d_w_signal,
+                                    const float* d_w_hist, const float* d_w_rsi, float* d_dclose, float* d_dalpha,
+                                    cudaStream_t stream) {
+  clear_error();
+  const char* who = "ct_b200_alpha_backward_d";
+  if (!d_close || !d_alpha || !d_checkpoints || !d_dclose || !d_dalpha || seriesLen <= 0 || numSeries <= 0)
+    return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": null pointer or invalid size");
+  tb::AlphaLaunch L{};
+  ctStatus_t st = alpha_params(params, L.P, who);
+  if (st != CT_STATUS_SUCCESS) return st;
+  L.x = d_close; L.alpha = d_alpha; L.T = seriesLen; L.S = numSeries;
+  L.ckpt = const_cast<double*>(d_checkpoints);
+  L.w_ema = d_w_ema; L.w_macd = d_w_macd; L.w_sig = d_w_signal; L.w_hist = d_w_hist; L.w_rsi = d_w_rsi;
+  L.dx = d_dclose; L.dalpha = d_dalpha;
+  const cudaError_t e = tb::alpha_backward(L, stream);
   if (e != cudaSuccess) return cuda_fail(CT_STATUS_KERNEL_FAILED, who, e);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return finish(stream, who);
