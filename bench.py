@@ -223,6 +223,123 @@ def run_ours(args, rank, world, local):
     return stats, clocks.summary(), h2d, d2h, launches0
 
 
+def _event_ms(fn, reps, warm=2, stream=None):
+    """Median CUDA-event time of fn() on the current stream."""
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return statistics.median(ts)
+
+
+def run_extras(dev, peak):
+    """The other measured workloads, each timed with CUDA events (inputs larger
+    than L2 where the workload is; config 1 is latency-bound and L2-resident)."""
+    import torch
+    import tacuda_b200 as tb
+    from tacuda_b200 import synthetic, workloads
+    from tacuda_b200 import torch_api as TA
+    out = {}
+    torch.cuda.synchronize()
+
+    # config 1: one 100,000-bar close series, SMA20 EMA30 RSI14 MACD12/26/9
+    x = torch.from_numpy(synthetic.single_close(100_000, seed=11).astype(np.float32)).to(dev).reshape(1, -1)
+    o1 = {n: torch.empty_like(x) for n in ("sma", "ema", "rsi", "macd", "sig", "hist")}
+    j1 = [tb.make_job("sma", (20,), (), [o1["sma"].data_ptr()]), tb.make_job("ema", (30,), (), [o1["ema"].data_ptr()]),
+          tb.make_job("rsi", (14,), (), [o1["rsi"].data_ptr()]),
+          tb.make_job("macd", (12, 26, 9), (), [o1[k].data_ptr() for k in ("macd", "sig", "hist")])]
+    s1 = tb.make_series({"close": x.data_ptr()}, 1, x.shape[1])
+    st = torch.cuda.current_stream().cuda_stream
+    f_ms = _event_ms(lambda: tb.fused_batch_d(s1, j1, st), 20)
+    p_ms = _event_ms(lambda: [tb.fused_batch_d(s1, [j], st) for j in j1], 20)
+    out["config1_single_100k"] = {"workload": "1 series x 100,000 bars: SMA20 EMA30 RSI14 MACD12/26/9 (6 outputs)",
+                                  "fused_us": f_ms * 1e3, "plain_us": p_ms * 1e3,
+                                  "value": 4 * 100_000 / (f_ms * 1e-3), "unit": "indicator-bars/s",
+                                  "bound": "latency"}
+    del x, o1
+
+    # config 3: 10,000 ragged series (log-uniform 50..20,000 bars), 13-pass + 61 CDL int32
+    lengths = synthetic.ragged_lengths(10_000, 50, 20_000, seed=7)
+    planes, off = synthetic.ragged_ohlcv(lengths, seed=4)
+    N = int(off[-1])
+    dp = {k: torch.from_numpy(v).to(dev) for k, v in planes.items()}
+    doff = torch.from_numpy(off).to(dev)
+    outs = {n: torch.empty(N, device=dev) for n in workloads.PASS13_OUTPUTS}
+    names = tb.cdl_names()
+    mask = sum(1 << k for k, n in enumerate(names) if n not in ("bullish_engulfing", "bearish_engulfing"))
+    cdl = torch.empty((len(names), N), dtype=torch.int32, device=dev)
+    jobs = [tb.make_job(fam, p, fp, [outs[o].data_ptr() for o in on]) for _, fam, p, fp, on in workloads.PASS13]
+    jobs.append(tb.make_job("cdl", (), (), [cdl.data_ptr()], cdl_mask=mask, cdl_stride=N, cdl_int32=True))
+    ser = tb.make_series({k: v.data_ptr() for k, v in dp.items()}, len(lengths), 0, doff.data_ptr())
+    plan = tb.Plan(jobs, len(lengths), 0, off)
+    fused = _event_ms(lambda: plan.execute(ser, jobs, st), 5)
+    plans = [tb.Plan([j], len(lengths), 0, off) for j in jobs]
+    plain = _event_ms(lambda: [pl.execute(ser, [j], st) for pl, j in zip(plans, jobs)], 3)
+    ncdl = bin(mask).count("1")
+    bytes3 = N * (20 + 4 * len(workloads.PASS13_OUTPUTS) + 4 * ncdl)
+    gbs = bytes3 / (fused * 1e-3) / 1e9
+    out["config3_ragged_13_plus_cdl61"] = {
+        "workload": f"10,000 ragged series (sum {N} bars), 13-indicator pass + 61 CDL int32, one plan (2 launches)",
+        "ms": fused, "plain_ms": plain, "fused_speedup": plain / fused,
+        "value": (13 + ncdl) * N / (fused * 1e-3), "unit": "indicator-bars/s",
+        "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                     "algorithmic_bytes_per_launch": bytes3},
+        "l2": "inputs and outputs far larger than L2"}
+    for pl in plans:
+        pl.close()
+    plan.close()
+    del dp, doff, outs, cdl
+
+    # config 4: per-series alpha EMA/MACD/RSI, forward and adjoint, 4096 x 2048
+    rng = np.random.default_rng(4)
+    c4 = torch.from_numpy(synthetic.ohlcv(4096, 2048, seed=4)["close"]).to(dev)
+    a4 = torch.from_numpy(rng.uniform(0.01, 0.5, 4096).astype(np.float32)).to(dev)
+    w4 = [torch.from_numpy(rng.standard_normal((4096, 2048)).astype(np.float32)).to(dev) for _ in range(5)]
+    ck = TA.alpha_forward(c4, a4)[5]
+    fwd = _event_ms(lambda: TA.alpha_forward(c4, a4), 5)
+    bwd = _event_ms(lambda: TA.alpha_backward(c4, a4, ck, w4), 5)
+    n4 = 4096 * 2048
+    out["config4_alpha_adjoint"] = {
+        "workload": "4096 series x 2048 bars, EMA14 MACD12/26/9 RSI14 with per-series alpha; adjoint of a "
+                    "N(0,1)-weighted sum of the 5 outputs; checkpoints every 256 bars",
+        "forward_ms": fwd, "adjoint_ms": bwd, "adjoint_over_forward": bwd / fwd,
+        "forward_GBs": n4 * 24 / (fwd * 1e-3) / 1e9, "adjoint_GBs": n4 * 28 / (bwd * 1e-3) / 1e9}
+    del c4, a4, w4, ck
+
+    # config 5: 4 series x 50,000,000 bars with a +1e4 level, look-back across tiles
+    T5 = 50_000_000
+    x5 = torch.from_numpy(synthetic.level_walk(4, T5, seed=5)).to(dev)
+    y5 = torch.from_numpy(synthetic.level_walk(4, T5, seed=6)).to(dev)
+    o5 = {n: torch.empty_like(x5) for n in ("sma", "stddev", "var", "linearreg", "correl", "ema")}
+    j5 = [tb.make_job("sma", (200,), (), [o5["sma"].data_ptr()]),
+          tb.make_job("stddev", (200,), (1.0,), [o5["stddev"].data_ptr()]),
+          tb.make_job("var", (200,), (), [o5["var"].data_ptr()]),
+          tb.make_job("linearreg", (200,), (), [o5["linearreg"].data_ptr()]),
+          tb.make_job("correl", (30,), (), [o5["correl"].data_ptr()], inputs=("close", "aux")),
+          tb.make_job("ema", (500,), (), [o5["ema"].data_ptr()])]
+    s5 = tb.make_series({"close": x5.data_ptr(), "aux": y5.data_ptr()}, 4, T5)
+    ms5 = _event_ms(lambda: tb.fused_batch_d(s5, j5, st), 3, warm=1)
+    bytes5 = 4 * T5 * (8 + 4 * len(o5))
+    g5 = bytes5 / (ms5 * 1e-3) / 1e9
+    out["config5_long_4x50M"] = {
+        "workload": "4 series x 50,000,000 bars (+1e4 level): SMA/STDDEV/VAR/LINEARREG 200, CORREL30, EMA500, "
+                    "FP64 carries, decoupled look-back",
+        "ms": ms5, "value": 6 * 4 * T5 / (ms5 * 1e-3), "unit": "indicator-bars/s",
+        "roofline": {"bound": "hbm", "achieved": g5, "peak": peak, "unit": "GB/s", "frac": g5 / peak,
+                     "algorithmic_bytes_per_launch": bytes5}}
+    del x5, y5, o5
+    torch.cuda.synchronize()
+    return out
+
+
 def cpu_baseline_pass13(S, T, threads, seed=2024):
     """Reference CPU path of the 13-indicator pass on `threads` host threads."""
     from oracle import oracle as O
@@ -247,6 +364,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--series", type=int, default=S_DEFAULT)
     ap.add_argument("--length", type=int, default=T_DEFAULT)
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="skip the other measured workloads (single long series, ragged + candles, "
+                         "alpha adjoint, 4 x 50M bars)")
     args = ap.parse_args()
     rank, world, local = dist_env()
     n_ind = 13
@@ -315,6 +435,8 @@ def main():
             "gpu_launches": args.steps,
             "clocks": clocks,
         }
+        if args.extras:
+            line["other_workloads"] = run_extras(torch.device("cuda", local), peak)
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()

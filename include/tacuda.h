@@ -340,7 +340,7 @@ CTAPI_EXPORT int ct_b200_cdl_lookback(int pattern);
 /* Allocation-free look-back launch (no counterpart in the reference): the jobs
  * of a uniform batch (no candle jobs) on the look-back engine, with its scratch
  * in a static 8 MiB device array per device instead of the stream-ordered pool.
- * The batch must need at most 8 MiB of scratch: 256 B plus 96 B per
+ * The batch must need at most 8 MiB of scratch: 256 B plus 144 B per
  * (round of a row, recurrence stage); larger batches fail with
  * CT_STATUS_INVALID_ARGUMENT. The first call on a device looks up the array's
  * address and must come before any stream capture. Each call zeroes the

@@ -20,7 +20,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OUT = PKG / "libtacuda_b200.so"
-SOURCES = ["engine.cu", "adjoint.cu", "api.cu", "scheduler.cpp"]
+SOURCES = ["engine.cu", "adjoint.cu", "api.cu", "scheduler.cpp", "pool.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -26,6 +26,7 @@
 // segment's forward quantities are recomputed from its checkpoint into a
 // per-series scratch line, then consumed in reverse.
 #include "adjoint.h"
+#include "pool.h"
 #include "families.cuh"
 
 namespace tb {
@@ -81,6 +82,7 @@ struct BarOut {
   bool ema_ok, macd_ok, rsi_ok;
 };
 
+template <bool kGrad>
 __device__ __forceinline__ BarOut step(const Stages& s, int t, double x, double xprev, State& st, BarQ& q) {
   BarOut o;
   q.eE = x - st.e;
@@ -115,10 +117,13 @@ __device__ __forceinline__ BarOut step(const Stages& s, int t, double x, double 
   if (o.rsi_ok) {
     const double tot = st.rg + st.rl;
     if (tot > 0.0) {
-      o.rsi = 100.0 * (st.rg / tot);
-      const double inv2 = 100.0 / (tot * tot);
-      q.cG = st.rl * inv2;
-      q.cL = -st.rg * inv2;
+      if (kGrad) {
+        const double inv2 = 100.0 / (tot * tot);
+        q.cG = st.rl * inv2;
+        q.cL = -st.rg * inv2;
+      } else {
+        o.rsi = 100.0 * (st.rg / tot);
+      }
     }
   }
   return o;
@@ -148,7 +153,7 @@ __global__ void alpha_forward_kernel(AlphaLaunch L) {
     }
     const double x = L.x[base + t];
     BarQ q;
-    const BarOut o = step(s, t, x, xprev, st, q);
+    const BarOut o = step<false>(s, t, x, xprev, st, q);
     xprev = x;
     if (L.ema) L.ema[base + t] = o.ema_ok ? (float)o.ema : nan;
     if (L.macd) L.macd[base + t] = o.macd_ok ? (float)o.macd : nan;
@@ -180,7 +185,7 @@ __global__ void alpha_backward_kernel(AlphaLaunch L) {
     for (int t = t0; t < t1; ++t) {
       const double x = L.x[base + t];
       BarQ q;
-      step(s, t, x, xprev, st, q);
+      step<true>(s, t, x, xprev, st, q);
       xprev = x;
       const int i = t - t0;
       qat(i, 0) = q.eE; qat(i, 1) = q.eF; qat(i, 2) = q.cG;
@@ -248,14 +253,14 @@ cudaError_t alpha_forward(const AlphaLaunch& L, cudaStream_t stream) {
 cudaError_t alpha_backward(AlphaLaunch L, cudaStream_t stream) {
   const size_t bytes = (size_t)kSeg * kQ * L.S * sizeof(double);
   double* scratch = nullptr;
-  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&scratch), bytes, stream);
+  cudaError_t e = scratch_alloc(reinterpret_cast<void**>(&scratch), bytes, stream);
   if (e != cudaSuccess) return e;
   L.scratch = scratch;
   const int threads = 32;
   const int blocks = (L.S + threads - 1) / threads;
   alpha_backward_kernel<<<blocks, threads, 0, stream>>>(L);
   e = cudaGetLastError();
-  const cudaError_t ef = cudaFreeAsync(scratch, stream);
+  const cudaError_t ef = scratch_free(scratch, stream);
   return e != cudaSuccess ? e : ef;
 }
 

@@ -7,6 +7,7 @@
 
 #include "adjoint.h"
 #include "engine.h"
+#include "pool.h"
 #include "families.cuh"
 #include "scheduler.h"
 
@@ -691,11 +692,11 @@ ctStatus_t ct_b200_fused_batch(const ctB200Series* hs, const ctB200Job* hjobs, i
   std::vector<void*> owned;
   auto alloc = [&](size_t b) -> void* {
     void* p = nullptr;
-    if (cudaMallocAsync(&p, b, stream) != cudaSuccess) return nullptr;
+    if (tb::scratch_alloc(&p, b, stream) != cudaSuccess) return nullptr;
     owned.push_back(p);
     return p;
   };
-  auto release = [&]() { for (void* p : owned) cudaFreeAsync(p, stream); };
+  auto release = [&]() { for (void* p : owned) tb::scratch_free(p, stream); };
   const float* hplanes[tb::P_COUNT];
   for (int p = 0; p < tb::P_COUNT; ++p) {
     hplanes[p] = L.plane[p];
@@ -931,19 +932,19 @@ static ctStatus_t host_run(const std::vector<const float*>& hin, const std::vect
                                              cudaStream_t),
                            void* ctx) {
   std::vector<void*> owned;
-  auto release = [&]() { for (void* p : owned) cudaFreeAsync(p, stream); };
+  auto release = [&]() { for (void* p : owned) tb::scratch_free(p, stream); };
   std::vector<const float*> din;
   std::vector<float*> dout;
   for (const float* h : hin) {
     void* d = nullptr;
-    if (cudaMallocAsync(&d, n * 4, stream) != cudaSuccess) { release(); return fail(CT_STATUS_ALLOC_FAILED, std::string(who) + ": device allocation failed"); }
+    if (tb::scratch_alloc(&d, n * 4, stream) != cudaSuccess) { release(); return fail(CT_STATUS_ALLOC_FAILED, std::string(who) + ": device allocation failed"); }
     owned.push_back(d);
     if (cudaMemcpyAsync(d, h, n * 4, cudaMemcpyHostToDevice, stream) != cudaSuccess) { release(); return fail(CT_STATUS_COPY_FAILED, std::string(who) + ": copy failed"); }
     din.push_back(static_cast<const float*>(d));
   }
   for (size_t i = 0; i < hout.size(); ++i) {
     void* d = nullptr;
-    if (cudaMallocAsync(&d, n * 4, stream) != cudaSuccess) { release(); return fail(CT_STATUS_ALLOC_FAILED, std::string(who) + ": device allocation failed"); }
+    if (tb::scratch_alloc(&d, n * 4, stream) != cudaSuccess) { release(); return fail(CT_STATUS_ALLOC_FAILED, std::string(who) + ": device allocation failed"); }
     owned.push_back(d);
     dout.push_back(static_cast<float*>(d));
   }

@@ -9,6 +9,7 @@
 // Outputs are staged per warp and written back with coalesced stores, so each
 // input byte is read from HBM once per launch and each output byte written once.
 #include "engine.h"
+#include "pool.h"
 #include "families.cuh"
 #include "candles.cuh"
 #include "scheduler.h"
@@ -637,7 +638,7 @@ cudaError_t launch_lookback(Launch& L, const SchedulePlan& plan, long long total
   const size_t ts_bytes = L.offsets ? (((size_t)(L.S + 1) * 8 + 255) & ~(size_t)255) : 0;
   const size_t desc_bytes = (size_t)ntiles * nslots * sizeof(LbDesc);
   unsigned char* scratch = nullptr;
-  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&scratch), head + ts_bytes + desc_bytes, stream);
+  cudaError_t e = scratch_alloc(reinterpret_cast<void**>(&scratch), head + ts_bytes + desc_bytes, stream);
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(scratch, 0, head + ts_bytes + desc_bytes, stream);
   if (e == cudaSuccess) {
@@ -661,7 +662,7 @@ cudaError_t launch_lookback(Launch& L, const SchedulePlan& plan, long long total
       if (e == cudaSuccess && herr != 0) e = cudaErrorLaunchTimeout;
     }
   }
-  const cudaError_t ef = cudaFreeAsync(scratch, stream);
+  const cudaError_t ef = scratch_free(scratch, stream);
   return e != cudaSuccess ? e : ef;
 }
 

@@ -21,8 +21,10 @@ namespace tb {
 struct __align__(16) LbDesc {
   int flag;   // 0 nothing, 1 aggregate, 2 inclusive
   int f;      // first-index carries: local (aggregate) / inclusive value, -1 = none
-  int pad0, pad1;
+  int gflag;  // last tile of a group of 32: 1 once GA/GB hold the group's aggregate
+  int pad1;
   double A[3], B[3], Y[3];
+  double GA[3], GB[3];
 };
 
 constexpr int kLbAgg = 1, kLbInc = 2;
@@ -38,6 +40,20 @@ __device__ __forceinline__ void lb_store_flag(LbDesc* d, int v) {
 }
 
 // Wait (bounded) until flag >= want; returns the flag or 0 on timeout.
+__device__ __forceinline__ int lb_wait_on(const int* flag, int want, int* err) {
+  long long spins = 0;
+  int v;
+  while ((v = *reinterpret_cast<const volatile int*>(flag)) < want) {
+    if (++spins > kLbSpinLimit) {
+      atomicExch(err, 1);
+      return 0;
+    }
+    __nanosleep(32);
+  }
+  __threadfence();
+  return v;
+}
+
 __device__ __forceinline__ int lb_wait(const LbDesc* d, int want, int* err) {
   long long spins = 0;
   int v;
@@ -66,6 +82,14 @@ __device__ __forceinline__ int lb_first_index(LbDesc* base, long long stride, in
       lb_store_flag(me, kLbAgg);
       int best = -1;
       int j = tile - 1;
+      // common case first: tile 0 (published at once) already holds the index
+      if (lb_wait(base, kLbInc, err) == kLbInc) {
+        const int f0 = *reinterpret_cast<const volatile int*>(&base->f);
+        if (f0 >= 0) {
+          best = f0;
+          j = -1;
+        }
+      }
       for (; j >= 0; --j) {
         const LbDesc* d = base + (long long)j * stride;
         const int fl = lb_wait(d, kLbAgg, err);
@@ -92,49 +116,28 @@ __device__ __forceinline__ int lb_first_index(LbDesc* base, long long stride, in
 //   init:         state before the series' first tile.
 // The state before tile t is composed from a fixed set of predecessors: the
 // aggregates of tiles stop+1 .. t-1 applied to the inclusive state of tile
-// `stop`, the latest checkpoint (a multiple of kLbSpan) or the last tile still
-// in warm-up, whichever is later. Lane l handles tile t-1-l and the warp
-// combines the maps in a fixed tree, so the result does not depend on timing.
-constexpr int kLbSpan = 32;
+// `stop`, the latest checkpoint (a multiple of kLbSpan tiles) or the last tile
+// still in warm-up, whichever is later. Whole groups of 32 tiles inside that
+// range enter through their group aggregate, which the last tile of each
+// steady group publishes; the rest enter tile by tile. Every lane composes up
+// to three consecutive items and the warp folds the lanes in a fixed tree, so
+// the result does not depend on timing. Only the checkpoints chain inclusive
+// states, one hop per kLbSpan tiles.
+constexpr int kLbGroup = 32;
+constexpr int kLbSpan = 1024;  // 32 groups
 
 template <int NC>
-__device__ __forceinline__ void lb_resolve(LbDesc* base, long long stride, int tile, const double (&tA)[NC],
-                                           const double (&tB)[NC], const double (&init)[NC], int first_steady,
-                                           double (&Y)[NC], int* err, int lane) {
-  if (tile == 0) {
+__device__ __forceinline__ void lb_compose(double (&a)[NC], double (&b)[NC], const double* A, const double* B) {
+  // (a, b) := (a, b) o (A, B): the new map is applied first
 #pragma unroll
-    for (int ch = 0; ch < NC; ++ch) Y[ch] = init[ch];
-    return;
+  for (int ch = 0; ch < NC; ++ch) {
+    b[ch] = fma(a[ch], B[ch], b[ch]);
+    a[ch] = a[ch] * A[ch];
   }
-  if (lane == 0) {
-    LbDesc* me = base + (long long)tile * stride;
-#pragma unroll
-    for (int ch = 0; ch < NC; ++ch) { me->A[ch] = tA[ch]; me->B[ch] = tB[ch]; }
-    lb_store_flag(me, kLbAgg);
-  }
-  const int ckpt = ((tile - 1) / kLbSpan) * kLbSpan;
-  int stop = first_steady - 1 > ckpt ? first_steady - 1 : ckpt;
-  if (stop > tile - 1) stop = tile - 1;
-  const int j = tile - 1 - lane;
-  double a[NC], b[NC];
-#pragma unroll
-  for (int ch = 0; ch < NC; ++ch) { a[ch] = 1.0; b[ch] = 0.0; }
-  if (j >= stop) {
-    const LbDesc* d = base + (long long)j * stride;
-    const bool inc = j == stop;
-    if (lb_wait(d, inc ? kLbInc : kLbAgg, err) != 0) {
-#pragma unroll
-      for (int ch = 0; ch < NC; ++ch) {
-        if (inc) {
-          a[ch] = 0.0;  // constant map to the inclusive state
-          b[ch] = *reinterpret_cast<const volatile double*>(&d->Y[ch]);
-        } else {
-          a[ch] = *reinterpret_cast<const volatile double*>(&d->A[ch]);
-          b[ch] = *reinterpret_cast<const volatile double*>(&d->B[ch]);
-        }
-      }
-    }
-  }
+}
+
+template <int NC>
+__device__ __forceinline__ void lb_fold(double (&a)[NC], double (&b)[NC], int lane) {
   // lane l's map is applied after lane l+1's: fold the inner maps upward
 #pragma unroll
   for (int dd = 1; dd < 32; dd <<= 1) {
@@ -148,6 +151,107 @@ __device__ __forceinline__ void lb_resolve(LbDesc* base, long long stride, int t
       }
     }
   }
+}
+
+template <int NC>
+__device__ __forceinline__ void lb_resolve(LbDesc* base, long long stride, int tile, const double (&tA)[NC],
+                                           const double (&tB)[NC], const double (&init)[NC], int first_steady,
+                                           double (&Y)[NC], int* err, int lane) {
+  if (tile == 0) {
+#pragma unroll
+    for (int ch = 0; ch < NC; ++ch) Y[ch] = init[ch];
+    return;
+  }
+  LbDesc* me = base + (long long)tile * stride;
+  if (lane == 0) {
+#pragma unroll
+    for (int ch = 0; ch < NC; ++ch) { me->A[ch] = tA[ch]; me->B[ch] = tB[ch]; }
+    lb_store_flag(me, kLbAgg);
+  }
+  double a[NC], b[NC];
+  // last tile of a steady group (other than group 0): publish the group's aggregate
+  const int g = tile / kLbGroup;
+  if (tile % kLbGroup == kLbGroup - 1 && g > 0 && g * kLbGroup >= first_steady) {
+#pragma unroll
+    for (int ch = 0; ch < NC; ++ch) { a[ch] = 1.0; b[ch] = 0.0; }
+    const int j = tile - lane;  // lane 0 = this tile (outermost)
+    if (lane == 0) {
+#pragma unroll
+      for (int ch = 0; ch < NC; ++ch) { a[ch] = tA[ch]; b[ch] = tB[ch]; }
+    } else {
+      const LbDesc* d = base + (long long)j * stride;
+      if (lb_wait(d, kLbAgg, err) != 0) {
+#pragma unroll
+        for (int ch = 0; ch < NC; ++ch) {
+          a[ch] = *reinterpret_cast<const volatile double*>(&d->A[ch]);
+          b[ch] = *reinterpret_cast<const volatile double*>(&d->B[ch]);
+        }
+      }
+    }
+    lb_fold<NC>(a, b, lane);
+    if (lane == 0) {
+#pragma unroll
+      for (int ch = 0; ch < NC; ++ch) { me->GA[ch] = a[ch]; me->GB[ch] = b[ch]; }
+      __threadfence();
+      *reinterpret_cast<volatile int*>(&me->gflag) = 1;
+    }
+  }
+  const int ckpt = ((tile - 1) / kLbSpan) * kLbSpan;
+  int stop = first_steady - 1 > ckpt ? first_steady - 1 : ckpt;
+  if (stop > tile - 1) stop = tile - 1;
+  // items after the anchor, latest first: tail tiles of this tile's group,
+  // whole groups, head tiles of the first partial group, then the anchor
+  const int first = stop + 1;                   // first tile after the anchor
+  const int tg0 = (tile / kLbGroup) * kLbGroup;  // first tile of this group
+  int nTail, nGroups, nHead, headEnd, grpEnd;
+  if (first >= tg0) {
+    nTail = tile - first;
+    nGroups = 0;
+    nHead = 0;
+    headEnd = grpEnd = 0;
+  } else {
+    nTail = tile - tg0;
+    const int gFull = (first + kLbGroup - 1) / kLbGroup;  // first whole group
+    grpEnd = tg0 / kLbGroup;                               // groups gFull .. grpEnd-1
+    nGroups = grpEnd - gFull;
+    headEnd = gFull * kLbGroup;                            // head tiles first .. headEnd-1
+    nHead = headEnd - first;
+  }
+  const int nItems = nTail + nGroups + nHead;
+#pragma unroll
+  for (int ch = 0; ch < NC; ++ch) { a[ch] = 1.0; b[ch] = 0.0; }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int r = 3 * lane + k;
+    if (r > nItems) break;
+    double A[NC], B[NC];
+    if (r == nItems) {  // the anchor: constant map to its inclusive state
+      const LbDesc* d = base + (long long)stop * stride;
+      if (lb_wait(d, kLbInc, err) == 0) break;
+#pragma unroll
+      for (int ch = 0; ch < NC; ++ch) { A[ch] = 0.0; B[ch] = *reinterpret_cast<const volatile double*>(&d->Y[ch]); }
+    } else if (r < nTail || r >= nTail + nGroups) {
+      const int j = r < nTail ? tile - 1 - r : headEnd - 1 - (r - nTail - nGroups);
+      const LbDesc* d = base + (long long)j * stride;
+      if (lb_wait(d, kLbAgg, err) == 0) break;
+#pragma unroll
+      for (int ch = 0; ch < NC; ++ch) {
+        A[ch] = *reinterpret_cast<const volatile double*>(&d->A[ch]);
+        B[ch] = *reinterpret_cast<const volatile double*>(&d->B[ch]);
+      }
+    } else {
+      const int gi = grpEnd - 1 - (r - nTail);
+      const LbDesc* d = base + ((long long)gi * kLbGroup + kLbGroup - 1) * stride;
+      if (lb_wait_on(&d->gflag, 1, err) == 0) break;
+#pragma unroll
+      for (int ch = 0; ch < NC; ++ch) {
+        A[ch] = *reinterpret_cast<const volatile double*>(&d->GA[ch]);
+        B[ch] = *reinterpret_cast<const volatile double*>(&d->GB[ch]);
+      }
+    }
+    lb_compose<NC>(a, b, A, B);
+  }
+  lb_fold<NC>(a, b, lane);
 #pragma unroll
   for (int ch = 0; ch < NC; ++ch) Y[ch] = __shfl_sync(kFull, b[ch], 0);
 }

@@ -286,3 +286,27 @@ def test_lookback_fused_pass_on_long_rows():
         for name, r in zip(onames, ref):
             compare(outs[name].cpu().numpy(), r, f"lookback fused {name}")
     plan.close()
+
+
+@pytest.mark.parametrize("name", ["ema", "macd", "rsi", "adx", "obv", "t3", "correl", "atr"])
+def test_lookback_beyond_checkpoint_span(name):
+    """Rows of 2,344 tiles (128-bar rounds): several checkpoint spans of 1,024
+    tiles, whole-group aggregates, and (single-input families) a 200,000-bar
+    leading NaN run that keeps the first 1,500 tiles in warm-up."""
+    os.environ["TACUDA_B200_MODE"] = "lb"
+    os.environ["TACUDA_B200_BARS_PER_LANE"] = "4"
+    try:
+        d = oracle_data(synthetic.ohlcv(2, 300_000, seed=29))
+        if name in SINGLE_INPUT:
+            d["close"][1, :200_000] = np.nan
+        p = DEFAULTS[name]
+        dp = device_planes(d)
+        got = to_np(call_batch_d(name, dp, p))
+        again = to_np(call_batch_d(name, dp, p))
+        ref = O.run(name, d, **p)
+        for i, (g, a, r) in enumerate(zip(got, again, ref)):
+            compare(g, r, f"span {name}[{i}]")
+            np.testing.assert_array_equal(g.view(np.uint32), a.view(np.uint32))
+    finally:
+        del os.environ["TACUDA_B200_MODE"]
+        del os.environ["TACUDA_B200_BARS_PER_LANE"]
