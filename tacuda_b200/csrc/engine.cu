@@ -136,10 +136,14 @@ __global__ void __launch_bounds__(256, (K <= 8 ? 2 : 1)) batch_kernel(const __gr
     c.err = L.err;
     const long long tps = L.lb_tile_start ? 0 : (L.T + TILE - 1) / TILE;
     const long long ntiles = L.lb_tile_start ? L.lb_tile_start[L.S] : L.lb_tiles;
-    for (;;) {
-      unsigned long long g = 0;
-      if (lane == 0) g = atomicAdd(L.lb_counter, 1ull);
-      g = __shfl_sync(kFull, g, 0);
+    for (long long pass = 0;; ++pass) {
+      // tiles in order from the counter; without recurrence carries (no
+      // counter) tiles are independent and assigned statically
+      unsigned long long g = (unsigned long long)(pass * W + gw);
+      if (L.lb_counter) {
+        if (lane == 0) g = atomicAdd(L.lb_counter, 1ull);
+        g = __shfl_sync(kFull, g, 0);
+      }
       if ((long long)g >= ntiles) break;
       long long s, first;
       if (L.lb_tile_start) {
@@ -630,6 +634,17 @@ cudaError_t launch_lookback(Launch& L, const SchedulePlan& plan, long long total
   for (int j = 0; j < L.njobs; ++j) {
     L.jobs[j].lb_slot = nslots;
     nslots += lb_slots(L.jobs[j]);
+  }
+  if (nslots == 0 && !L.offsets) {
+    // windows only: independent tiles, no scratch
+    L.lb = 1;
+    L.lb_counter = nullptr;
+    L.err = nullptr;
+    L.lb_tile_start = nullptr;
+    L.lb_desc = nullptr;
+    L.lb_nslots = 0;
+    L.lb_tiles = (long long)L.S * ((L.T + TILE - 1) / TILE);
+    return launch_k<K>(L, plan, stream, stats);
   }
   if (nslots == 0) nslots = 1;
   // bound on the tile count (exact for uniform rows)

@@ -28,7 +28,7 @@ struct __align__(16) LbDesc {
 };
 
 constexpr int kLbAgg = 1, kLbInc = 2;
-constexpr long long kLbSpinLimit = 1ll << 26;  // about a second of polling
+constexpr long long kLbSpinLimit = 1ll << 26;  // polls / 32 at up to 1 us each: about two seconds
 
 __device__ __forceinline__ int lb_load_flag(const LbDesc* d) {
   return *reinterpret_cast<const volatile int*>(&d->flag);
@@ -42,27 +42,51 @@ __device__ __forceinline__ void lb_store_flag(LbDesc* d, int v) {
 // Wait (bounded) until flag >= want; returns the flag or 0 on timeout.
 __device__ __forceinline__ int lb_wait_on(const int* flag, int want, int* err) {
   long long spins = 0;
+  unsigned ns = 32;
   int v;
   while ((v = *reinterpret_cast<const volatile int*>(flag)) < want) {
-    if (++spins > kLbSpinLimit) {
+    if (++spins > (kLbSpinLimit >> 5)) {
       atomicExch(err, 1);
       return 0;
     }
-    __nanosleep(32);
+    __nanosleep(ns);
+    if (ns < 1024) ns <<= 1;
   }
   __threadfence();
   return v;
 }
 
+// Warp-uniform wait: every lane with `active` set waits until *flag >= want.
+// The warp polls together with a growing back-off, so waiting lanes neither
+// diverge nor flood L2 with polls. Returns false (and sets *err) on timeout.
+__device__ __forceinline__ bool lb_wait_all(const int* flag, int want, bool active, int* err) {
+  long long spins = 0;
+  unsigned ns = 32;
+  for (;;) {
+    const bool ok = !active || *reinterpret_cast<const volatile int*>(flag) >= want;
+    if (__all_sync(kFull, ok)) break;
+    if (++spins > (kLbSpinLimit >> 5)) {
+      if (active) atomicExch(err, 1);
+      return false;
+    }
+    __nanosleep(ns);
+    if (ns < 1024) ns <<= 1;
+  }
+  __threadfence();
+  return true;
+}
+
 __device__ __forceinline__ int lb_wait(const LbDesc* d, int want, int* err) {
   long long spins = 0;
+  unsigned ns = 32;
   int v;
   while ((v = lb_load_flag(d)) < want) {
-    if (++spins > kLbSpinLimit) {
+    if (++spins > (kLbSpinLimit >> 5)) {
       atomicExch(err, 1);
       return 0;
     }
-    __nanosleep(32);
+    __nanosleep(ns);
+    if (ns < 1024) ns <<= 1;
   }
   __threadfence();
   return v;
@@ -175,17 +199,16 @@ __device__ __forceinline__ void lb_resolve(LbDesc* base, long long stride, int t
 #pragma unroll
     for (int ch = 0; ch < NC; ++ch) { a[ch] = 1.0; b[ch] = 0.0; }
     const int j = tile - lane;  // lane 0 = this tile (outermost)
+    const LbDesc* d = base + (long long)j * stride;
+    const bool ok = lb_wait_all(&d->flag, kLbAgg, lane != 0, err);
     if (lane == 0) {
 #pragma unroll
       for (int ch = 0; ch < NC; ++ch) { a[ch] = tA[ch]; b[ch] = tB[ch]; }
-    } else {
-      const LbDesc* d = base + (long long)j * stride;
-      if (lb_wait(d, kLbAgg, err) != 0) {
+    } else if (ok) {
 #pragma unroll
-        for (int ch = 0; ch < NC; ++ch) {
-          a[ch] = *reinterpret_cast<const volatile double*>(&d->A[ch]);
-          b[ch] = *reinterpret_cast<const volatile double*>(&d->B[ch]);
-        }
+      for (int ch = 0; ch < NC; ++ch) {
+        a[ch] = *reinterpret_cast<const volatile double*>(&d->A[ch]);
+        b[ch] = *reinterpret_cast<const volatile double*>(&d->B[ch]);
       }
     }
     lb_fold<NC>(a, b, lane);
@@ -220,36 +243,52 @@ __device__ __forceinline__ void lb_resolve(LbDesc* base, long long stride, int t
   const int nItems = nTail + nGroups + nHead;
 #pragma unroll
   for (int ch = 0; ch < NC; ++ch) { a[ch] = 1.0; b[ch] = 0.0; }
+  bool ok = true;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const int r = 3 * lane + k;
-    if (r > nItems) break;
-    double A[NC], B[NC];
-    if (r == nItems) {  // the anchor: constant map to its inclusive state
-      const LbDesc* d = base + (long long)stop * stride;
-      if (lb_wait(d, kLbInc, err) == 0) break;
-#pragma unroll
-      for (int ch = 0; ch < NC; ++ch) { A[ch] = 0.0; B[ch] = *reinterpret_cast<const volatile double*>(&d->Y[ch]); }
-    } else if (r < nTail || r >= nTail + nGroups) {
-      const int j = r < nTail ? tile - 1 - r : headEnd - 1 - (r - nTail - nGroups);
-      const LbDesc* d = base + (long long)j * stride;
-      if (lb_wait(d, kLbAgg, err) == 0) break;
-#pragma unroll
-      for (int ch = 0; ch < NC; ++ch) {
-        A[ch] = *reinterpret_cast<const volatile double*>(&d->A[ch]);
-        B[ch] = *reinterpret_cast<const volatile double*>(&d->B[ch]);
-      }
-    } else {
-      const int gi = grpEnd - 1 - (r - nTail);
-      const LbDesc* d = base + ((long long)gi * kLbGroup + kLbGroup - 1) * stride;
-      if (lb_wait_on(&d->gflag, 1, err) == 0) break;
-#pragma unroll
-      for (int ch = 0; ch < NC; ++ch) {
-        A[ch] = *reinterpret_cast<const volatile double*>(&d->GA[ch]);
-        B[ch] = *reinterpret_cast<const volatile double*>(&d->GB[ch]);
+    const bool active = r <= nItems;
+    // the item's descriptor, the flag to wait for and the map's fields
+    const LbDesc* d = base;
+    const int* flag = &base->flag;
+    int want = kLbAgg;
+    int kind = 0;  // 0 tile aggregate, 1 group aggregate, 2 anchor
+    if (active) {
+      if (r == nItems) {
+        d = base + (long long)stop * stride;
+        flag = &d->flag;
+        want = kLbInc;
+        kind = 2;
+      } else if (r < nTail || r >= nTail + nGroups) {
+        const int j = r < nTail ? tile - 1 - r : headEnd - 1 - (r - nTail - nGroups);
+        d = base + (long long)j * stride;
+        flag = &d->flag;
+      } else {
+        const int gi = grpEnd - 1 - (r - nTail);
+        d = base + ((long long)gi * kLbGroup + kLbGroup - 1) * stride;
+        flag = &d->gflag;
+        want = 1;
+        kind = 1;
       }
     }
-    lb_compose<NC>(a, b, A, B);
+    ok = lb_wait_all(flag, want, active && ok, err) && ok;
+    if (active && ok) {
+      double A[NC], B[NC];
+#pragma unroll
+      for (int ch = 0; ch < NC; ++ch) {
+        if (kind == 2) {  // the anchor: constant map to its inclusive state
+          A[ch] = 0.0;
+          B[ch] = *reinterpret_cast<const volatile double*>(&d->Y[ch]);
+        } else if (kind == 1) {
+          A[ch] = *reinterpret_cast<const volatile double*>(&d->GA[ch]);
+          B[ch] = *reinterpret_cast<const volatile double*>(&d->GB[ch]);
+        } else {
+          A[ch] = *reinterpret_cast<const volatile double*>(&d->A[ch]);
+          B[ch] = *reinterpret_cast<const volatile double*>(&d->B[ch]);
+        }
+      }
+      lb_compose<NC>(a, b, A, B);
+    }
   }
   lb_fold<NC>(a, b, lane);
 #pragma unroll
