@@ -294,6 +294,12 @@ typedef struct ctB200Job {
   uint64_t cdl_mask;
   int64_t cdl_stride;
   int cdl_int32;
+  /* Arithmetic of SMA SUM WMA BBANDS STDDEV VAR LINEARREG CORREL EMA:
+   * 0 FP64 (default), 1 plain FP32, 2 compensated FP32 (float pairs with
+   * two-sum / two-product), 3 FP32 per bar with FP64 carries between lanes and
+   * tiles (EMA; the windows carry nothing). Other families accept only 0. All
+   * jobs of one launch use the same precision. */
+  int precision;
 } ctB200Job;
 
 /* Evaluate all jobs over a uniform batch in one kernel launch. */

@@ -52,7 +52,7 @@ class ctB200Series(ct.Structure):
 class ctB200Job(ct.Structure):
     _fields_ = [("family", _I), ("params", _I * 3), ("fparams", ct.c_double * 2), ("inputs", _I * 4),
                 ("outputs", _P * 3), ("cdl_mask", ct.c_uint64), ("cdl_stride", ct.c_int64),
-                ("cdl_int32", _I)]
+                ("cdl_int32", _I), ("precision", _I)]
 
 
 class ctB200AlphaParams(ct.Structure):
@@ -224,8 +224,11 @@ def stochastic_batch(high: Any, low: Any, close: Any, kPeriod: int = 14, dPeriod
 
 # --- fused jobs ----------------------------------------------------------------
 
+PRECISIONS = {"fp64": 0, "fp32": 1, "fp32c": 2, "fp32/fp64carry": 3}
+
+
 def make_job(family: str, params=(), fparams=(), outputs=(), inputs=None, cdl_mask: int = 0,
-             cdl_stride: int = 0, cdl_int32: bool = False) -> ctB200Job:
+             cdl_stride: int = 0, cdl_int32: bool = False, precision="fp64") -> ctB200Job:
     j = ctB200Job()
     j.family = FAMILY_ID[family]
     for i, v in enumerate(params):
@@ -242,6 +245,7 @@ def make_job(family: str, params=(), fparams=(), outputs=(), inputs=None, cdl_ma
     j.cdl_mask = int(cdl_mask)
     j.cdl_stride = int(cdl_stride)
     j.cdl_int32 = 1 if cdl_int32 else 0
+    j.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
     return j
 
 

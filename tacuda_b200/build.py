@@ -20,7 +20,11 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OUT = PKG / "libtacuda_b200.so"
-SOURCES = ["engine.cu", "adjoint.cu", "api.cu", "scheduler.cpp", "pool.cpp"]
+# (source, object name, extra defines): engine.cu is compiled twice, the second
+# time for the kernels of the precision variants only
+SOURCES = [("engine.cu", "engine.cu.o", []), ("engine.cu", "engine_prec.cu.o", ["-DTB_PREC_TU"]),
+           ("adjoint.cu", "adjoint.cu.o", []), ("api.cu", "api.cu.o", []),
+           ("scheduler.cpp", "scheduler.cpp.o", []), ("pool.cpp", "pool.cpp.o", [])]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -36,21 +40,27 @@ def _run(cmd):
 
 
 def build_library(verbose: bool = False) -> Path:
-    srcs = [s for s in SOURCES if (CSRC / s).exists()]
+    from concurrent.futures import ThreadPoolExecutor
     objdir = ROOT / "_build"
     objdir.mkdir(exist_ok=True)
-    objs = []
-    for s in srcs:
-        obj = objdir / (s + ".o")
-        src = CSRC / s
-        deps = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(CSRC.glob("*.inc")) + [ROOT / "include" / "tacuda.h", src]
-        if not obj.exists() or any(d.stat().st_mtime > obj.stat().st_mtime for d in deps):
+    deps = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(CSRC.glob("*.inc")) + [ROOT / "include" / "tacuda.h"]
+    jobs, objs = [], []
+    for src_name, obj_name, defines in SOURCES:
+        src = CSRC / src_name
+        if not src.exists():
+            continue
+        obj = objdir / obj_name
+        objs.append(str(obj))
+        if not obj.exists() or any(d.stat().st_mtime > obj.stat().st_mtime for d in deps + [src]):
             cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC,-fvisibility=hidden",
-                   f"-I{ROOT / 'include'}", f"-I{CSRC}", "-c", str(src), "-o", str(obj)]
+                   f"-I{ROOT / 'include'}", f"-I{CSRC}", *defines, "-c", str(src), "-o", str(obj)]
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
-            _run(cmd)
-        objs.append(str(obj))
+            jobs.append(cmd)
+    # translation units compile in parallel (the two engine halves dominate)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_run, cmd) for cmd in jobs]:
+            f.result()
     _run([nvcc(), *ARCH, "-shared", "-o", str(OUT), *objs])
     return OUT
 

@@ -80,6 +80,13 @@ ctStatus_t make_job(const ctB200Job& u, Job& j, const char* who) {
   if (u.family < 0 || u.family >= tb::F_COUNT) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": unknown family");
   for (int i = 0; i < 3; ++i) j.ip[i] = u.params[i];
   const int f = u.family;
+  j.prec = u.precision;
+  if (u.precision < 0 || u.precision > 3)
+    return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": precision must be 0..3");
+  if (u.precision != 0 && f != tb::F_SMA && f != tb::F_SUM && f != tb::F_WMA && f != tb::F_BBANDS &&
+      f != tb::F_STDDEV && f != tb::F_VAR && f != tb::F_LINEARREG && f != tb::F_CORREL && f != tb::F_EMA)
+    return fail(CT_STATUS_INVALID_ARGUMENT,
+                std::string(who) + ": precision variants exist for SMA SUM WMA BBANDS STDDEV VAR LINEARREG CORREL EMA");
   const int mp = min_period(f);
   if (mp > 0 && u.params[0] < mp) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": invalid period");
   if ((f == tb::F_MACD && (u.params[1] < 1 || u.params[2] < 1)) ||
@@ -578,6 +585,8 @@ static ctStatus_t build_launch(const ctB200Series* series, const ctB200Job* jobs
   for (int j = 0; j < numJobs; ++j) {
     const ctStatus_t st = make_job(jobs[j], L.jobs[j], who);
     if (st != CT_STATUS_SUCCESS) return st;
+    if (L.jobs[j].prec != L.jobs[0].prec)
+      return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": all jobs of a launch need the same precision");
   }
   return check_planes(L, who);
 }
@@ -603,9 +612,12 @@ ctStatus_t ct_b200_fused_lookback_static_d(const ctB200Series* series, const ctB
   ctStatus_t st = build_launch(series, jobs, numJobs, L, who);
   if (st != CT_STATUS_SUCCESS) return st;
   if (L.offsets) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": uniform rows only");
-  for (int j = 0; j < L.njobs; ++j)
+  for (int j = 0; j < L.njobs; ++j) {
     if (L.jobs[j].family == tb::F_CDL)
       return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": candle jobs are not supported");
+    if (L.jobs[j].prec != 0)
+      return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": FP64 jobs only");
+  }
   tb::SchedulePlan plan = tb::plan_for(L, L.T * (long long)L.S, L.T);
   plan.mode = 2;
   size_t need = 0;

@@ -8,14 +8,22 @@
 // them; per-job recurrence state is carried between rounds in shared memory.
 // Outputs are staged per warp and written back with coalesced stores, so each
 // input byte is read from HBM once per launch and each output byte written once.
+//
+// This file is compiled twice: normally (FP64 engines, candles, entry-side
+// launch logic) and with TB_PREC_TU defined, which builds only the kernels of
+// the precision variants (launch_prec), so the two halves compile in parallel.
 #include "engine.h"
 #include "pool.h"
 #include "families.cuh"
-#include "candles.cuh"
+#include "families_prec.cuh"
 #include "scheduler.h"
+#ifndef TB_PREC_TU
+#include "candles.cuh"
 #include "sp_candles.cuh"
+#endif
 
 #include <algorithm>
+#include <type_traits>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -33,8 +41,32 @@ struct SmemLayout {
   int plane_slot[P_COUNT];
 };
 
-template <int K>
+// Precision variants: P = 1 plain FP32, 2 compensated FP32, 3 FP32 bars with
+// FP64 carries (families_prec.cuh); other families run in FP64.
+template <int K, int P>
+__device__ __forceinline__ bool run_job_prec(const Ctx<K>& c, const Job& j, Carry& cy) {
+  // T: per-bar terms and state, C: running sums and carries
+  using T = typename std::conditional<P == 2, F2, float>::type;
+  using C = typename std::conditional<P == 2, F2, typename std::conditional<P == 3, double, float>::type>::type;
+  switch (j.family) {
+    case F_SMA: sum_window_p<K, T, C>(c, j, 0); return true;
+    case F_SUM: sum_window_p<K, T, C>(c, j, 1); return true;
+    case F_WMA: sum_window_p<K, T, C>(c, j, 2); return true;
+    case F_BBANDS: moment_window_p<K, T, C>(c, j, 0); return true;
+    case F_STDDEV: moment_window_p<K, T, C>(c, j, 1); return true;
+    case F_VAR: moment_window_p<K, T, C>(c, j, 2); return true;
+    case F_LINEARREG: linreg_p<K, T, C>(c, j); return true;
+    case F_CORREL: correl_p<K, T, C>(c, j, cy); return true;
+    case F_EMA: ema_p<K, T, C>(c, j, cy); return true;
+    default: return false;
+  }
+}
+
+template <int K, int P>
 __device__ __forceinline__ void run_job(const Ctx<K>& c, const Job& j, Carry& cy) {
+  if constexpr (P != 0) {
+    if (run_job_prec<K, P>(c, j, cy)) return;
+  }
   switch (j.family) {
     case F_SMA: sum_window_round(c, j, 0); break;
     case F_SUM: sum_window_round(c, j, 1); break;
@@ -73,7 +105,7 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src, bool val
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
 }
 
-template <int K>
+template <int K, int P>
 __global__ void __launch_bounds__(256, (K <= 8 ? 2 : 1)) batch_kernel(const __grid_constant__ Launch L, const SmemLayout lay) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int TILE = 32 * K;
@@ -171,7 +203,7 @@ __global__ void __launch_bounds__(256, (K <= 8 ? 2 : 1)) batch_kernel(const __gr
         cy.f = -1;
 #pragma unroll
         for (int v = 0; v < 10; ++v) cy.v[v] = 0.0;
-        run_job<K>(c, L.jobs[j], cy);
+        run_job<K, P>(c, L.jobs[j], cy);
         __syncwarp();
       }
     }
@@ -200,7 +232,7 @@ __global__ void __launch_bounds__(256, (K <= 8 ? 2 : 1)) batch_kernel(const __gr
       stage_round_inputs(t0);
       for (int j = 0; j < L.njobs; ++j) {
         Carry cy = carry[j];
-        run_job<K>(c, L.jobs[j], cy);
+        run_job<K, P>(c, L.jobs[j], cy);
         __syncwarp();
         if (lane == 0) carry[j] = cy;
         __syncwarp();
@@ -209,6 +241,7 @@ __global__ void __launch_bounds__(256, (K <= 8 ? 2 : 1)) batch_kernel(const __gr
   }
 }
 
+#ifndef TB_PREC_TU
 // ------------------------------------------------------- series-parallel
 
 __device__ void sp_run_job(sp::Driver& drv, const Job& j, const sp::Stage& st, const sp::Line& ln, int lane) {
@@ -298,9 +331,11 @@ __global__ void __launch_bounds__(768) sp_kernel(const __grid_constant__ Launch 
   }
 }
 
+#endif  // TB_PREC_TU
+
 // First look-back tile of every ragged series: tile_start[s] = sum over
 // earlier series of ceil(n / tile), tile_start[S] = total. One block.
-__global__ void __launch_bounds__(1024) lb_tile_start_kernel(const long long* offsets, int S, int tile,
+static __global__ void __launch_bounds__(1024) lb_tile_start_kernel(const long long* offsets, int S, int tile,
                                                              long long* tile_start) {
   __shared__ long long part[1024];
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -428,7 +463,7 @@ struct OccEntry { int k, warps, smem, per_sm; };
 struct DeviceInfo {
   int sms = 0;
   int smem_optin = 0;
-  bool attr_set[3] = {false, false, false};
+  bool attr_set[3][4] = {};
   bool sp_attr = false;
   int cdl_per_sm = 0;
   std::vector<OccEntry> occ;
@@ -450,7 +485,7 @@ DeviceInfo& device_info(int dev) {
   return d;
 }
 
-template <int K>
+template <int K, int P = 0>
 cudaError_t launch_k(Launch& L, const SchedulePlan& plan, cudaStream_t stream, LaunchStats* stats) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -467,17 +502,17 @@ cudaError_t launch_k(Launch& L, const SchedulePlan& plan, cudaStream_t stream, L
   int per_sm = -1;
   {
     std::lock_guard<std::mutex> lk(g_mutex);
-    if (!di.attr_set[k_slot(K)]) {
-      e = cudaFuncSetAttribute(batch_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, di.smem_optin);
+    if (!di.attr_set[k_slot(K)][P]) {
+      e = cudaFuncSetAttribute(batch_kernel<K, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, di.smem_optin);
       if (e != cudaSuccess) return e;
-      di.attr_set[k_slot(K)] = true;
+      di.attr_set[k_slot(K)][P] = true;
     }
     for (const OccEntry& o : di.occ)
-      if (o.k == K && o.warps == warps && o.smem == (int)smem) per_sm = o.per_sm;
+      if (o.k == K + 100 * P && o.warps == warps && o.smem == (int)smem) per_sm = o.per_sm;
     if (per_sm < 0) {
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<K>, warps * 32, smem);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<K, P>, warps * 32, smem);
       if (e != cudaSuccess) return e;
-      di.occ.push_back({K, warps, (int)smem, per_sm});
+      di.occ.push_back({K + 100 * P, warps, (int)smem, per_sm});
     }
   }
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
@@ -488,7 +523,7 @@ cudaError_t launch_k(Launch& L, const SchedulePlan& plan, cudaStream_t stream, L
   if (plan.max_blocks > 0) cap = std::min<long long>(cap, plan.max_blocks);
   const int blocks = (int)std::max<long long>(1, std::min(want, cap));
   L.total_warps = blocks * warps;
-  batch_kernel<K><<<blocks, warps * 32, smem, stream>>>(L, lay);
+  batch_kernel<K, P><<<blocks, warps * 32, smem, stream>>>(L, lay);
   if (stats) {
     stats->blocks = blocks;
     stats->warps_per_block = warps;
@@ -499,6 +534,7 @@ cudaError_t launch_k(Launch& L, const SchedulePlan& plan, cudaStream_t stream, L
   return cudaGetLastError();
 }
 
+#ifndef TB_PREC_TU
 cudaError_t launch_sp(Launch& L, const SchedulePlan& plan, cudaStream_t stream, LaunchStats* stats) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -584,8 +620,11 @@ cudaError_t launch_sp(Launch& L, const SchedulePlan& plan, cudaStream_t stream, 
   return cudaGetLastError();
 }
 
+#endif  // TB_PREC_TU
+
 }  // namespace
 
+#ifndef TB_PREC_TU
 int max_lookback_halo(const Launch& L) {
   int h = 1;
   for (int j = 0; j < L.njobs; ++j) h = std::max(h, job_halo(L.jobs[j]));
@@ -626,7 +665,9 @@ cudaError_t launch_candles(const Launch& L, const Job* jobs, int n, cudaStream_t
   return cudaSuccess;
 }
 
-template <int K>
+#endif  // TB_PREC_TU
+
+template <int K, int P>
 cudaError_t launch_lookback(Launch& L, const SchedulePlan& plan, long long total_bars, cudaStream_t stream,
                             LaunchStats* stats) {
   constexpr int TILE = 32 * K;
@@ -644,7 +685,7 @@ cudaError_t launch_lookback(Launch& L, const SchedulePlan& plan, long long total
     L.lb_desc = nullptr;
     L.lb_nslots = 0;
     L.lb_tiles = (long long)L.S * ((L.T + TILE - 1) / TILE);
-    return launch_k<K>(L, plan, stream, stats);
+    return launch_k<K, P>(L, plan, stream, stats);
   }
   if (nslots == 0) nslots = 1;
   // bound on the tile count (exact for uniform rows)
@@ -668,7 +709,7 @@ cudaError_t launch_lookback(Launch& L, const SchedulePlan& plan, long long total
       lb_tile_start_kernel<<<1, 1024, 0, stream>>>(L.offsets, L.S, TILE, L.lb_tile_start);
       e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = launch_k<K>(L, plan, stream, stats);
+    if (e == cudaSuccess) e = launch_k<K, P>(L, plan, stream, stats);
     if (e == cudaSuccess && stream == 0) {
       // synchronous calls report a look-back wait that ran out
       int herr = 0;
@@ -680,6 +721,22 @@ cudaError_t launch_lookback(Launch& L, const SchedulePlan& plan, long long total
   const cudaError_t ef = scratch_free(scratch, stream);
   return e != cudaSuccess ? e : ef;
 }
+
+#ifdef TB_PREC_TU
+// Precision variants (rounds of 512 bars): warp-scan or look-back engine.
+cudaError_t launch_prec(Launch& L, const SchedulePlan& plan, long long total_bars, cudaStream_t stream,
+                        LaunchStats* stats) {
+  const bool lb = plan.mode == 2;
+  switch (L.jobs[0].prec) {
+    case 1: return lb ? launch_lookback<16, 1>(L, plan, total_bars, stream, stats) : launch_k<16, 1>(L, plan, stream, stats);
+    case 2: return lb ? launch_lookback<16, 2>(L, plan, total_bars, stream, stats) : launch_k<16, 2>(L, plan, stream, stats);
+    case 3: return lb ? launch_lookback<16, 3>(L, plan, total_bars, stream, stats) : launch_k<16, 3>(L, plan, stream, stats);
+    default: return cudaErrorInvalidValue;
+  }
+}
+#else
+cudaError_t launch_prec(Launch& L, const SchedulePlan& plan, long long total_bars, cudaStream_t stream,
+                        LaunchStats* stats);
 
 // Look-back scratch of the allocation-free entry point: a file-scope device
 // array (one copy per device, created when the module loads there). Its
@@ -776,7 +833,7 @@ cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, long long total_ba
   L.need_tp = need_tp;
   const int h = max_lookback_halo(L);
   L.halo = ((h + 31) / 32) * 32;
-  if (plan.mode == 1) return launch_sp(L, plan, stream, stats);
+  if (plan.mode == 1 && !(L.njobs > 0 && L.jobs[0].prec != 0)) return launch_sp(L, plan, stream, stats);
   // candle jobs go to the bar-parallel tile kernel, the rest to the engine
   int ncdl = 0;
   Job cdl_jobs[kMaxJobs];
@@ -793,11 +850,12 @@ cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, long long total_ba
     return launch_candles(L, cdl_jobs, ncdl, stream);
   }
   L.lb = 0;
+  if (L.njobs > 0 && L.jobs[0].prec != 0) return launch_prec(L, plan, total_bars, stream, stats);
   if (plan.mode == 2) {
     switch (plan.k) {
-      case 4: return launch_lookback<4>(L, plan, total_bars, stream, stats);
-      case 16: return launch_lookback<16>(L, plan, total_bars, stream, stats);
-      default: return launch_lookback<8>(L, plan, total_bars, stream, stats);
+      case 4: return launch_lookback<4, 0>(L, plan, total_bars, stream, stats);
+      case 16: return launch_lookback<16, 0>(L, plan, total_bars, stream, stats);
+      default: return launch_lookback<8, 0>(L, plan, total_bars, stream, stats);
     }
   }
   switch (plan.k) {
@@ -806,5 +864,7 @@ cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, long long total_ba
     default: return launch_k<8>(L, plan, stream, stats);
   }
 }
+
+#endif  // TB_PREC_TU
 
 }  // namespace tb

@@ -36,6 +36,7 @@ struct Job {
   int cdl_int32;
   int halo;         // bars of history this job reads before a round
   int lb_slot;      // first look-back descriptor slot of this job (look-back mode)
+  int prec;         // 0 FP64, 1 FP32, 2 compensated FP32, 3 FP32 with FP64 carries
 };
 
 struct LbDesc;

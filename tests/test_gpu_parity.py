@@ -310,3 +310,54 @@ def test_lookback_beyond_checkpoint_span(name):
     finally:
         del os.environ["TACUDA_B200_MODE"]
         del os.environ["TACUDA_B200_BARS_PER_LANE"]
+
+
+PREC_JOBS = [("sma", dict(period=200)), ("stddev", dict(period=200, nbdev=1.0)), ("var", dict(period=200)),
+             ("linearreg", dict(period=200)), ("correl", dict(period=30)), ("ema", dict(period=500)),
+             ("bbands", dict(period=20, up=2.0, dn=1.5)), ("wma", dict(period=30)), ("sum", dict(period=50))]
+# tolerance of each precision variant against the FP64 oracle on a +1e4-level
+# random walk: |gpu - ref| <= tol*|ref| + tol*max|ref row|. Plain FP32 has no
+# bound there (its running sums lose the digits the level offset cancels); it
+# is only checked for its NaN mask, and its error is what the long-series
+# precision report measures.
+PREC_TOL = {"fp32": None, "fp32c": 1e-6, "fp32/fp64carry": 1e-5}
+
+
+@pytest.mark.parametrize("engine", ["ws", "lb"])
+@pytest.mark.parametrize("prec", sorted(PREC_TOL))
+def test_precision_variants_on_level_offset_rows(prec, engine):
+    """FP32, compensated FP32 and FP32-with-FP64-carry variants of the long
+    window families and the EMA, against the FP64 oracle on level-offset
+    rows (the long-series precision stress at a testable size)."""
+    os.environ["TACUDA_B200_MODE"] = engine
+    try:
+        S, T = 3, 20000
+        x = synthetic.level_walk(S, T, seed=41)
+        y = synthetic.level_walk(S, T, seed=42)
+        d = {"close": x, "x": x, "y": y, "aux": y}
+        dx = torch.from_numpy(x).cuda()
+        dy = torch.from_numpy(y).cuda()
+        for name, params in PREC_JOBS:
+            fam = name
+            nout = 3 if name == "bbands" else 1
+            outs = [torch.full((S, T), 777.0, device="cuda") for _ in range(nout)]
+            spec_p = tuple(v for k, v in params.items() if k == "period")
+            fp = tuple(v for k, v in params.items() if k in ("nbdev", "up", "dn"))
+            job = tb.make_job(fam, spec_p, fp, [o.data_ptr() for o in outs],
+                              inputs=("close", "aux") if name == "correl" else None, precision=prec)
+            series = tb.make_series({"close": dx.data_ptr(), "aux": dy.data_ptr()}, S, T)
+            tb.fused_batch_d(series, [job], 0)
+            torch.cuda.synchronize()
+            ref = O.run(name, d, **params)
+            tol = PREC_TOL[prec]
+            for i, (g, r) in enumerate(zip(outs, ref)):
+                g = g.cpu().numpy().astype(np.float64)
+                np.testing.assert_array_equal(np.isnan(g), np.isnan(r), err_msg=f"{prec} {name} NaN mask")
+                if tol is None:
+                    continue
+                m = ~np.isnan(r)
+                bound = tol * np.abs(r[m]) + tol * np.max(np.abs(r[m]))
+                err = np.abs(g[m] - r[m])
+                assert np.all(err <= bound), f"{prec} {engine} {name}[{i}]: worst excess {np.max(err - bound)}"
+    finally:
+        del os.environ["TACUDA_B200_MODE"]
