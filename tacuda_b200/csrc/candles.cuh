@@ -27,6 +27,7 @@ constexpr int kAnchors = kTileBars + sp::kCdlBack;
 struct TileSmem {
   float o[kSpan], h[kSpan], l[kSpan], c[kSpan];
   double rng[3][kSpan];         // body, high-low, shadows of each staged bar
+  double us[kSpan], ls[kSpan];  // upper and lower shadow of each staged bar
   double mean[4][kAnchors];     // trailing mean of each table slot at anchors t0-5 ..
 };
 
@@ -40,8 +41,8 @@ struct TileBars {
   __device__ __forceinline__ float L(int d) const { return s->l[i - d]; }
   __device__ __forceinline__ float C(int d) const { return s->c[i - d]; }
   __device__ __forceinline__ double RB(int d) const { return s->rng[0][i - d]; }
-  __device__ __forceinline__ double US(int d) const { return (double)H(d) - fmax((double)O(d), (double)C(d)); }
-  __device__ __forceinline__ double LS(int d) const { return fmin((double)O(d), (double)C(d)) - (double)L(d); }
+  __device__ __forceinline__ double US(int d) const { return s->us[i - d]; }
+  __device__ __forceinline__ double LS(int d) const { return s->ls[i - d]; }
   __device__ __forceinline__ int COL(int d) const { return C(d) >= O(d) ? 1 : -1; }
   __device__ __forceinline__ float TOP(int d) const { return fmaxf(O(d), C(d)); }
   __device__ __forceinline__ float BOT(int d) const { return fminf(O(d), C(d)); }
@@ -52,8 +53,8 @@ struct TileBars {
   // TA-Lib candle average of setting st anchored at bar t-d:
   // factor * (sum / count) / divisor, the mean precomputed per anchor.
   __device__ __forceinline__ double AVG(int st, int d) const {
-    const int slot = sp::kSetSlot[st];
-    const double factor = (double)sp::kSetFactor[st];
+    const int slot = sp::set_slot(st);
+    const double factor = (double)sp::set_factor(st);
     if (slot < 0) return factor * RB(d);
     const double m = s->mean[slot][i - kHalo - d + sp::kCdlBack];
     return slot == 2 ? factor * m / 2.0 : factor * m;
@@ -100,6 +101,8 @@ __global__ void __launch_bounds__(kTileBars) tile_kernel(const __grid_constant__
         sm.rng[0][i] = sp::cdl_range(sp::CR_BODY, o, h, l, c);
         sm.rng[1][i] = sp::cdl_range(sp::CR_HL, o, h, l, c);
         sm.rng[2][i] = sp::cdl_range(sp::CR_SHADOW, o, h, l, c);
+        sm.us[i] = (double)h - fmax((double)o, (double)c);
+        sm.ls[i] = fmin((double)o, (double)c) - (double)l;
       }
       __syncthreads();
       for (int j = tid; j < 4 * kAnchors; j += kTileBars) {

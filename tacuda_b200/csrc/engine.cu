@@ -221,21 +221,25 @@ __global__ void __launch_bounds__(256, (K <= 8 ? 2 : 1)) batch_kernel(const __gr
       c.base = (long long)s * L.T;
       c.n = (int)L.T;
     }
-    for (int j = 0; j < L.njobs; ++j) {
-      if (lane == 0) {
-        carry[j].f = -1;
-        for (int v = 0; v < 10; ++v) carry[j].v[v] = 0.0;
-      }
-    }
-    __syncwarp();
     for (int t0 = 0; t0 < c.n; t0 += TILE) {
       stage_round_inputs(t0);
+      const bool first = t0 == 0, last = t0 + TILE >= c.n;
       for (int j = 0; j < L.njobs; ++j) {
-        Carry cy = carry[j];
+        // a row's first round starts from the empty carry, its last keeps none
+        Carry cy;
+        if (first) {
+          cy.f = -1;
+#pragma unroll
+          for (int v = 0; v < 10; ++v) cy.v[v] = 0.0;
+        } else {
+          cy = carry[j];
+        }
         run_job<K, P>(c, L.jobs[j], cy);
-        __syncwarp();
-        if (lane == 0) carry[j] = cy;
-        __syncwarp();
+        if (!last) {
+          __syncwarp();
+          if (lane == 0) carry[j] = cy;
+          __syncwarp();
+        }
       }
     }
   }

@@ -1,8 +1,8 @@
 // Launch planner and autotuner cache for the batch engine.
 //
-// The heuristic picks the round width from the batch shape: short rows use
-// K = 4 or 8 bars per lane (a 128/256-bar round covers a whole row with few
-// idle lanes), long rows K = 16 (fewer halo re-reads and scan steps per bar).
+// The heuristic picks the round width from the batch shape: rows of at most
+// 128 bars use K = 4 bars per lane, others K = 8 (two blocks per SM), and the
+// look-back engine for few long rows K = 16.
 // Candle jobs run on their own bar-parallel kernel unless the series-parallel
 // engine is forced (it evaluates them in the same pass).
 // Measured plans (ct_b200_autotune) override it; they are keyed by a coarse
@@ -74,15 +74,19 @@ SchedulePlan plan_for(const Launch& L, long long total_bars, long long max_len) 
   }
   SchedulePlan p;
   const long long mean = L.S > 0 ? total_bars / L.S : 0;
-  if (max_len <= 128) p.k = 4;
-  else if (mean <= 512) p.k = 8;
-  else p.k = 16;
+  // K = 8 runs two blocks per SM and beat K = 16 on long ragged rows too
+  p.k = max_len <= 128 ? 4 : 8;
+  (void)mean;
   p.warps_per_block = 8;
   // A warp per series splitting each round across its lanes; when there are
   // too few series to fill the GPU and they span many rounds, rounds of one
-  // series go to different warps chained by decoupled look-back.
+  // series go to different warps chained by decoupled look-back (512-bar
+  // rounds: fewer tiles and hops).
   p.mode = 0;
-  if (L.S < 1024 && max_len >= 8ll * 32 * p.k) p.mode = 2;
+  if (L.S < 1024 && max_len >= 8ll * 32 * 16) {
+    p.mode = 2;
+    p.k = 16;
+  }
   if (const char* e = std::getenv("TACUDA_B200_MODE")) {
     if (std::strcmp(e, "sp") == 0) p.mode = 1;
     if (std::strcmp(e, "ws") == 0) p.mode = 0;

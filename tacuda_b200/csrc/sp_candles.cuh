@@ -27,6 +27,15 @@ enum CdlSet {
 __device__ __constant__ const int kSetSlot[11] = {0, 0, 0, 1, -1, -1, 2, 1, 3, 3, 3};
 __device__ __constant__ const float kSetFactor[11] = {1.0f, 3.0f, 1.0f, 0.1f, 1.0f, 2.0f, 1.0f, 0.1f, 0.2f, 0.6f, 0.05f};
 __device__ __constant__ const int kSlotPeriod[4] = {10, 10, 10, 5};
+// The same tables as constant expressions: the pattern functions pass literal
+// settings, so these fold at compile time.
+__host__ __device__ constexpr int set_slot(int s) {
+  return s <= 2 ? 0 : s == 3 ? 1 : s <= 5 ? -1 : s == 6 ? 2 : s == 7 ? 1 : 3;
+}
+__host__ __device__ constexpr float set_factor(int s) {
+  return s == 0 ? 1.0f : s == 1 ? 3.0f : s == 2 ? 1.0f : s == 3 ? 0.1f : s == 4 ? 1.0f : s == 5 ? 2.0f
+       : s == 6 ? 1.0f : s == 7 ? 0.1f : s == 8 ? 0.2f : s == 9 ? 0.6f : 0.05f;
+}
 
 constexpr int kCdlBack = 5;  // anchors r-5 .. r (HIKKAKEMOD reads NEAR at r-5)
 
@@ -69,8 +78,8 @@ struct Bars {
   __device__ __forceinline__ bool RGAP_DN(int a, int b) const { return H(a) < L(b); }
   // TA-Lib candle average of setting s anchored at bar r-d
   __device__ __forceinline__ double AVG(int s, int d) const {
-    const int slot = kSetSlot[s];
-    const double factor = (double)kSetFactor[s];
+    const int slot = set_slot(s);
+    const double factor = (double)set_factor(s);
     const double div = slot == 2 ? 2.0 : 1.0;
     const long long a = t - d;
     if (slot < 0) return factor * RB(d) / div;
