@@ -361,3 +361,24 @@ def test_precision_variants_on_level_offset_rows(prec, engine):
                 assert np.all(err <= bound), f"{prec} {engine} {name}[{i}]: worst excess {np.max(err - bound)}"
     finally:
         del os.environ["TACUDA_B200_MODE"]
+
+
+@pytest.mark.parametrize("S,T", [(4000, 234), (37, 50), (9, 3001)])
+def test_host_entry_matches_device_entry(S, T):
+    """ct_b200_fused_batch (host buffers; large batches pipelined in row
+    chunks over auxiliary streams) gives the device entry point's bits."""
+    d = synthetic.ohlcv(S, T, seed=31)
+    dp = device_planes(d)
+    douts = {n: torch.full((S, T), 777.0, device="cuda") for n in workloads.PASS13_OUTPUTS}
+    jobs = [tb.make_job(fam, p, fp, [douts[o].data_ptr() for o in on]) for _, fam, p, fp, on in workloads.PASS13]
+    tb.fused_batch_d(tb.make_series({k: v.data_ptr() for k, v in dp.items() if k in tb.PLANE_ID}, S, T), jobs, 0)
+    torch.cuda.synchronize()
+    hp = {k: torch.from_numpy(v).pin_memory() for k, v in d.items()}
+    houts = {n: torch.full((S, T), 555.0).pin_memory() for n in workloads.PASS13_OUTPUTS}
+    hjobs = [tb.make_job(fam, p, fp, [houts[o].data_ptr() for o in on]) for _, fam, p, fp, on in workloads.PASS13]
+    s = torch.cuda.Stream()
+    tb.fused_batch(tb.make_series({k: v.data_ptr() for k, v in hp.items() if k in tb.PLANE_ID}, S, T), hjobs,
+                   s.cuda_stream)
+    for n in workloads.PASS13_OUTPUTS:
+        np.testing.assert_array_equal(houts[n].numpy().view(np.uint32), douts[n].cpu().numpy().view(np.uint32),
+                                      err_msg=n)
