@@ -115,6 +115,21 @@ def committed_traffic():
     return None
 
 
+def max_over_ranks(values, device):
+    """Element-wise max of per-rank timings over the process group (the job's
+    time is its slowest rank's)."""
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def whole_job_value(work_per_rank, world, ms):
+    """Whole-job throughput: every rank processes its own batch (weak scaling),
+    so the job does world x the per-rank work in the slowest rank's time."""
+    return work_per_rank * world / (ms * 1e-3)
+
+
 def run_ours(args, rank, world, local):
     import torch
     import tacuda_b200 as tb
@@ -216,9 +231,7 @@ def run_ours(args, rank, world, local):
 
     stats = {"ms": ms, "plain_ms": plain_ms, "e2e_ms": e2e_ms, "times": times}
     if world > 1:
-        t = torch.tensor([ms, plain_ms, e2e_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        stats["ms"], stats["plain_ms"], stats["e2e_ms"] = (float(x) for x in t.tolist())
+        stats["ms"], stats["plain_ms"], stats["e2e_ms"] = max_over_ranks([ms, plain_ms, e2e_ms], dev)
     del g
     return stats, clocks.summary(), h2d, d2h, launches0
 
@@ -405,7 +418,7 @@ def main():
         from tacuda_b200 import workloads
         peak, peak_kind = measured_peak()
         ms = stats["ms"]
-        value = work_per_step * world / (ms * 1e-3)
+        value = whole_job_value(work_per_step, world, ms)
         algo_bytes = workloads.PASS13_FUSED_BYTES_PER_BAR * args.series * args.length
         achieved = algo_bytes / (ms * 1e-3) / 1e9
         traffic = committed_traffic()
