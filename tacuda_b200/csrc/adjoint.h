@@ -26,7 +26,6 @@ struct AlphaLaunch {
   const float *w_ema, *w_macd, *w_sig, *w_hist, *w_rsi;
   float* dx;            // dL/dclose, S*T
   float* dalpha;        // dL/dalpha, S
-  double* scratch;      // set by alpha_backward
 };
 
 cudaError_t alpha_forward(const AlphaLaunch& L, cudaStream_t stream);

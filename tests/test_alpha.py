@@ -78,7 +78,7 @@ def test_entry_points_validate_arguments():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("shape", [(1, 30), (16, 700), (5, 2048)])
+@pytest.mark.parametrize("shape", [(1, 30), (16, 700), (5, 2048), (3, 10000)])
 def test_forward_matches_reference(shape):
     from tacuda_b200 import torch_api as TA
     close, alpha, _ = _data(*shape, seed=11)
@@ -99,7 +99,7 @@ def test_forward_at_talib_coefficients_matches_talib_oracle():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("shape", [(3, 40), (8, 600), (4, 2048)])
+@pytest.mark.parametrize("shape", [(3, 40), (8, 600), (4, 2048), (2, 10000), (37, 300)])
 def test_adjoint_matches_unrolled_autograd(shape):
     from tacuda_b200 import torch_api as TA
     close, alpha, w = _data(*shape, seed=17)
