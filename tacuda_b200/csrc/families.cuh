@@ -596,8 +596,9 @@ __device__ __forceinline__ void adx_round(const Ctx<K>& c, const Job& j, Carry& 
       tr = a * tr + r;
       pd = a * pd + pl;
       md = a * md + mi;
-      const double dip = tr > 0.0 ? 100.0 * pd / tr : 0.0;
-      const double dim = tr > 0.0 ? 100.0 * md / tr : 0.0;
+      const double rtr = tr > 0.0 ? 100.0 / tr : 0.0;
+      const double dip = pd * rtr;
+      const double dim = md * rtr;
       const double tot = dip + dim;
       dx = tot > 0.0 ? 100.0 * fabs(dip - dim) / tot : 0.0;
     }
@@ -751,6 +752,9 @@ __device__ __forceinline__ void sum_window_round(const Ctx<K>& c, const Job& j, 
     }
   }
   const double divider = (double)p * (p + 1) / 2.0;
+  // constant divisors as reciprocals: one FP64 multiply per bar instead of a
+  // division (within an ulp of FP64, far below the float outputs' rounding)
+  const double inv_p = 1.0 / (double)p, inv_div = 1.0 / divider;
   for (int k = 0; k < K; ++k) {
     const int t = g0 + k;
     if (!c.valid(t)) break;
@@ -764,9 +768,9 @@ __device__ __forceinline__ void sum_window_round(const Ctx<K>& c, const Job& j, 
         else { s += (double)vin; if (mode == 2) w += (double)vin * (double)p; }
       }
       if (nn == 0) {
-        if (mode == 0) o = (float)(s / (double)p);
+        if (mode == 0) o = (float)(s * inv_p);
         else if (mode == 1) o = (float)s;
-        else o = p == 1 ? c.x(pl, t) : (float)(w / divider);
+        else o = p == 1 ? c.x(pl, t) : (float)(w * inv_div);
       }
     }
     c.put(0, k, o);
@@ -819,7 +823,7 @@ __device__ __forceinline__ void moment_window_round(const Ctx<K>& c, const Job& 
           const double sd = var != 0.0 ? sqrt(var) : 0.0;
           if (mode == 1) o0 = (float)(up != 1.0 ? sd * up : sd);
           else {
-            const double mid = raw / (double)p;
+            const double mid = raw * inv;
             if (up == dn) { const double dv = sd * up; o0 = (float)(mid + dv); o2 = (float)(mid - dv); }
             else { o0 = (float)fma(sd, up, mid); o2 = (float)(mid - sd * dn); }
             o1 = (float)mid;
@@ -846,6 +850,7 @@ __device__ __forceinline__ void linreg_round(const Ctx<K>& c, const Job& j) {
   const double sumX = (double)p * (p - 1) * 0.5;
   const double sumXSqr = (double)p * (p - 1) * (2 * p - 1) / 6.0;
   const double divisor = sumX * sumX - p * sumXSqr;
+  const double inv_divisor = 1.0 / divisor, inv_p = 1.0 / (double)p;
   double sy = 0.0, sxy = 0.0, o = 0.0;
   int nn = 0;
   if (tf < g0 + K && c.valid(tf)) {
@@ -871,8 +876,8 @@ __device__ __forceinline__ void linreg_round(const Ctx<K>& c, const Job& j) {
         nn += (isnan(vin) ? 1 : 0) - (isnan(vout) ? 1 : 0);
       }
       if (nn == 0) {
-        const double m = (p * sxy - sumX * sy) / divisor;
-        const double b = (sy - m * sumX) / (double)p;
+        const double m = (p * sxy - sumX * sy) * inv_divisor;
+        const double b = (sy - m * sumX) * inv_p;
         out = (float)(o + fma(m, (double)(p - 1), b));
       }
     }
@@ -1004,6 +1009,7 @@ template <int K>
 __device__ __forceinline__ void cci_round(const Ctx<K>& c, const Job& j) {
   const int p = j.ip[0];
   const int g0 = c.gb0();
+  const double inv_p = 1.0 / (double)p;
   for (int k = 0; k < K; ++k) {
     const int t = g0 + k;
     if (!c.valid(t)) break;
@@ -1011,10 +1017,10 @@ __device__ __forceinline__ void cci_round(const Ctx<K>& c, const Job& j) {
     if (t >= p - 1) {
       double sum = 0.0;
       for (int i = 0; i < p; ++i) sum += c.typ(t - i);
-      const double sma = sum / p;
+      const double sma = sum * inv_p;
       double dev = 0.0;
       for (int i = 0; i < p; ++i) dev += fabs(c.typ(t - i) - sma);
-      const double md = dev / p;
+      const double md = dev * inv_p;
       const double num = c.typ(t) - sma;
       o = (num != 0.0 && md != 0.0) ? (float)(num / (0.015 * md)) : 0.0f;
     }
@@ -1107,7 +1113,7 @@ __device__ __forceinline__ void correl_round(const Ctx<K>& c, const Job& j, Carr
       sx += dx; sy += dy; sxx += dx * dx; syy += dy * dy; sxy += dx * dy;
     }
   }
-  const double pp = (double)p;
+  const double inv_pp = 1.0 / (double)p;
   for (int k = 0; k < K; ++k) {
     const int t = g0 + k;
     if (!c.valid(t)) break;
@@ -1121,10 +1127,10 @@ __device__ __forceinline__ void correl_round(const Ctx<K>& c, const Job& j, Carr
       }
       if (bad >= 0 && t >= bad) o = 0.0f;
       else {
-        const double cov = sxy - sx * sy / pp;
-        const double vx = sxx - sx * sx / pp, vy = syy - sy * sy / pp;
+        const double cov = sxy - sx * sy * inv_pp;
+        const double vx = sxx - sx * sx * inv_pp, vy = syy - sy * sy * inv_pp;
         const double prod = vx * vy;
-        o = (vx > 0.0 && vy > 0.0 && prod > 1e-14) ? (float)(cov / sqrt(prod)) : 0.0f;
+        o = (vx > 0.0 && vy > 0.0 && prod > 1e-14) ? (float)(cov * rsqrt(prod)) : 0.0f;
       }
     }
     c.put(0, k, o);

@@ -20,12 +20,17 @@ namespace tb {
 
 struct __align__(16) LbDesc {
   int flag;   // 0 nothing, 1 aggregate, 2 inclusive
-  int f;      // first-index carries: local (aggregate) / inclusive value, -1 = none
-  int gflag;  // last tile of a group of 32: 1 once GA/GB hold the group's aggregate
-  int pad1;
+  int f;      // first-index carries: inclusive value (-1 = none yet)
+  int gflag;  // last tile of a group of 32: 1 once its group aggregate is set
+  int floc;   // first-index carries: this tile's own value (-1 = none)
+  int gf;     // first-index carries: the group's earliest value (-1 = none)
+  int pad;
   double A[3], B[3], Y[3];
   double GA[3], GB[3];
 };
+
+constexpr int kLbGroup = 32;
+constexpr int kLbSpan = 1024;  // 32 groups
 
 constexpr int kLbAgg = 1, kLbInc = 2;
 constexpr long long kLbSpinLimit = 1ll << 26;  // polls / 32 at up to 1 us each: about two seconds
@@ -92,45 +97,115 @@ __device__ __forceinline__ int lb_wait(const LbDesc* d, int want, int* err) {
   return v;
 }
 
-// First-index carry: the earliest bar with a property (first non-NaN input,
-// first non-finite pair). local = this tile's earliest such bar or -1.
-// Lane 0 performs the protocol; the result is broadcast.
-__device__ __forceinline__ int lb_first_index(LbDesc* base, long long stride, int tile, int local, int* err, int lane) {
-  int res = -1;
-  if (lane == 0) {
-    LbDesc* me = base + (long long)tile * stride;
-    if (tile == 0) {
-      res = local;
+// The predecessors a tile combines, latest first: the tiles of its own group
+// before it, then whole groups, then the tiles of the first partial group,
+// then the anchor `stop`, whose inclusive value closes the range.
+struct LbItems {
+  int tile, stop, nTail, nGroups, nHead, headEnd, grpEnd;
+  __device__ __forceinline__ LbItems(int tile_, int stop_) : tile(tile_), stop(stop_) {
+    const int first = stop + 1;
+    const int tg0 = (tile / kLbGroup) * kLbGroup;
+    if (first >= tg0) {
+      nTail = tile - first;
+      nGroups = nHead = headEnd = grpEnd = 0;
     } else {
-      me->f = local;
-      lb_store_flag(me, kLbAgg);
-      int best = -1;
-      int j = tile - 1;
-      // common case first: tile 0 (published at once) already holds the index
-      if (lb_wait(base, kLbInc, err) == kLbInc) {
-        const int f0 = *reinterpret_cast<const volatile int*>(&base->f);
-        if (f0 >= 0) {
-          best = f0;
-          j = -1;
-        }
-      }
-      for (; j >= 0; --j) {
-        const LbDesc* d = base + (long long)j * stride;
-        const int fl = lb_wait(d, kLbAgg, err);
-        if (fl == 0) break;
-        const int fv = *reinterpret_cast<const volatile int*>(&d->f);
-        if (fl == kLbInc) {
-          if (fv >= 0) best = fv;
-          break;
-        }
-        if (fv >= 0) best = fv;
-      }
-      res = best >= 0 ? best : local;
+      nTail = tile - tg0;
+      const int gFull = (first + kLbGroup - 1) / kLbGroup;  // first whole group
+      grpEnd = tg0 / kLbGroup;                               // groups gFull .. grpEnd-1
+      nGroups = grpEnd - gFull;
+      headEnd = gFull * kLbGroup;                            // head tiles first .. headEnd-1
+      nHead = headEnd - first;
     }
+  }
+  __device__ __forceinline__ int count() const { return nTail + nGroups + nHead; }
+  // item r < count(): kind 0 = tile aggregate of tile idx, 1 = group aggregate
+  // held by tile idx (the group's last); r == count(): kind 2 = anchor
+  __device__ __forceinline__ void item(int r, int& idx, int& kind) const {
+    if (r == count()) { idx = stop; kind = 2; }
+    else if (r < nTail) { idx = tile - 1 - r; kind = 0; }
+    else if (r >= nTail + nGroups) { idx = headEnd - 1 - (r - nTail - nGroups); kind = 0; }
+    else { idx = (grpEnd - 1 - (r - nTail)) * kLbGroup + kLbGroup - 1; kind = 1; }
+  }
+};
+
+// First-index carry: the earliest bar with a property (first non-NaN input,
+// first non-finite pair) up to this tile; local = this tile's earliest such
+// bar or -1. Bar indices grow with the tile, so the earliest is the least
+// non-negative value. The tile combines its own value, its predecessors'
+// values and group minima back to the latest kLbSpan checkpoint, and that
+// checkpoint's inclusive value, like lb_resolve; the last tile of each group
+// publishes the group's minimum.
+__device__ __forceinline__ int lb_first_index(LbDesc* base, long long stride, int tile, int local, int* err, int lane) {
+  LbDesc* me = base + (long long)tile * stride;
+  if (tile == 0) {
+    if (lane == 0) {
+      me->floc = local;
+      me->f = local;
+      lb_store_flag(me, kLbInc);
+    }
+    return local;
+  }
+  if (lane == 0) {
+    me->floc = local;
+    lb_store_flag(me, kLbAgg);
+  }
+  auto earliest = [](int v) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v = min(v, __shfl_xor_sync(kFull, v, d));
+    return v;
+  };
+  const int kNone = 0x7fffffff;
+  const int g = tile / kLbGroup;
+  if (tile % kLbGroup == kLbGroup - 1 && g > 0) {
+    const LbDesc* d = base + (long long)(tile - lane) * stride;
+    const bool ok = lb_wait_all(&d->flag, kLbAgg, lane != 0, err);
+    int v = lane == 0 ? local : (ok ? *reinterpret_cast<const volatile int*>(&d->floc) : -1);
+    v = earliest(v >= 0 ? v : kNone);
+    if (lane == 0) {
+      me->gf = v == kNone ? -1 : v;
+      __threadfence();
+      *reinterpret_cast<volatile int*>(&me->gflag) = 1;
+    }
+  }
+  // common case first: tile 0 (resolved at once) already holds the index
+  {
+    const bool ok0 = lb_wait_all(&base->flag, kLbInc, lane == 0, err);
+    int f0 = -1;
+    if (lane == 0 && ok0) f0 = *reinterpret_cast<const volatile int*>(&base->f);
+    f0 = __shfl_sync(kFull, f0, 0);
+    if (f0 >= 0) {
+      if (lane == 0) {
+        me->f = f0;
+        lb_store_flag(me, kLbInc);
+      }
+      return f0;
+    }
+  }
+  const LbItems it(tile, ((tile - 1) / kLbSpan) * kLbSpan);
+  int best = local >= 0 ? local : kNone;
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int r = 3 * lane + k;
+    const bool active = r <= it.count();
+    int idx = 0, kind = 0;
+    if (active) it.item(r, idx, kind);
+    const LbDesc* d = base + (long long)idx * stride;
+    const int* flag = kind == 1 ? &d->gflag : &d->flag;
+    const int want = kind == 1 ? 1 : (kind == 2 ? kLbInc : kLbAgg);
+    ok = lb_wait_all(flag, want, active && ok, err) && ok;
+    if (active && ok) {
+      const int v = *reinterpret_cast<const volatile int*>(kind == 0 ? &d->floc : (kind == 1 ? &d->gf : &d->f));
+      if (v >= 0 && v < best) best = v;
+    }
+  }
+  best = earliest(best);
+  const int res = best == kNone ? -1 : best;
+  if (lane == 0) {
     me->f = res;
     lb_store_flag(me, kLbInc);
   }
-  return __shfl_sync(kFull, res, 0);
+  return res;
 }
 
 // Resolve the incoming state of an NC-channel stage, deterministically.
@@ -147,9 +222,6 @@ __device__ __forceinline__ int lb_first_index(LbDesc* base, long long stride, in
 // to three consecutive items and the warp folds the lanes in a fixed tree, so
 // the result does not depend on timing. Only the checkpoints chain inclusive
 // states, one hop per kLbSpan tiles.
-constexpr int kLbGroup = 32;
-constexpr int kLbSpan = 1024;  // 32 groups
-
 template <int NC>
 __device__ __forceinline__ void lb_compose(double (&a)[NC], double (&b)[NC], const double* A, const double* B) {
   // (a, b) := (a, b) o (A, B): the new map is applied first
@@ -222,25 +294,8 @@ __device__ __forceinline__ void lb_resolve(LbDesc* base, long long stride, int t
   const int ckpt = ((tile - 1) / kLbSpan) * kLbSpan;
   int stop = first_steady - 1 > ckpt ? first_steady - 1 : ckpt;
   if (stop > tile - 1) stop = tile - 1;
-  // items after the anchor, latest first: tail tiles of this tile's group,
-  // whole groups, head tiles of the first partial group, then the anchor
-  const int first = stop + 1;                   // first tile after the anchor
-  const int tg0 = (tile / kLbGroup) * kLbGroup;  // first tile of this group
-  int nTail, nGroups, nHead, headEnd, grpEnd;
-  if (first >= tg0) {
-    nTail = tile - first;
-    nGroups = 0;
-    nHead = 0;
-    headEnd = grpEnd = 0;
-  } else {
-    nTail = tile - tg0;
-    const int gFull = (first + kLbGroup - 1) / kLbGroup;  // first whole group
-    grpEnd = tg0 / kLbGroup;                               // groups gFull .. grpEnd-1
-    nGroups = grpEnd - gFull;
-    headEnd = gFull * kLbGroup;                            // head tiles first .. headEnd-1
-    nHead = headEnd - first;
-  }
-  const int nItems = nTail + nGroups + nHead;
+  const LbItems it(tile, stop);
+  const int nItems = it.count();
 #pragma unroll
   for (int ch = 0; ch < NC; ++ch) { a[ch] = 1.0; b[ch] = 0.0; }
   bool ok = true;
@@ -249,28 +304,11 @@ __device__ __forceinline__ void lb_resolve(LbDesc* base, long long stride, int t
     const int r = 3 * lane + k;
     const bool active = r <= nItems;
     // the item's descriptor, the flag to wait for and the map's fields
-    const LbDesc* d = base;
-    const int* flag = &base->flag;
-    int want = kLbAgg;
-    int kind = 0;  // 0 tile aggregate, 1 group aggregate, 2 anchor
-    if (active) {
-      if (r == nItems) {
-        d = base + (long long)stop * stride;
-        flag = &d->flag;
-        want = kLbInc;
-        kind = 2;
-      } else if (r < nTail || r >= nTail + nGroups) {
-        const int j = r < nTail ? tile - 1 - r : headEnd - 1 - (r - nTail - nGroups);
-        d = base + (long long)j * stride;
-        flag = &d->flag;
-      } else {
-        const int gi = grpEnd - 1 - (r - nTail);
-        d = base + ((long long)gi * kLbGroup + kLbGroup - 1) * stride;
-        flag = &d->gflag;
-        want = 1;
-        kind = 1;
-      }
-    }
+    int idx = 0, kind = 0;  // kind: 0 tile aggregate, 1 group aggregate, 2 anchor
+    if (active) it.item(r, idx, kind);
+    const LbDesc* d = base + (long long)idx * stride;
+    const int* flag = kind == 1 ? &d->gflag : &d->flag;
+    const int want = kind == 1 ? 1 : (kind == 2 ? kLbInc : kLbAgg);
     ok = lb_wait_all(flag, want, active && ok, err) && ok;
     if (active && ok) {
       double A[NC], B[NC];
