@@ -886,6 +886,42 @@ __device__ __forceinline__ void linreg_round(const Ctx<K>& c, const Job& j) {
   c.flush(0, (float*)j.out[0]);
 }
 
+// Extremes of the lane's K windows [t-p+1, t], t = g0 .. g0+K-1, for p-1 >= K
+// (van Herk / Gil-Werman): a suffix sweep over the p-1 bars before g0 keeps
+// the extreme of [g0-p+1+k, g0-1] for each k, a prefix sweep over the lane's
+// bars the extreme of [g0, g0+k]; out[k] combines the two. About 2 + p/K
+// comparisons per bar instead of p. Returns whether a NaN was met: callers
+// whose NaN rule depends on the comparison order then use the direct window.
+template <int K, bool kMax>
+__device__ __forceinline__ bool lane_window_ext(const Ctx<K>& c, int pl, int p, float (&out)[K]) {
+  auto op = [](float run, float v) { return kMax ? (v > run ? v : run) : (v < run ? v : run); };
+  const int g0 = c.gb0();
+  bool nan = false;
+  float run = kMax ? -INFINITY : INFINITY;
+  for (int i = g0 - 1; i > g0 - p + K; --i) {
+    const float v = c.x(pl, i);
+    nan |= isnan(v);
+    run = op(run, v);
+  }
+  float suf[K];
+#pragma unroll
+  for (int k = K - 1; k >= 0; --k) {
+    const float v = c.x(pl, g0 - p + 1 + k);
+    nan |= isnan(v);
+    run = op(run, v);
+    suf[k] = run;
+  }
+  float pre = kMax ? -INFINITY : INFINITY;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const float v = c.x(pl, g0 + k);
+    nan |= isnan(v);
+    pre = op(pre, v);
+    out[k] = op(suf[k], pre);
+  }
+  return __any_sync(kFull, nan) ? true : false;
+}
+
 // Window extrema over [t-p+1, t] of a float plane; fmaxf/fminf ignore NaN.
 template <int K>
 __device__ __forceinline__ float win_max(const Ctx<K>& c, int pl, int t, int p) {
@@ -907,12 +943,16 @@ __device__ __forceinline__ void minmax_round(const Ctx<K>& c, const Job& j, Carr
   const int pl = j.in[0], p = j.ip[0];
   const int f = resolve_start(c, cy, pl, j.lb_slot);
   const int g0 = c.gb0();
+  float ext[K];
+  const bool fast = p - 1 >= K && !(is_max ? lane_window_ext<K, true>(c, pl, p, ext)
+                                           : lane_window_ext<K, false>(c, pl, p, ext));
+#pragma unroll
   for (int k = 0; k < K; ++k) {
     const int t = g0 + k;
     if (!c.valid(t)) break;
     float o = qnan();
     if (t >= p - 1) {
-      o = is_max ? win_max(c, pl, t, p) : win_min(c, pl, t, p);
+      o = fast ? ext[k] : (is_max ? win_max(c, pl, t, p) : win_min(c, pl, t, p));
       if (f < 0 || t - p + 1 < f) o = qnan();
     }
     c.put(0, k, o);
@@ -928,16 +968,28 @@ template <int K>
 __device__ __forceinline__ void willr_round(const Ctx<K>& c, const Job& j) {
   const int ph = j.in[0], plo = j.in[1], pc = j.in[2], p = j.ip[0];
   const int g0 = c.gb0();
+  float his[K], los[K];
+  bool fast = p - 1 >= K;
+  if (fast) {
+    const bool n1 = lane_window_ext<K, true>(c, ph, p, his);
+    const bool n2 = lane_window_ext<K, false>(c, plo, p, los);
+    fast = !n1 && !n2;
+  }
+#pragma unroll
   for (int k = 0; k < K; ++k) {
     const int t = g0 + k;
     if (!c.valid(t)) break;
     float o = qnan();
     if (t >= p - 1) {
-      float hi = c.x(ph, t), lo = c.x(plo, t);
-      for (int i = 1; i < p; ++i) {
-        const float h = c.x(ph, t - i), l = c.x(plo, t - i);
-        if (h > hi) hi = h;
-        if (l < lo) lo = l;
+      float hi = his[k], lo = los[k];
+      if (!fast) {
+        hi = c.x(ph, t);
+        lo = c.x(plo, t);
+        for (int i = 1; i < p; ++i) {
+          const float h = c.x(ph, t - i), l = c.x(plo, t - i);
+          if (h > hi) hi = h;
+          if (l < lo) lo = l;
+        }
       }
       const double den = (double)hi - (double)lo;
       const double v = den == 0.0 ? 0.0 : (((double)hi - (double)c.x(pc, t)) / den) * -100.0;
@@ -970,10 +1022,26 @@ __device__ __forceinline__ void stoch_round(const Ctx<K>& c, const Job& j) {
     return fabs(range) <= 1e-14 * (fabs(hi) + fabs(lo)) ? 0.0 : ((double)c.x(pc, t) - lo) / range * 100.0;
   };
   const int g0 = c.gb0();
+  float his[K], los[K];
+  bool fast = p - 1 >= K;
+  if (fast) {
+    const bool n1 = lane_window_ext<K, true>(c, ph, p, his);
+    const bool n2 = lane_window_ext<K, false>(c, plo, p, los);
+    fast = !n1 && !n2;
+  }
+#pragma unroll
   for (int k = 0; k < K; ++k) {
     const int t = g0 + k;
     if (!c.valid(t)) break;
-    c.line(0, k) = fastk(t);
+    double v;
+    if (!fast || t < p - 1) {
+      v = fastk(t);
+    } else {
+      const double lo = los[k], hi = his[k];
+      const double range = hi - lo;
+      v = fabs(range) <= 1e-14 * (fabs(hi) + fabs(lo)) ? 0.0 : ((double)c.x(pc, t) - lo) / range * 100.0;
+    }
+    c.line(0, k) = v;
   }
   for (int i = c.lane; i < ext; i += 32) c.eline(0, i - ext) = fastk(c.t0 - ext + i);
   __syncwarp();
