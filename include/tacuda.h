@@ -248,6 +248,45 @@ CTAPI_EXPORT ctStatus_t ct_macd_batch(const float *host_inputs, float *host_macd
 CTAPI_EXPORT ctStatus_t ct_bbands_batch(const float *host_inputs, float *host_uppers, float *host_middles, float *host_lowers, int seriesLen, int numSeries, int period, float upperMul, float lowerMul, int maxConcurrency, cudaStream_t stream); /* tacuda.h:877 */
 CTAPI_EXPORT ctStatus_t ct_stochastic_batch(const float *host_highs, const float *host_lows, const float *host_closes, float *host_ks, float *host_ds, int seriesLen, int numSeries, int kPeriod, int dPeriod, int maxConcurrency, cudaStream_t stream); /* tacuda.h:885 */
 
+/* ---- batch streams (include/tacuda_stream.h:155-269): one handle advances
+ * numSeries series of one indicator by n bars per append; the appends' outputs
+ * equal one batch call over the concatenated bars. Host matrices, series-major
+ * (series s's n bars at [s*n, s*n+n)). Every append runs on the GPU. ---- */
+typedef struct ctStreamBatch ctStreamBatch_t;
+typedef enum ctStreamExec {
+  CT_STREAM_EXEC_AUTO = 0,
+  CT_STREAM_EXEC_CPU = 1,
+  CT_STREAM_EXEC_GPU = 2,
+} ctStreamExec_t;                                                                       /* tacuda_stream.h:180 */
+CTAPI_EXPORT ctStatus_t ct_stream_batch_destroy(ctStreamBatch_t *batch);                 /* tacuda_stream.h:186 */
+CTAPI_EXPORT ctStatus_t ct_stream_batch_reset(ctStreamBatch_t *batch);                   /* tacuda_stream.h:187 */
+CTAPI_EXPORT ctStatus_t ct_stream_batch_lookback(const ctStreamBatch_t *batch, int *outLookback); /* tacuda_stream.h:188 */
+CTAPI_EXPORT ctStatus_t ct_stream_batch_series(const ctStreamBatch_t *batch, int *outSeries);     /* tacuda_stream.h:190 */
+CTAPI_EXPORT ctStatus_t ct_stream_batch_outputs(const ctStreamBatch_t *batch, int *outCount);     /* tacuda_stream.h:192 */
+CTAPI_EXPORT ctStatus_t ct_stream_batch_bars(const ctStreamBatch_t *batch, long long *outBars);    /* tacuda_stream.h:194 */
+/* CT_STREAM_EXEC_CPU returns CT_STATUS_UNSUPPORTED: appends always run on the GPU. */
+CTAPI_EXPORT ctStatus_t ct_stream_batch_set_exec(ctStreamBatch_t *batch, ctStreamExec_t exec);    /* tacuda_stream.h:196 */
+CTAPI_EXPORT ctStatus_t ct_sma_stream_batch_create(int period, int numSeries, ctStreamBatch_t **outBatch);  /* tacuda_stream.h:199 */
+CTAPI_EXPORT ctStatus_t ct_ema_stream_batch_create(int period, int numSeries, ctStreamBatch_t **outBatch);  /* tacuda_stream.h:201 */
+CTAPI_EXPORT ctStatus_t ct_wma_stream_batch_create(int period, int numSeries, ctStreamBatch_t **outBatch);  /* tacuda_stream.h:203 */
+CTAPI_EXPORT ctStatus_t ct_rsi_stream_batch_create(int period, int numSeries, ctStreamBatch_t **outBatch);  /* tacuda_stream.h:205 */
+CTAPI_EXPORT ctStatus_t ct_atr_stream_batch_create(int period, int numSeries, ctStreamBatch_t **outBatch);  /* tacuda_stream.h:207 */
+CTAPI_EXPORT ctStatus_t ct_natr_stream_batch_create(int period, int numSeries, ctStreamBatch_t **outBatch); /* tacuda_stream.h:209 */
+CTAPI_EXPORT ctStatus_t ct_obv_stream_batch_create(int numSeries, ctStreamBatch_t **outBatch);              /* tacuda_stream.h:211 */
+CTAPI_EXPORT ctStatus_t ct_ad_stream_batch_create(int numSeries, ctStreamBatch_t **outBatch);               /* tacuda_stream.h:213 */
+CTAPI_EXPORT ctStatus_t ct_macd_stream_batch_create(int fastPeriod, int slowPeriod, int signalPeriod, int numSeries, ctStreamBatch_t **outBatch); /* tacuda_stream.h:215 */
+CTAPI_EXPORT ctStatus_t ct_bbands_stream_batch_create(int period, float upperMul, float lowerMul, int numSeries, ctStreamBatch_t **outBatch);    /* tacuda_stream.h:218 */
+CTAPI_EXPORT ctStatus_t ct_sma_stream_batch_append(ctStreamBatch_t *batch, const float *closes, int n, float *outs);  /* tacuda_stream.h:222 */
+CTAPI_EXPORT ctStatus_t ct_ema_stream_batch_append(ctStreamBatch_t *batch, const float *closes, int n, float *outs);  /* tacuda_stream.h:225 */
+CTAPI_EXPORT ctStatus_t ct_wma_stream_batch_append(ctStreamBatch_t *batch, const float *closes, int n, float *outs);  /* tacuda_stream.h:228 */
+CTAPI_EXPORT ctStatus_t ct_rsi_stream_batch_append(ctStreamBatch_t *batch, const float *closes, int n, float *outs);  /* tacuda_stream.h:231 */
+CTAPI_EXPORT ctStatus_t ct_atr_stream_batch_append(ctStreamBatch_t *batch, const float *highs, const float *lows, const float *closes, int n, float *outs);  /* tacuda_stream.h:234 */
+CTAPI_EXPORT ctStatus_t ct_natr_stream_batch_append(ctStreamBatch_t *batch, const float *highs, const float *lows, const float *closes, int n, float *outs); /* tacuda_stream.h:239 */
+CTAPI_EXPORT ctStatus_t ct_obv_stream_batch_append(ctStreamBatch_t *batch, const float *closes, const float *volumes, int n, float *outs);                   /* tacuda_stream.h:244 */
+CTAPI_EXPORT ctStatus_t ct_ad_stream_batch_append(ctStreamBatch_t *batch, const float *highs, const float *lows, const float *closes, const float *volumes, int n, float *outs); /* tacuda_stream.h:248 */
+CTAPI_EXPORT ctStatus_t ct_macd_stream_batch_append(ctStreamBatch_t *batch, const float *closes, int n, float *outMacd, float *outSignal, float *outHist);  /* tacuda_stream.h:254 */
+CTAPI_EXPORT ctStatus_t ct_bbands_stream_batch_append(ctStreamBatch_t *batch, const float *closes, int n, float *outUpper, float *outMiddle, float *outLower); /* tacuda_stream.h:259 */
+
 /* ========================================================================
  * ct_b200_*: new surface with no counterpart in the reference.
  * ======================================================================== */

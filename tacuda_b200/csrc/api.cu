@@ -12,6 +12,7 @@
 #include "scheduler.h"
 
 #include <algorithm>
+#include <functional>
 #include <atomic>
 #include <cstdio>
 #include <cstdlib>
@@ -837,6 +838,347 @@ ctStatus_t ct_b200_fused_batch(const ctB200Series* hs, const ctB200Job* hjobs, i
   const cudaError_t e = cudaStreamSynchronize(stream);
   if (e != cudaSuccess) return cuda_fail(CT_STATUS_DEVICE_ERROR, who, e);
   return CT_STATUS_SUCCESS;
+}
+
+// ------------------------------------------------------------ stream batches
+//
+// include/tacuda_stream.h:155-269 in the reference: one handle advances the
+// state of numSeries series of one indicator by n bars per append, so that a
+// run of appends gives the outputs of one batch call over the concatenated
+// bars. Here every append runs the warp-scan engine on the GPU from the state
+// the previous append left: the per-series recurrence carries (kept in device
+// memory) and the last `hist` bars of every input row (the windows' halo),
+// kept at the front of a double-buffered device staging matrix whose rows
+// hold [hist bars | up to cap new bars].
+
+struct ctStreamBatch {
+  int family;
+  Job job;            // validated job (outputs set per append)
+  int S;
+  long long seen;     // bars appended so far (per series)
+  int hist, cap;      // history bars kept, new bars a staging row holds
+  int nin, in_plane[4];
+  int lookback, nout;
+  float* stage[2];    // nin planes x S rows x (hist + cap)
+  int cur;
+  void* carry;        // S x Carry
+  int dev;
+  bool gpu_only;
+};
+
+namespace {
+std::mutex g_stream_mutex;
+std::vector<ctStreamBatch*> g_streams;  // live handles
+
+bool stream_live(const ctStreamBatch* b) {
+  std::lock_guard<std::mutex> lk(g_stream_mutex);
+  for (auto* p : g_streams)
+    if (p == b) return true;
+  return false;
+}
+
+int stream_lookback(const Job& j) {
+  switch (j.family) {
+    case tb::F_SMA: case tb::F_EMA: case tb::F_WMA: case tb::F_BBANDS: return j.ip[0] - 1;
+    case tb::F_RSI: case tb::F_ATR: case tb::F_NATR: return j.ip[0];
+    case tb::F_MACD: return j.ip[1] + j.ip[2] - 2;
+    default: return 0;  // OBV, AD
+  }
+}
+
+ctStatus_t stream_create(const ctB200Job& u, int numSeries, ctStreamBatch** out, const char* who) {
+  clear_error();
+  if (!out) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": null out parameter");
+  *out = nullptr;
+  if (numSeries <= 0) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": numSeries must be > 0");
+  auto* b = new (std::nothrow) ctStreamBatch();
+  if (!b) return fail(CT_STATUS_ALLOC_FAILED, std::string(who) + ": allocation failed");
+  // the job is validated now; its output pointers are placeholders that every
+  // append replaces before launching
+  ctB200Job v = u;
+  for (int k = 0; k < 3; ++k) v.outputs[k] = reinterpret_cast<void*>(static_cast<uintptr_t>(256));
+  ctStatus_t st = make_job(v, b->job, who);
+  if (st != CT_STATUS_SUCCESS) { delete b; return st; }
+  b->family = u.family;
+  b->S = numSeries;
+  b->seen = 0;
+  b->nin = default_inputs(u.family, b->in_plane);
+  b->nout = output_count(u.family);
+  b->lookback = stream_lookback(b->job);
+  Launch L;
+  std::memset(&L, 0, sizeof(L));
+  L.njobs = 1;
+  L.jobs[0] = b->job;
+  b->hist = ((tb::max_lookback_halo(L) + 31) / 32) * 32;
+  b->cap = 0;
+  b->stage[0] = b->stage[1] = nullptr;
+  b->cur = 0;
+  b->gpu_only = true;
+  if (cudaGetDevice(&b->dev) != cudaSuccess || cudaMalloc(&b->carry, sizeof(tb::Carry) * (size_t)numSeries) != cudaSuccess) {
+    delete b;
+    return fail(CT_STATUS_ALLOC_FAILED, std::string(who) + ": device allocation failed");
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_stream_mutex);
+    g_streams.push_back(b);
+  }
+  *out = b;
+  return CT_STATUS_SUCCESS;
+}
+
+// Grow the staging rows to hold n new bars, keeping the history rows.
+ctStatus_t stream_reserve(ctStreamBatch* b, int n, const char* who) {
+  if (n <= b->cap) return CT_STATUS_SUCCESS;
+  const int cap = std::max(n, 2 * b->cap);
+  const size_t row = (size_t)b->hist + cap;
+  const size_t bytes = row * (size_t)b->S * b->nin * sizeof(float);
+  float* fresh[2] = {nullptr, nullptr};
+  for (int i = 0; i < 2; ++i)
+    if (cudaMalloc(&fresh[i], bytes) != cudaSuccess) {
+      if (fresh[0]) cudaFree(fresh[0]);
+      return fail(CT_STATUS_ALLOC_FAILED, std::string(who) + ": device allocation failed");
+    }
+  if (b->stage[b->cur] && b->hist > 0) {
+    const size_t old_row = (size_t)b->hist + b->cap;
+    if (cudaMemcpy2D(fresh[0], row * sizeof(float), b->stage[b->cur], old_row * sizeof(float),
+                     (size_t)b->hist * sizeof(float), (size_t)b->S * b->nin, cudaMemcpyDeviceToDevice) != cudaSuccess) {
+      cudaFree(fresh[0]);
+      cudaFree(fresh[1]);
+      return fail(CT_STATUS_COPY_FAILED, std::string(who) + ": history copy failed");
+    }
+  }
+  for (int i = 0; i < 2; ++i)
+    if (b->stage[i]) cudaFree(b->stage[i]);
+  b->stage[0] = fresh[0];
+  b->stage[1] = fresh[1];
+  b->cur = 0;
+  b->cap = cap;
+  return CT_STATUS_SUCCESS;
+}
+
+ctStatus_t stream_append(ctStreamBatch* b, int family, const float* const* ins, int n, float* const* outs,
+                         const char* who) {
+  clear_error();
+  if (!stream_live(b)) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": invalid or destroyed batch handle");
+  if (b->family != family)
+    return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": batch was created for a different indicator");
+  if (n <= 0) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": n must be > 0");
+  for (int i = 0; i < b->nin; ++i)
+    if (!ins[i]) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": null input pointer");
+  for (int k = 0; k < b->nout; ++k)
+    if (!outs[k]) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": null output pointer");
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev != b->dev)
+    return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": batch belongs to another device");
+  ctStatus_t st = stream_reserve(b, n, who);
+  if (st != CT_STATUS_SUCCESS) return st;
+  const cudaStream_t stream = 0;
+  const size_t row = (size_t)b->hist + b->cap;
+  const size_t plane_stride = row * b->S;
+  float* cur = b->stage[b->cur];
+  float* nxt = b->stage[b->cur ^ 1];
+  // new bars after each row's history
+  for (int i = 0; i < b->nin; ++i)
+    if (cudaMemcpy2DAsync(cur + i * plane_stride + b->hist, row * sizeof(float), ins[i], (size_t)n * sizeof(float),
+                          (size_t)n * sizeof(float), b->S, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+      return fail(CT_STATUS_COPY_FAILED, std::string(who) + ": host to device copy failed");
+  float* dout = nullptr;
+  const size_t out_elems = (size_t)n * b->S;
+  if (tb::scratch_alloc(reinterpret_cast<void**>(&dout), out_elems * b->nout * sizeof(float), stream) != cudaSuccess)
+    return fail(CT_STATUS_ALLOC_FAILED, std::string(who) + ": device allocation failed");
+  Launch L;
+  std::memset(&L, 0, sizeof(L));
+  for (int i = 0; i < b->nin; ++i) L.plane[b->in_plane[i]] = cur + i * plane_stride;
+  L.T = n;
+  L.S = b->S;
+  L.njobs = 1;
+  L.jobs[0] = b->job;
+  for (int k = 0; k < b->nout; ++k) L.jobs[0].out[k] = dout + k * out_elems;
+  L.st_carry = b->carry;
+  L.st_seen = b->seen;
+  L.st_hist = b->hist;
+  L.st_row = (long long)row;
+  tb::SchedulePlan plan = tb::plan_for(L, (long long)n * b->S, n);
+  plan.mode = 0;  // rows continue from their kept carries: warp-per-series engine
+  const cudaError_t e = tb::launch_batch(L, plan, (long long)n * b->S, stream, nullptr);
+  if (e != cudaSuccess) {
+    tb::scratch_free(dout, stream);
+    return cuda_fail(CT_STATUS_KERNEL_FAILED, who, e);
+  }
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  for (int k = 0; k < b->nout; ++k)
+    if (cudaMemcpyAsync(outs[k], dout + k * out_elems, out_elems * sizeof(float), cudaMemcpyDeviceToHost, stream) !=
+        cudaSuccess) {
+      tb::scratch_free(dout, stream);
+      return fail(CT_STATUS_COPY_FAILED, std::string(who) + ": device to host copy failed");
+    }
+  // the last `hist` bars of every row become the next append's history
+  if (b->hist > 0 &&
+      cudaMemcpy2DAsync(nxt, row * sizeof(float), cur + n, row * sizeof(float), (size_t)b->hist * sizeof(float),
+                        (size_t)b->S * b->nin, cudaMemcpyDeviceToDevice, stream) != cudaSuccess) {
+    tb::scratch_free(dout, stream);
+    return fail(CT_STATUS_COPY_FAILED, std::string(who) + ": history copy failed");
+  }
+  tb::scratch_free(dout, stream);
+  const cudaError_t es = cudaStreamSynchronize(stream);
+  if (es != cudaSuccess) return cuda_fail(CT_STATUS_DEVICE_ERROR, who, es);
+  b->cur ^= 1;
+  b->seen += n;
+  return CT_STATUS_SUCCESS;
+}
+
+ctStatus_t stream_query(const ctStreamBatch* b, const char* who, const std::function<ctStatus_t()>& f) {
+  clear_error();
+  if (!stream_live(b)) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": invalid or destroyed batch handle");
+  return f();
+}
+}  // namespace
+
+ctStatus_t ct_stream_batch_destroy(ctStreamBatch_t* batch) {
+  clear_error();
+  if (!batch) return CT_STATUS_SUCCESS;
+  {
+    std::lock_guard<std::mutex> lk(g_stream_mutex);
+    auto it = std::find(g_streams.begin(), g_streams.end(), batch);
+    if (it == g_streams.end())
+      return fail(CT_STATUS_INVALID_ARGUMENT, "ct_stream_batch_destroy: invalid or destroyed batch handle");
+    g_streams.erase(it);
+  }
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(batch->dev);
+  for (auto* p : batch->stage)
+    if (p) cudaFree(p);
+  cudaFree(batch->carry);
+  cudaSetDevice(cur);
+  delete batch;
+  return CT_STATUS_SUCCESS;
+}
+
+ctStatus_t ct_stream_batch_reset(ctStreamBatch_t* batch) {
+  return stream_query(batch, "ct_stream_batch_reset", [&] {
+    batch->seen = 0;  // the next append starts every series from the empty state
+    return CT_STATUS_SUCCESS;
+  });
+}
+
+ctStatus_t ct_stream_batch_lookback(const ctStreamBatch_t* batch, int* outLookback) {
+  return stream_query(batch, "ct_stream_batch_lookback", [&] {
+    if (!outLookback) return fail(CT_STATUS_INVALID_ARGUMENT, "ct_stream_batch_lookback: null out parameter");
+    *outLookback = batch->lookback;
+    return CT_STATUS_SUCCESS;
+  });
+}
+
+ctStatus_t ct_stream_batch_series(const ctStreamBatch_t* batch, int* outSeries) {
+  return stream_query(batch, "ct_stream_batch_series", [&] {
+    if (!outSeries) return fail(CT_STATUS_INVALID_ARGUMENT, "ct_stream_batch_series: null out parameter");
+    *outSeries = batch->S;
+    return CT_STATUS_SUCCESS;
+  });
+}
+
+ctStatus_t ct_stream_batch_outputs(const ctStreamBatch_t* batch, int* outCount) {
+  return stream_query(batch, "ct_stream_batch_outputs", [&] {
+    if (!outCount) return fail(CT_STATUS_INVALID_ARGUMENT, "ct_stream_batch_outputs: null out parameter");
+    *outCount = batch->nout;
+    return CT_STATUS_SUCCESS;
+  });
+}
+
+ctStatus_t ct_stream_batch_bars(const ctStreamBatch_t* batch, long long* outBars) {
+  return stream_query(batch, "ct_stream_batch_bars", [&] {
+    if (!outBars) return fail(CT_STATUS_INVALID_ARGUMENT, "ct_stream_batch_bars: null out parameter");
+    *outBars = batch->seen;
+    return CT_STATUS_SUCCESS;
+  });
+}
+
+ctStatus_t ct_stream_batch_set_exec(ctStreamBatch_t* batch, ctStreamExec_t exec) {
+  return stream_query(batch, "ct_stream_batch_set_exec", [&] {
+    if (exec == CT_STREAM_EXEC_AUTO || exec == CT_STREAM_EXEC_GPU) return CT_STATUS_SUCCESS;
+    if (exec == CT_STREAM_EXEC_CPU)
+      return fail(CT_STATUS_UNSUPPORTED, "ct_stream_batch_set_exec: this library runs every append on the GPU");
+    return fail(CT_STATUS_INVALID_ARGUMENT, "ct_stream_batch_set_exec: unknown execution policy");
+  });
+}
+
+#define TB_STREAM_PERIOD_CREATE(name, fam)                                                   \
+  ctStatus_t ct_##name##_stream_batch_create(int period, int numSeries, ctStreamBatch_t** out) { \
+    return stream_create(job_of(fam, period), numSeries, out, "ct_" #name "_stream_batch_create"); \
+  }
+TB_STREAM_PERIOD_CREATE(sma, tb::F_SMA)
+TB_STREAM_PERIOD_CREATE(ema, tb::F_EMA)
+TB_STREAM_PERIOD_CREATE(wma, tb::F_WMA)
+TB_STREAM_PERIOD_CREATE(rsi, tb::F_RSI)
+TB_STREAM_PERIOD_CREATE(atr, tb::F_ATR)
+TB_STREAM_PERIOD_CREATE(natr, tb::F_NATR)
+#undef TB_STREAM_PERIOD_CREATE
+
+ctStatus_t ct_obv_stream_batch_create(int numSeries, ctStreamBatch_t** out) {
+  return stream_create(job_of(tb::F_OBV), numSeries, out, "ct_obv_stream_batch_create");
+}
+ctStatus_t ct_ad_stream_batch_create(int numSeries, ctStreamBatch_t** out) {
+  return stream_create(job_of(tb::F_AD), numSeries, out, "ct_ad_stream_batch_create");
+}
+ctStatus_t ct_macd_stream_batch_create(int fastPeriod, int slowPeriod, int signalPeriod, int numSeries,
+                                       ctStreamBatch_t** out) {
+  return stream_create(job_of(tb::F_MACD, fastPeriod, slowPeriod, signalPeriod), numSeries, out,
+                       "ct_macd_stream_batch_create");
+}
+ctStatus_t ct_bbands_stream_batch_create(int period, float upperMul, float lowerMul, int numSeries,
+                                         ctStreamBatch_t** out) {
+  return stream_create(job_of(tb::F_BBANDS, period, 0, 0, upperMul, lowerMul), numSeries, out,
+                       "ct_bbands_stream_batch_create");
+}
+
+#define TB_STREAM_CLOSE_APPEND(name, fam)                                                          \
+  ctStatus_t ct_##name##_stream_batch_append(ctStreamBatch_t* batch, const float* closes, int n, float* outs) { \
+    const float* in[1] = {closes};                                                                 \
+    float* o[1] = {outs};                                                                          \
+    return stream_append(batch, fam, in, n, o, "ct_" #name "_stream_batch_append");               \
+  }
+TB_STREAM_CLOSE_APPEND(sma, tb::F_SMA)
+TB_STREAM_CLOSE_APPEND(ema, tb::F_EMA)
+TB_STREAM_CLOSE_APPEND(wma, tb::F_WMA)
+TB_STREAM_CLOSE_APPEND(rsi, tb::F_RSI)
+#undef TB_STREAM_CLOSE_APPEND
+
+ctStatus_t ct_atr_stream_batch_append(ctStreamBatch_t* batch, const float* highs, const float* lows,
+                                      const float* closes, int n, float* outs) {
+  const float* in[3] = {highs, lows, closes};
+  float* o[1] = {outs};
+  return stream_append(batch, tb::F_ATR, in, n, o, "ct_atr_stream_batch_append");
+}
+ctStatus_t ct_natr_stream_batch_append(ctStreamBatch_t* batch, const float* highs, const float* lows,
+                                       const float* closes, int n, float* outs) {
+  const float* in[3] = {highs, lows, closes};
+  float* o[1] = {outs};
+  return stream_append(batch, tb::F_NATR, in, n, o, "ct_natr_stream_batch_append");
+}
+ctStatus_t ct_obv_stream_batch_append(ctStreamBatch_t* batch, const float* closes, const float* volumes, int n,
+                                      float* outs) {
+  const float* in[2] = {closes, volumes};
+  float* o[1] = {outs};
+  return stream_append(batch, tb::F_OBV, in, n, o, "ct_obv_stream_batch_append");
+}
+ctStatus_t ct_ad_stream_batch_append(ctStreamBatch_t* batch, const float* highs, const float* lows,
+                                     const float* closes, const float* volumes, int n, float* outs) {
+  const float* in[4] = {highs, lows, closes, volumes};
+  float* o[1] = {outs};
+  return stream_append(batch, tb::F_AD, in, n, o, "ct_ad_stream_batch_append");
+}
+ctStatus_t ct_macd_stream_batch_append(ctStreamBatch_t* batch, const float* closes, int n, float* outMacd,
+                                       float* outSignal, float* outHist) {
+  const float* in[1] = {closes};
+  float* o[3] = {outMacd, outSignal, outHist};
+  return stream_append(batch, tb::F_MACD, in, n, o, "ct_macd_stream_batch_append");
+}
+ctStatus_t ct_bbands_stream_batch_append(ctStreamBatch_t* batch, const float* closes, int n, float* outUpper,
+                                         float* outMiddle, float* outLower) {
+  const float* in[1] = {closes};
+  float* o[3] = {outUpper, outMiddle, outLower};
+  return stream_append(batch, tb::F_BBANDS, in, n, o, "ct_bbands_stream_batch_append");
 }
 
 // ------------------------------------------------------------ plans

@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(256, (K <= 8 ? 2 : 1)) batch_kernel(const __gr
       float* dst = planes + lay.plane_slot[p] * lay.plane_len;
       for (int i = lane; i < span; i += 32) {
         const int t = tlo + i;
-        const bool ok = t >= 0 && t < c.n;
+        const bool ok = t >= c.lo && t < c.n;
         cp_async4(dst + pad(i), ok ? src + t : src, ok);
       }
     }
@@ -160,6 +160,7 @@ __global__ void __launch_bounds__(256, (K <= 8 ? 2 : 1)) batch_kernel(const __gr
     }
     __syncwarp();
   };
+  c.lo = 0;
   if (L.lb) {
     // Look-back mode: tiles of one round taken in order from a global counter;
     // the carries between tiles come from the descriptors, not shared memory.
@@ -195,6 +196,7 @@ __global__ void __launch_bounds__(256, (K <= 8 ? 2 : 1)) batch_kernel(const __gr
         c.base = s * L.T;
         c.n = (int)L.T;
       }
+      c.obase = c.base;
       c.tile = (int)((long long)g - first);
       c.lbd = L.lb_desc + first * L.lb_nslots;
       stage_round_inputs(c.tile * TILE);
@@ -214,23 +216,37 @@ __global__ void __launch_bounds__(256, (K <= 8 ? 2 : 1)) batch_kernel(const __gr
     const long long idx = (long long)pass * W + ((pass & 1) ? (W - 1 - gw) : gw);
     if (idx >= L.S) break;
     const int s = L.order ? L.order[idx] : (int)idx;
-    if (L.offsets) {
+    int t_start = 0;
+    Carry* keep = nullptr;  // streaming: carries kept between appends
+    if (L.st_carry) {
+      t_start = (int)L.st_seen;
+      c.base = (long long)s * L.st_row + L.st_hist - L.st_seen;
+      c.obase = (long long)s * L.T - L.st_seen;
+      c.n = (int)(L.st_seen + L.T);
+      c.lo = (int)(L.st_seen > L.st_hist ? L.st_seen - L.st_hist : 0);
+      keep = static_cast<Carry*>(L.st_carry) + (long long)s * L.njobs;
+    } else if (L.offsets) {
       c.base = L.offsets[s];
       c.n = (int)(L.offsets[s + 1] - c.base);
+      c.obase = c.base;
     } else {
       c.base = (long long)s * L.T;
       c.n = (int)L.T;
+      c.obase = c.base;
     }
-    for (int t0 = 0; t0 < c.n; t0 += TILE) {
+    for (int t0 = t_start; t0 < c.n; t0 += TILE) {
       stage_round_inputs(t0);
-      const bool first = t0 == 0, last = t0 + TILE >= c.n;
+      const bool first = t0 == t_start, last = t0 + TILE >= c.n;
       for (int j = 0; j < L.njobs; ++j) {
-        // a row's first round starts from the empty carry, its last keeps none
+        // a row's first round starts from the empty carry (or the one kept by
+        // the previous append), its last keeps none (or hands it to the next)
         Carry cy;
-        if (first) {
+        if (first && (!keep || t_start == 0)) {
           cy.f = -1;
 #pragma unroll
           for (int v = 0; v < 10; ++v) cy.v[v] = 0.0;
+        } else if (first) {
+          cy = keep[j];
         } else {
           cy = carry[j];
         }
@@ -238,6 +254,10 @@ __global__ void __launch_bounds__(256, (K <= 8 ? 2 : 1)) batch_kernel(const __gr
         if (!last) {
           __syncwarp();
           if (lane == 0) carry[j] = cy;
+          __syncwarp();
+        } else if (keep) {
+          __syncwarp();
+          if (lane == 0) keep[j] = cy;
           __syncwarp();
         }
       }

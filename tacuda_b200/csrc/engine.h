@@ -61,6 +61,13 @@ struct Launch {
   long long* lb_tile_start;  // ragged: first tile of each series (S+1), else nullptr
   LbDesc* lb_desc;           // lb_tiles * lb_nslots descriptors (zeroed)
   int lb_nslots;
+  // streaming append: rows continue earlier appends. Bar t of row s (t counted
+  // from the row's first bar ever) is at plane[s*st_row + st_hist - st_seen + t]
+  // for t >= st_seen - st_hist; the T new bars start at st_seen; outputs go to
+  // out[s*T + t - st_seen]; carries persist in st_carry (S x njobs). Null
+  // st_carry: an ordinary batch.
+  void* st_carry;
+  long long st_seen, st_hist, st_row;
   Job jobs[kMaxJobs];
 };
 

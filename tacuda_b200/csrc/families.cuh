@@ -35,6 +35,8 @@ struct Ctx {
   int L;           // bars in the round
   int H;           // staged halo
   long long base;  // row offset in the planes (64-bit); bar indices within a row are int
+  long long obase; // row offset in the outputs (= base except for streaming appends)
+  int lo;          // first bar of the row held in the planes (0 except for appends)
   // This warp's shared memory, addressed from the kernel's extern __shared__
   // base so every access below compiles to a shared-space load or store.
   unsigned char* sm;
@@ -72,7 +74,7 @@ struct Ctx {
   // Coalesced copy of staged output j to out[base + t0 .. + L).
   __device__ __forceinline__ void flush(int j, float* out) const {
     __syncwarp();
-    float* dst = out + base + t0;
+    float* dst = out + obase + t0;
     const float* src = stage(j);
     for (int i = lane; i < L; i += 32) dst[i] = src[pad(i)];
     __syncwarp();
