@@ -327,6 +327,39 @@ def run_extras(dev, peak):
         "forward_GBs": n4 * 24 / (fwd * 1e-3) / 1e9, "adjoint_GBs": n4 * 28 / (bwd * 1e-3) / 1e9}
     del c4, a4, w4, ck
 
+    # batch streams: 4096 series, EMA14 and MACD12/26/9 handles, 64 bars per append
+    # (host buffers in and out, synchronous, as the reference's append)
+    import ctypes as ct
+    lib = tb.get_lib()
+    Ss, n = 4096, 64
+    dd = synthetic.ohlcv(Ss, 16 * n, seed=9)["close"]
+    outs_e = np.empty((Ss, n), np.float32)
+    outs_m = [np.empty((Ss, n), np.float32) for _ in range(3)]
+    he, hm = ct.c_void_p(), ct.c_void_p()
+    lib.ct_ema_stream_batch_create(14, Ss, ct.byref(he))
+    lib.ct_macd_stream_batch_create(12, 26, 9, Ss, ct.byref(hm))
+    chunks = [np.ascontiguousarray(dd[:, i * n:(i + 1) * n]) for i in range(16)]
+    P = ct.c_void_p
+    for i in range(2):
+        lib.ct_ema_stream_batch_append(he, chunks[i].ctypes.data_as(P), n, outs_e.ctypes.data_as(P))
+    t0 = time.perf_counter()
+    for i in range(2, 16):
+        lib.ct_ema_stream_batch_append(he, chunks[i].ctypes.data_as(P), n, outs_e.ctypes.data_as(P))
+    ema_ms = (time.perf_counter() - t0) * 1e3 / 14
+    for i in range(2):
+        lib.ct_macd_stream_batch_append(hm, chunks[i].ctypes.data_as(P), n, *(o.ctypes.data_as(P) for o in outs_m))
+    t0 = time.perf_counter()
+    for i in range(2, 16):
+        lib.ct_macd_stream_batch_append(hm, chunks[i].ctypes.data_as(P), n, *(o.ctypes.data_as(P) for o in outs_m))
+    macd_ms = (time.perf_counter() - t0) * 1e3 / 14
+    lib.ct_stream_batch_destroy(he)
+    lib.ct_stream_batch_destroy(hm)
+    out["stream_append_4096x64"] = {
+        "workload": "batch streams of 4096 series, 64 bars per append, host buffers, synchronous (host wall clock "
+                    "per append, copies included)",
+        "ema14_ms_per_append": ema_ms, "macd_ms_per_append": macd_ms,
+        "ema14_bars_per_s": Ss * n / (ema_ms * 1e-3), "macd_bars_per_s": Ss * n / (macd_ms * 1e-3)}
+
     # config 5: 4 series x 50,000,000 bars with a +1e4 level, look-back across tiles
     T5 = 50_000_000
     x5 = torch.from_numpy(synthetic.level_walk(4, T5, seed=5)).to(dev)
