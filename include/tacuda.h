@@ -79,6 +79,11 @@ CTAPI_EXPORT ctStatus_t ct_mfi_batch_d(const float *d_highs, const float *d_lows
 CTAPI_EXPORT ctStatus_t ct_ad_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, const float *d_volumes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1468 */
 CTAPI_EXPORT ctStatus_t ct_adosc_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, const float *d_volumes, float *d_outputs, int seriesLen, int numSeries, int fastPeriod, int slowPeriod, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1483 */
 CTAPI_EXPORT ctStatus_t ct_correl_batch_d(const float *d_xs, const float *d_ys, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1826 */
+CTAPI_EXPORT ctStatus_t ct_roc_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1007 */
+CTAPI_EXPORT ctStatus_t ct_rma_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:4110 */
+CTAPI_EXPORT ctStatus_t ct_typprice_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1300 */
+CTAPI_EXPORT ctStatus_t ct_medprice_batch_d(const float *d_highs, const float *d_lows, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1339 */
+CTAPI_EXPORT ctStatus_t ct_midprice_batch_d(const float *d_highs, const float *d_lows, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1727 */
 
 /* candlestick patterns: float signal (+-100/+-80/+-200), warm-up 0 */
 CTAPI_EXPORT ctStatus_t ct_cdl_doji_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1877 */
@@ -174,6 +179,11 @@ CTAPI_EXPORT ctStatus_t ct_max_d(const float* d_input, float* d_output, int size
 CTAPI_EXPORT ctStatus_t ct_min_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:331 */
 CTAPI_EXPORT ctStatus_t ct_linearreg_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:357 */
 CTAPI_EXPORT ctStatus_t ct_correl_d(const float* d_x, const float* d_y, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:540 */
+CTAPI_EXPORT ctStatus_t ct_roc_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:174 */
+CTAPI_EXPORT ctStatus_t ct_medprice_d(const float* d_high, const float* d_low, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:342 */
+CTAPI_EXPORT ctStatus_t ct_typprice_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:345 */
+CTAPI_EXPORT ctStatus_t ct_midprice_d(const float* d_high, const float* d_low, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:511 */
+CTAPI_EXPORT ctStatus_t ct_rma_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:1212 */
 CTAPI_EXPORT ctStatus_t ct_cdl_doji_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:555 */
 CTAPI_EXPORT ctStatus_t ct_cdl_hammer_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:559 */
 CTAPI_EXPORT ctStatus_t ct_cdl_inverted_hammer_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:565 */
@@ -297,7 +307,8 @@ typedef enum ctB200Family {
   CT_B200_NATR, CT_B200_TRANGE, CT_B200_ADX, CT_B200_DX, CT_B200_BBANDS, CT_B200_STOCH,
   CT_B200_CCI, CT_B200_OBV, CT_B200_AD, CT_B200_ADOSC, CT_B200_MFI, CT_B200_WILLR,
   CT_B200_SUM, CT_B200_MIN, CT_B200_MAX, CT_B200_STDDEV, CT_B200_VAR, CT_B200_LINEARREG,
-  CT_B200_CORREL, CT_B200_DEMA, CT_B200_TEMA, CT_B200_T3, CT_B200_CDL
+  CT_B200_CORREL, CT_B200_DEMA, CT_B200_TEMA, CT_B200_T3, CT_B200_CDL,
+  CT_B200_ROC, CT_B200_RMA, CT_B200_MEDPRICE, CT_B200_TYPPRICE, CT_B200_MIDPRICE
 } ctB200Family_t;
 
 /* Input planes of a batch. */

@@ -50,6 +50,11 @@ FAMILIES = {
     "dema": (25, ("close",), ("out",), ("period",), ()),
     "tema": (26, ("close",), ("out",), ("period",), ()),
     "t3": (27, ("close",), ("out",), ("period",), ("vfactor",)),
+    "roc": (28, ("close",), ("out",), ("period",), ()),
+    "rma": (29, ("close",), ("out",), ("period",), ()),
+    "medprice": (30, ("high", "low"), ("out",), (), ()),
+    "typprice": (31, ("high", "low", "close"), ("out",), (), ()),
+    "midprice": (32, ("high", "low"), ("out",), ("period",), ()),
 }
 
 _P = ct.c_void_p
@@ -149,21 +154,24 @@ def _load_ref():
         lib.ref_hlc.argtypes = [ct.c_int, _P, _P, _P, ct.c_int, ct.c_int, ct.c_int, ct.c_int, _P, _P, ct.c_int]
         lib.ref_states.argtypes = [ct.c_int, _P, _P, _P, _P, ct.c_int, ct.c_int, ct.c_int, ct.c_int, _P, ct.c_int]
         lib.ref_cdl.argtypes = [ct.c_int, _P, _P, _P, _P, ct.c_int, ct.c_int, _P, ct.c_int]
+        lib.ref_price.argtypes = [ct.c_int, _P, _P, _P, ct.c_int, ct.c_int, ct.c_int, _P, ct.c_int]
         _ref = lib
     return _ref
 
 
 _REF_SINGLE = {"sma": 0, "ema": 1, "wma": 2, "rsi": 3, "stddev": 4, "var": 5,
-               "linearreg": 6, "dema": 7, "tema": 8, "t3": 9}
+               "linearreg": 6, "dema": 7, "tema": 8, "t3": 9, "roc": 10, "rma": 11}
 _REF_STATES = {"obv": 0, "ad": 1, "mfi": 2, "adosc": 3, "natr": 4}
-REF_FAMILIES = tuple(_REF_SINGLE) + ("macd", "bbands", "atr", "trange", "stoch") + tuple(_REF_STATES)
+_REF_PRICE = {"medprice": 0, "typprice": 1, "midprice": 2}
+REF_FAMILIES = (tuple(_REF_SINGLE) + ("macd", "bbands", "atr", "trange", "stoch") + tuple(_REF_STATES)
+                + tuple(_REF_PRICE))
 
 
 def ref_run(name: str, data: dict, threads: int = 0, **params):
     """Run the reference's own CPU code for ``name`` (see REF_FAMILIES)."""
     lib = _load_ref()
     c = _f4(data["close"]) if "close" in data else None
-    shape = c.shape
+    shape = (c if c is not None else _f4(data["high"])).shape
     S, T = shape
     if name in _REF_SINGLE:
         out = np.empty(shape, np.float64)
@@ -184,6 +192,12 @@ def ref_run(name: str, data: dict, threads: int = 0, **params):
                             float(params["dn"]), *(o.ctypes.data for o in outs), threads)
         return tuple(outs) if rc == 0 else None
     h, l = _f4(data.get("high", c)), _f4(data.get("low", c))
+    if name in _REF_PRICE:
+        out = np.empty(shape, np.float64)
+        rc = lib.ref_price(_REF_PRICE[name], h.ctypes.data, l.ctypes.data,
+                           c.ctypes.data if c is not None else None, S, T,
+                           int(params.get("period", 0)), out.ctypes.data, threads)
+        return (out,) if rc == 0 else None
     if name in ("atr", "trange", "stoch"):
         fam = {"atr": 0, "trange": 1, "stoch": 2}[name]
         o0, o1 = np.empty(shape, np.float64), np.empty(shape, np.float64)

@@ -8,7 +8,7 @@
 //     TA-Lib 0.8.3 C (commit 62021c1d, third_party/ta_lib_0_8_3/PROVENANCE.json)
 //     in FP64: TA_SMA, TA_EMA, TA_WMA, TA_RSI, TA_MACD, TA_ATR, TA_BBANDS,
 //     TA_STOCH, TA_STDDEV, TA_VAR, TA_LINEARREG, TA_DEMA, TA_TEMA, TA_T3,
-//     TA_TRANGE.
+//     TA_TRANGE, TA_ROC, TA_RMA, TA_MEDPRICE, TA_TYPPRICE, TA_MIDPRICE.
 //   * include/utils/StreamStates.h: ObvState, AdState, precise::MfiState,
 //     precise::AdoscState, precise::NatrState (the fused batch arithmetic).
 //   * include/utils/CandleUtils.h: the cdl_*_talib pattern decisions.
@@ -70,7 +70,8 @@ extern "C" {
 int ref_threads(void) { return omp_get_max_threads(); }
 
 // One-input, one-output TA-Lib families: 0 SMA, 1 EMA, 2 WMA, 3 RSI,
-// 4 STDDEV(nbdev=1), 5 VAR(nbdev=1), 6 LINEARREG, 7 DEMA, 8 TEMA, 9 T3(v=fparam).
+// 4 STDDEV(nbdev=1), 5 VAR(nbdev=1), 6 LINEARREG, 7 DEMA, 8 TEMA, 9 T3(v=fparam),
+// 10 ROC, 11 RMA.
 int ref_single(int fam, const float* x, int S, int T, int p, double fparam,
                double* out, int threads) {
   int rc_all = 0;
@@ -93,6 +94,8 @@ int ref_single(int fam, const float* x, int S, int T, int p, double fparam,
       case 7: rc = TA_DEMA(a, 0, T - 1, in, p, &beg, &nb, o); break;
       case 8: rc = TA_TEMA(a, 0, T - 1, in, p, &beg, &nb, o); break;
       case 9: rc = TA_T3(a, 0, T - 1, in, p, fparam, &beg, &nb, o); break;
+      case 10: rc = TA_ROC(a, 0, T - 1, in, p, &beg, &nb, o); break;
+      case 11: rc = TA_RMA(a, 0, T - 1, in, p, &beg, &nb, o); break;
       default: rc = TA_BAD_PARAM;
     }
     if (rc != TA_SUCCESS) { rc_all = static_cast<int>(rc); nb = 0; }
@@ -162,6 +165,31 @@ int ref_hlc(int fam, const float* h, const float* l, const float* c, int S, int 
     if (rc != TA_SUCCESS) { rc_all = static_cast<int>(rc); nb = 0; }
     scatter(out0 + o, r.out[0].data(), T, beg, nb);
     if (fam == 2 && out1) scatter(out1 + o, r.out[1].data(), T, beg, nb);
+  });
+  return rc_all;
+}
+
+// Price transforms: 0 MEDPRICE(h,l), 1 TYPPRICE(h,l,c), 2 MIDPRICE(h,l; p).
+int ref_price(int fam, const float* h, const float* l, const float* c, int S, int T, int p,
+              double* out, int threads) {
+  int rc_all = 0;
+  rows(S, threads, [&](int s) {
+    Row r(T);
+    const size_t o = static_cast<size_t>(s) * T;
+    load(r.buf[0], h + o, T); load(r.buf[1], l + o, T);
+    if (fam == 1) load(r.buf[2], c + o, T);
+    Arena a = r.make_arena();
+    int beg = 0, nb = 0;
+    TA_RetCode rc = TA_SUCCESS;
+    switch (fam) {
+      case 0: rc = TA_MEDPRICE(a, 0, T - 1, r.buf[0].data(), r.buf[1].data(), &beg, &nb, r.out[0].data()); break;
+      case 1: rc = TA_TYPPRICE(a, 0, T - 1, r.buf[0].data(), r.buf[1].data(), r.buf[2].data(), &beg, &nb,
+                               r.out[0].data()); break;
+      case 2: rc = TA_MIDPRICE(a, 0, T - 1, r.buf[0].data(), r.buf[1].data(), p, &beg, &nb, r.out[0].data()); break;
+      default: rc = TA_BAD_PARAM;
+    }
+    if (rc != TA_SUCCESS) { rc_all = static_cast<int>(rc); nb = 0; }
+    scatter(out + o, r.out[0].data(), T, beg, nb);
   });
   return rc_all;
 }

@@ -702,6 +702,59 @@ static void row_dema(RowCtx* r) { cascade_row(r->in[0], r->n, r->ip[0], 2, 0, 0.
 static void row_tema(RowCtx* r) { cascade_row(r->in[0], r->n, r->ip[0], 3, 0, 0.0, r->out[0]); }
 static void row_t3(RowCtx* r) { cascade_row(r->in[0], r->n, r->ip[0], 6, 1, r->fp[0], r->out[0]); }
 
+/* ------------------------------------------------- ROC, RMA, price transforms */
+
+/* src/indicators/ROC.cu:10-21: float ((x - prev) / prev) * 100 from bar p, 0
+ * where prev == 0; the float arithmetic is kept (C float ops, no contraction). */
+static void row_roc(RowCtx* r) {
+  const float* x = r->in[0]; int n = r->n, p = r->ip[0]; double* o = r->out[0];
+  fill_nan(o, n);
+  for (int t = p; t < n; ++t) {
+    const float prev = x[t - p], curr = x[t];
+    const float v = prev != 0.0f ? ((curr - prev) / prev) * 100.0f : 0.0f;
+    o[t] = (double)v;
+  }
+}
+
+/* talib08:13614-13683 TA_RMA (mean of the first p, then fma(wBeta, y,
+ * wAlpha * x)); the reference's TA-Lib runner starts after the row's leading
+ * NaNs (src/compat/Talib08.cu:72-84). No period-1 shortcut: a NaN propagates. */
+static void row_rma(RowCtx* r) {
+  const float* x = r->in[0]; int n = r->n, p = r->ip[0]; double* o = r->out[0];
+  fill_nan(o, n);
+  const int f = leading_nan(x, n);
+  if (n - f < p) return;
+  const double wb = (double)(p - 1) / (double)p, wa = 1.0 - wb;
+  double s = 0.0;
+  for (int t = f; t < f + p; ++t) s += (double)x[t];
+  double prev = s / p;
+  o[f + p - 1] = prev;
+  for (int t = f + p; t < n; ++t) { prev = fma(wb, prev, wa * (double)x[t]); o[t] = prev; }
+}
+
+/* src/indicators/MedPrice.cu:12-14: 0.5f * (h + l) in float. */
+static void row_medprice(RowCtx* r) {
+  for (int t = 0; t < r->n; ++t) r->out[0][t] = (double)(0.5f * (r->in[0][t] + r->in[1][t]));
+}
+
+/* src/indicators/TypPrice.cu:13-15: (h + l + c) / 3.0f in float. */
+static void row_typprice(RowCtx* r) {
+  for (int t = 0; t < r->n; ++t)
+    r->out[0][t] = (double)((r->in[0][t] + r->in[1][t] + r->in[2][t]) / 3.0f);
+}
+
+/* src/indicators/MIDPRICE.cu:11-24: fmaxf / fminf over [t-p+1, t] (NaN
+ * ignored unless the whole window is NaN), 0.5f * (max + min), from bar p-1. */
+static void row_midprice(RowCtx* r) {
+  const float* h = r->in[0]; const float* l = r->in[1]; int n = r->n, p = r->ip[0]; double* o = r->out[0];
+  fill_nan(o, n);
+  for (int t = p - 1; t < n; ++t) {
+    float hi = h[t - p + 1], lo = l[t - p + 1];
+    for (int k = t - p + 2; k <= t; ++k) { hi = fmaxf(hi, h[k]); lo = fminf(lo, l[k]); }
+    o[t] = (double)(0.5f * (hi + lo));
+  }
+}
+
 /* --------------------------------------------------------------- dispatch */
 
 typedef struct { int nin, nout, nip, nfp; void (*fn)(RowCtx*); int minp; } FamSpec;
@@ -724,6 +777,9 @@ static const FamSpec kFam[ORC_FAMILY_COUNT] = {
   [ORC_VAR] = {1, 1, 1, 0, row_var, 1},      [ORC_LINEARREG] = {1, 1, 1, 0, row_linearreg, 2},
   [ORC_CORREL] = {2, 1, 1, 0, row_correl, 1}, [ORC_DEMA] = {1, 1, 1, 0, row_dema, 1},
   [ORC_TEMA] = {1, 1, 1, 0, row_tema, 1},    [ORC_T3] = {1, 1, 1, 1, row_t3, 1},
+  [ORC_ROC] = {1, 1, 1, 0, row_roc, 1},      [ORC_RMA] = {1, 1, 1, 0, row_rma, 1},
+  [ORC_MEDPRICE] = {2, 1, 0, 0, row_medprice, 0}, [ORC_TYPPRICE] = {3, 1, 0, 0, row_typprice, 0},
+  [ORC_MIDPRICE] = {2, 1, 1, 0, row_midprice, 1},
 };
 
 static int check_params(int family, const int* ip) {

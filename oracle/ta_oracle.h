@@ -10,8 +10,14 @@
  * LINEARREG DEMA TEMA T3 are pinned against the vendored TA-Lib compiled from the
  * reference tree (oracle/_ref); OBV AD ADOSC MFI NATR and the candle patterns are
  * pinned against the reference's StreamStates.h / CandleUtils.h compiled on the
- * host. ADX DX CCI WILLR CORREL SUM MIN MAX have no CPU code in the reference:
- * they are pinned by known-answer tests only ("parity partially unpinned").
+ * host. RMA is pinned against the vendored TA_RMA (the reference's device path
+ * runs that same function). ROC MEDPRICE TYPPRICE MIDPRICE restate the
+ * reference's float kernels (src/indicators/ROC.cu, MedPrice.cu, TypPrice.cu,
+ * MIDPRICE.cu) operation for operation; they are pinned against the vendored
+ * TA_ROC / TA_MEDPRICE / TA_TYPPRICE / TA_MIDPRICE within the float tolerance
+ * and by known answers. ADX DX CCI WILLR CORREL SUM MIN MAX have no CPU code in
+ * the reference: they are pinned by known-answer tests only ("parity partially
+ * unpinned").
  */
 #ifndef TA_ORACLE_H
 #define TA_ORACLE_H
@@ -23,7 +29,8 @@ enum OracleFamily {
   ORC_SMA = 0, ORC_EMA, ORC_WMA, ORC_RSI, ORC_MACD, ORC_ATR, ORC_NATR, ORC_TRANGE,
   ORC_ADX, ORC_DX, ORC_BBANDS, ORC_STOCH, ORC_CCI, ORC_OBV, ORC_AD, ORC_ADOSC,
   ORC_MFI, ORC_WILLR, ORC_SUM, ORC_MIN, ORC_MAX, ORC_STDDEV, ORC_VAR, ORC_LINEARREG,
-  ORC_CORREL, ORC_DEMA, ORC_TEMA, ORC_T3, ORC_FAMILY_COUNT
+  ORC_CORREL, ORC_DEMA, ORC_TEMA, ORC_T3, ORC_ROC, ORC_RMA, ORC_MEDPRICE,
+  ORC_TYPPRICE, ORC_MIDPRICE, ORC_FAMILY_COUNT
 };
 
 /* ins: the family's input planes (see oracle/oracle.py INPUTS); outs: its output

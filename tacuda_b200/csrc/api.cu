@@ -45,7 +45,8 @@ ctStatus_t cuda_fail(ctStatus_t st, const char* where, cudaError_t e) {
 // Minimum valid period of each family's first integer parameter.
 int min_period(int family) {
   switch (family) {
-    case tb::F_OBV: case tb::F_AD: case tb::F_TRANGE: case tb::F_CDL: return 0;
+    case tb::F_OBV: case tb::F_AD: case tb::F_TRANGE: case tb::F_CDL: case tb::F_MEDPRICE: case tb::F_TYPPRICE:
+      return 0;
     default: return 1;
   }
 }
@@ -53,8 +54,9 @@ int min_period(int family) {
 int default_inputs(int family, int* in) {
   switch (family) {
     case tb::F_ATR: case tb::F_NATR: case tb::F_TRANGE: case tb::F_ADX: case tb::F_DX:
-    case tb::F_STOCH: case tb::F_WILLR: case tb::F_CCI:
+    case tb::F_STOCH: case tb::F_WILLR: case tb::F_CCI: case tb::F_TYPPRICE:
       in[0] = tb::P_HIGH; in[1] = tb::P_LOW; in[2] = tb::P_CLOSE; return 3;
+    case tb::F_MEDPRICE: case tb::F_MIDPRICE: in[0] = tb::P_HIGH; in[1] = tb::P_LOW; return 2;
     case tb::F_AD: case tb::F_ADOSC: case tb::F_MFI:
       in[0] = tb::P_HIGH; in[1] = tb::P_LOW; in[2] = tb::P_CLOSE; in[3] = tb::P_VOLUME; return 4;
     case tb::F_OBV: in[0] = tb::P_CLOSE; in[1] = tb::P_VOLUME; return 2;
@@ -98,7 +100,7 @@ ctStatus_t make_job(const ctB200Job& u, Job& j, const char* who) {
   switch (f) {
     case tb::F_SMA: case tb::F_SUM: case tb::F_WMA: case tb::F_BBANDS: case tb::F_STDDEV: case tb::F_VAR:
     case tb::F_LINEARREG: case tb::F_MIN: case tb::F_MAX: case tb::F_WILLR: case tb::F_CCI: case tb::F_MFI:
-    case tb::F_CORREL:
+    case tb::F_CORREL: case tb::F_ROC: case tb::F_MIDPRICE:
       if (u.params[0] > kMaxWindow) return fail(CT_STATUS_UNSUPPORTED, std::string(who) + ": window period above 4096");
       break;
     case tb::F_STOCH:
@@ -126,6 +128,13 @@ ctStatus_t make_job(const ctB200Job& u, Job& j, const char* who) {
       break;
     }
     case tb::F_ATR: case tb::F_NATR:
+      j.fp[0] = (double)(u.params[0] - 1) / (double)u.params[0];
+      j.fp[1] = 1.0 - j.fp[0];
+      break;
+    case tb::F_RMA:
+      // talib08:13614-13683 TA_RMA: wBeta, wAlpha; periods above 100000 are
+      // TA-Lib's TA_BAD_PARAM, an invalid argument at the reference's boundary
+      if (u.params[0] > 100000) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": invalid period");
       j.fp[0] = (double)(u.params[0] - 1) / (double)u.params[0];
       j.fp[1] = 1.0 - j.fp[0];
       break;
@@ -335,6 +344,8 @@ TB_S1(sum, tb::F_SUM)
 TB_S1(max, tb::F_MAX)
 TB_S1(min, tb::F_MIN)
 TB_S1(linearreg, tb::F_LINEARREG)
+TB_S1(roc, tb::F_ROC)  // tacuda.h:1007, tacuda_device.h:174
+TB_S1(rma, tb::F_RMA)  // tacuda.h:4110, tacuda_device.h:1212
 #undef TB_S1
 
 #define TB_HLC(NAME, FAM)                                                                                  \
@@ -537,6 +548,56 @@ ctStatus_t ct_correl_d(const float* d_x, const float* d_y, float* d_output, int 
   Planes P = close_only(d_x);
   P.p[tb::P_AUX] = d_y;
   return run_single(P.p, u, size, 1, stream, "ct_correl_d");
+}
+
+// ------------------------------------------------------------ price transforms
+
+ctStatus_t ct_medprice_batch_d(const float* d_highs, const float* d_lows, float* d_outputs, int seriesLen,
+                               int numSeries, int, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_MEDPRICE);
+  u.outputs[0] = d_outputs;
+  Planes P;
+  P.p[tb::P_HIGH] = d_highs; P.p[tb::P_LOW] = d_lows;
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_medprice_batch_d");
+}
+ctStatus_t ct_medprice_d(const float* d_high, const float* d_low, float* d_output, int size, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_MEDPRICE);
+  u.outputs[0] = d_output;
+  Planes P;
+  P.p[tb::P_HIGH] = d_high; P.p[tb::P_LOW] = d_low;
+  return run_single(P.p, u, size, 1, stream, "ct_medprice_d");
+}
+
+ctStatus_t ct_typprice_batch_d(const float* d_highs, const float* d_lows, const float* d_closes, float* d_outputs,
+                               int seriesLen, int numSeries, int, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_TYPPRICE);
+  u.outputs[0] = d_outputs;
+  const Planes P = hlc(d_highs, d_lows, d_closes);
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_typprice_batch_d");
+}
+ctStatus_t ct_typprice_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, int size,
+                         cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_TYPPRICE);
+  u.outputs[0] = d_output;
+  const Planes P = hlc(d_high, d_low, d_close);
+  return run_single(P.p, u, size, 1, stream, "ct_typprice_d");
+}
+
+ctStatus_t ct_midprice_batch_d(const float* d_highs, const float* d_lows, float* d_outputs, int seriesLen,
+                               int numSeries, int period, int, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_MIDPRICE, period);
+  u.outputs[0] = d_outputs;
+  Planes P;
+  P.p[tb::P_HIGH] = d_highs; P.p[tb::P_LOW] = d_lows;
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_midprice_batch_d");
+}
+ctStatus_t ct_midprice_d(const float* d_high, const float* d_low, float* d_output, int size, int period,
+                         cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_MIDPRICE, period);
+  u.outputs[0] = d_output;
+  Planes P;
+  P.p[tb::P_HIGH] = d_high; P.p[tb::P_LOW] = d_low;
+  return run_single(P.p, u, size, 1, stream, "ct_midprice_d");
 }
 
 // ------------------------------------------------------------ candles

@@ -8,11 +8,13 @@ namespace tb {
 
 // Indicator families the engine evaluates. Each maps to one reference batch
 // entry point (ct_<family>_batch_d) except CDL, which evaluates any subset of
-// the candle patterns in one pass.
+// the candle patterns in one pass. New families are appended after CDL so the
+// public ids stay stable.
 enum Family : int {
   F_SMA = 0, F_EMA, F_WMA, F_RSI, F_MACD, F_ATR, F_NATR, F_TRANGE, F_ADX, F_DX,
   F_BBANDS, F_STOCH, F_CCI, F_OBV, F_AD, F_ADOSC, F_MFI, F_WILLR, F_SUM, F_MIN,
   F_MAX, F_STDDEV, F_VAR, F_LINEARREG, F_CORREL, F_DEMA, F_TEMA, F_T3, F_CDL,
+  F_ROC, F_RMA, F_MEDPRICE, F_TYPPRICE, F_MIDPRICE,
   F_COUNT
 };
 

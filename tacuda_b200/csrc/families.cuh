@@ -122,9 +122,12 @@ __device__ __forceinline__ double round_tail(const Ctx<K>& c, double v) {
 struct EmaStage {
   int p, start;
   double beta, k, inv;
+  // period 1 copies the input (TA_EMA); RMA clears it and keeps the general
+  // steps, so a NaN propagates through fma(0, y, x) as in TA_RMA
+  bool copy1 = true;
   __device__ __forceinline__ void coef(int cnt, double& a, double& w) const {
     if (cnt < start) { a = 1.0; w = 0.0; return; }
-    if (p == 1) { a = 0.0; w = 1.0; return; }
+    if (p == 1 && copy1) { a = 0.0; w = 1.0; return; }
     const int r = cnt - start;
     if (r < p - 1) { a = 1.0; w = 1.0; }
     else if (r == p - 1) { a = inv; w = inv; }
@@ -138,7 +141,7 @@ struct EmaStage {
   }
   __device__ __forceinline__ double step(int cnt, double y, double x) const {
     if (cnt < start) return y;
-    if (p == 1) return x;
+    if (p == 1 && copy1) return x;
     const int r = cnt - start;
     if (r < p - 1) return y + x;
     if (r == p - 1) return (y + x) / p;
@@ -146,7 +149,7 @@ struct EmaStage {
   }
   __device__ __forceinline__ bool ready(int cnt) const { return cnt >= start + p - 1; }
   // first count whose map is the constant steady one
-  __device__ __forceinline__ int steady_from() const { return p == 1 ? 0 : start + p; }
+  __device__ __forceinline__ int steady_from() const { return p == 1 && copy1 ? 0 : start + p; }
 };
 
 // Scan one stage over the round. in(t, k) gives the FP64 input of the lane's
@@ -236,11 +239,15 @@ __host__ __device__ inline void talib_ema_coeffs(int p, double& beta, double& k)
 
 // EMA(p): talib08:5546-5627 TA_EMA; leading NaNs skipped (BatchFused.cu:34-41).
 // fp[0] = beta, fp[1] = k (host-precomputed TA-Lib coefficients).
+// RMA(p) is the same stage (talib08:13614-13683 TA_RMA: mean seed, then
+// fma(wBeta, y, wAlpha*x)) with wBeta = (p-1)/p, wAlpha = 1 - wBeta and no
+// period-1 copy; the reference's TA-Lib runner skips the row's leading NaNs
+// the same way (src/compat/Talib08.cu:72-84).
 template <int K>
 __device__ __forceinline__ void ema_round(const Ctx<K>& c, const Job& j, Carry& cy) {
   const int pl = j.in[0];
   const int f = resolve_start(c, cy, pl, j.lb_slot);
-  const EmaStage st{j.ip[0], 0, j.fp[0], j.fp[1], 1.0 / j.ip[0]};
+  const EmaStage st{j.ip[0], 0, j.fp[0], j.fp[1], 1.0 / j.ip[0], j.family != F_RMA};
   cy.v[0] = stage_round(
       c, f, st, cy.v[0], [&](int t, int) { return (double)c.x(pl, t); },
       [&](int k, int cnt, double v) { c.put(0, k, (cnt >= 0 && st.ready(cnt)) ? (float)v : qnan()); },
@@ -960,6 +967,73 @@ __device__ __forceinline__ void minmax_round(const Ctx<K>& c, const Job& j, Carr
     c.put(0, k, o);
   }
   cy.f = f;
+  c.flush(0, (float*)j.out[0]);
+}
+
+// ROC(p): src/indicators/ROC.cu:10-21, the reference's float arithmetic:
+// ((x[t] - x[t-p]) / x[t-p]) * 100 from bar p, 0 where x[t-p] == 0 (NaN
+// inputs propagate: NaN != 0).
+template <int K>
+__device__ __forceinline__ void roc_round(const Ctx<K>& c, const Job& j) {
+  const int pl = j.in[0], p = j.ip[0];
+  const int g0 = c.gb0();
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int t = g0 + k;
+    if (!c.valid(t)) break;
+    float o = qnan();
+    if (t >= p) {
+      const float prev = c.x(pl, t - p), curr = c.x(pl, t);
+      o = prev != 0.0f ? ((curr - prev) / prev) * 100.0f : 0.0f;
+    }
+    c.put(0, k, o);
+  }
+  c.flush(0, (float*)j.out[0]);
+}
+
+// MEDPRICE: src/indicators/MedPrice.cu:12-14, 0.5f * (h + l);
+// TYPPRICE: src/indicators/TypPrice.cu:13-15, (h + l + c) / 3.0f. Float
+// arithmetic in the reference's order; no warm-up.
+template <int K>
+__device__ __forceinline__ void price_round(const Ctx<K>& c, const Job& j, bool typ) {
+  const int ph = j.in[0], plo = j.in[1], pc = j.in[2];
+  const int g0 = c.gb0();
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int t = g0 + k;
+    if (!c.valid(t)) break;
+    const float h = c.x(ph, t), l = c.x(plo, t);
+    c.put(0, k, typ ? (h + l + c.x(pc, t)) / 3.0f : 0.5f * (h + l));
+  }
+  c.flush(0, (float*)j.out[0]);
+}
+
+// MIDPRICE(p): src/indicators/MIDPRICE.cu:11-24: fmaxf / fminf over the window
+// [t-p+1, t] of high / low (NaN ignored unless the whole window is NaN), then
+// 0.5f * (max + min), from bar p-1. Lane sweeps when the warp meets no NaN.
+template <int K>
+__device__ __forceinline__ void midprice_round(const Ctx<K>& c, const Job& j) {
+  const int ph = j.in[0], plo = j.in[1], p = j.ip[0];
+  const int g0 = c.gb0();
+  float his[K], los[K];
+  bool fast = p - 1 >= K;
+  if (fast) {
+    const bool n1 = lane_window_ext<K, true>(c, ph, p, his);
+    const bool n2 = lane_window_ext<K, false>(c, plo, p, los);
+    fast = !n1 && !n2;
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int t = g0 + k;
+    if (!c.valid(t)) break;
+    float o = qnan();
+    if (t >= p - 1) {
+      const float hi = fast ? his[k] : win_max(c, ph, t, p);
+      const float lo = fast ? los[k] : win_min(c, plo, t, p);
+      o = 0.5f * (hi + lo);
+    }
+    c.put(0, k, o);
+  }
   c.flush(0, (float*)j.out[0]);
 }
 

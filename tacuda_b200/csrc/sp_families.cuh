@@ -344,6 +344,69 @@ __device__ void sp_willr(SP_ARGS) {
   }
 }
 
+// ROC (src/indicators/ROC.cu:10-21, float arithmetic)
+__device__ void sp_roc(SP_ARGS) {
+  const int pl = j.in[0], p = j.ip[0];
+  for (int c = 0; c < drv.nchunks; ++c) {
+    drv.begin(c);
+    const Row rw = drv.row(c);
+    const float* X_pl = drv.pptr(c, pl);
+    for_chunk(rw, [&](int r, long long t) {
+      float o = qnan();
+      if (t >= p) {
+        const float prev = X_pl[r - p], curr = X_pl[r];
+        o = prev != 0.0f ? ((curr - prev) / prev) * 100.0f : 0.0f;
+      }
+      st.put(0, lane, r, o);
+    });
+    SP_FLUSH(0);
+    drv.end(c);
+  }
+}
+
+// MEDPRICE / TYPPRICE (src/indicators/MedPrice.cu:12-14, TypPrice.cu:13-15)
+__device__ void sp_price(SP_ARGS, bool typ) {
+  const int ph = j.in[0], plo = j.in[1], pc = j.in[2];
+  for (int c = 0; c < drv.nchunks; ++c) {
+    drv.begin(c);
+    const Row rw = drv.row(c);
+    const float* X_ph = drv.pptr(c, ph);
+    const float* X_plo = drv.pptr(c, plo);
+    const float* X_pc = typ ? drv.pptr(c, pc) : X_ph;
+    for_chunk(rw, [&](int r, long long) {
+      const float h = X_ph[r], l = X_plo[r];
+      st.put(0, lane, r, typ ? (h + l + X_pc[r]) / 3.0f : 0.5f * (h + l));
+    });
+    SP_FLUSH(0);
+    drv.end(c);
+  }
+}
+
+// MIDPRICE (src/indicators/MIDPRICE.cu:11-24): fmaxf / fminf window extrema
+__device__ void sp_midprice(SP_ARGS) {
+  const int ph = j.in[0], plo = j.in[1], p = j.ip[0];
+  for (int c = 0; c < drv.nchunks; ++c) {
+    drv.begin(c);
+    const Row rw = drv.row(c);
+    const float* X_ph = drv.pptr(c, ph);
+    const float* X_plo = drv.pptr(c, plo);
+    for_chunk(rw, [&](int r, long long t) {
+      float o = qnan();
+      if (t >= p - 1) {
+        float hi = X_ph[r - p + 1], lo = X_plo[r - p + 1];
+        for (int i = 1; i < p; ++i) {
+          hi = fmaxf(hi, X_ph[r - p + 1 + i]);
+          lo = fminf(lo, X_plo[r - p + 1 + i]);
+        }
+        o = 0.5f * (hi + lo);
+      }
+      st.put(0, lane, r, o);
+    });
+    SP_FLUSH(0);
+    drv.end(c);
+  }
+}
+
 // STOCH (talib08:16115-16302): fastK into the warp line for the chunk and the
 // 2(d-1) bars before it, then slowK / slowD as direct means.
 __device__ void sp_stoch(SP_ARGS) {
@@ -499,6 +562,7 @@ __device__ void sp_mfi(SP_ARGS) {
 __device__ void sp_ema(SP_ARGS) {
   const int pl = j.in[0], p = j.ip[0];
   const double beta = j.fp[0], kk = j.fp[1];
+  const bool copy1 = j.family != F_RMA;  // TA_RMA has no period-1 copy
   double y = 0.0;
   long long cnt = -1;  // count of the current bar since the first non-NaN
   for (int c = 0; c < drv.nchunks; ++c) {
@@ -510,7 +574,7 @@ __device__ void sp_ema(SP_ARGS) {
       float o = qnan();
       if (cnt >= 0 || !isnan(x)) {
         ++cnt;
-        if (p == 1) y = x;
+        if (p == 1 && copy1) y = x;
         else if (cnt < p - 1) y += x;
         else if (cnt == p - 1) y = (y + x) / p;
         else y = fma(beta, y, kk * x);

@@ -29,6 +29,7 @@ CASES = {
     "macd": dict(fast=12, slow=26, signal=9), "bbands": dict(period=20, up=2.0, dn=2.0),
     "atr": dict(period=14), "trange": {}, "stoch": dict(k=14, d=3), "obv": {}, "ad": {},
     "mfi": dict(period=14), "adosc": dict(fast=3, slow=10), "natr": dict(period=14),
+    "roc": dict(period=10), "rma": dict(period=14), "medprice": {}, "typprice": {}, "midprice": dict(period=14),
 }
 
 

@@ -41,6 +41,11 @@ SPECS = {
     "ad": ("ct_ad_batch_d", HLCV, 1, []),
     "adosc": ("ct_adosc_batch_d", HLCV, 1, [("i", "fast"), ("i", "slow")]),
     "correl": ("ct_correl_batch_d", ["x", "y"], 1, [("i", "period")]),
+    "roc": ("ct_roc_batch_d", ["close"], 1, [("i", "period")]),
+    "rma": ("ct_rma_batch_d", ["close"], 1, [("i", "period")]),
+    "medprice": ("ct_medprice_batch_d", ["high", "low"], 1, []),
+    "typprice": ("ct_typprice_batch_d", HLC, 1, []),
+    "midprice": ("ct_midprice_batch_d", ["high", "low"], 1, [("i", "period")]),
 }
 
 DEFAULTS = {
@@ -51,6 +56,7 @@ DEFAULTS = {
     "trange": {}, "adx": dict(period=14), "dx": dict(period=14), "willr": dict(period=14), "cci": dict(period=14),
     "macd": dict(fast=12, slow=26, signal=9), "bbands": dict(period=20, up=2.0, dn=2.0), "stoch": dict(k=14, d=3),
     "obv": {}, "mfi": dict(period=14), "ad": {}, "adosc": dict(fast=3, slow=10), "correl": dict(period=30),
+    "roc": dict(period=10), "rma": dict(period=14), "medprice": {}, "typprice": {}, "midprice": dict(period=14),
 }
 
 

@@ -77,6 +77,9 @@ VARIANTS = {
     "tema": [dict(period=2), dict(period=20)],
     "t3": [dict(period=1, vfactor=0.7), dict(period=8, vfactor=0.4)],
     "correl": [dict(period=2), dict(period=100)],
+    "roc": [dict(period=1), dict(period=2), dict(period=300)],
+    "rma": [dict(period=1), dict(period=2), dict(period=60)],
+    "midprice": [dict(period=1), dict(period=2), dict(period=40)],
 }
 
 
@@ -175,7 +178,8 @@ def test_leading_nan_and_interior_nan_semantics(mode):
         v[2, 300] = np.nan
     d = oracle_data(d)
     dp = device_planes(d)
-    for name in ("ema", "rsi", "macd", "sma", "bbands", "willr", "min", "max", "dema"):
+    for name in ("ema", "rsi", "macd", "sma", "bbands", "willr", "min", "max", "dema", "roc", "rma",
+                 "medprice", "typprice", "midprice"):
         got = to_np(call_batch_d(name, dp, DEFAULTS[name]))
         ref = O.run(name, d, **DEFAULTS[name])
         for i, (g, r) in enumerate(zip(got, ref)):
@@ -235,8 +239,8 @@ def test_graph_capture_replay_equals_eager(mode):
 
 
 LOOKBACK_FAMILIES = ["ema", "dema", "tema", "t3", "rsi", "macd", "atr", "natr", "adx", "dx", "obv", "ad", "adosc",
-                     "min", "max", "correl", "sma", "stoch", "mfi"]
-SINGLE_INPUT = {"ema", "dema", "tema", "t3", "rsi", "macd", "min", "max", "sma"}
+                     "min", "max", "correl", "sma", "stoch", "mfi", "rma", "roc", "midprice"]
+SINGLE_INPUT = {"ema", "dema", "tema", "t3", "rsi", "macd", "min", "max", "sma", "rma", "roc"}
 
 
 @pytest.mark.parametrize("bars", ["4", "16"])
@@ -382,3 +386,81 @@ def test_host_entry_matches_device_entry(S, T):
     for n in workloads.PASS13_OUTPUTS:
         np.testing.assert_array_equal(houts[n].numpy().view(np.uint32), douts[n].cpu().numpy().view(np.uint32),
                                       err_msg=n)
+
+
+FLOAT_KERNELS = {"roc": [dict(period=1), dict(period=10), dict(period=700)], "medprice": [{}], "typprice": [{}],
+                 "midprice": [dict(period=1), dict(period=7), dict(period=100)]}
+
+
+@pytest.mark.parametrize("name", sorted(FLOAT_KERNELS))
+def test_float_kernel_families_bit_exact(name, mode):
+    """ROC, MEDPRICE, TYPPRICE and MIDPRICE repeat the reference kernels' float
+    arithmetic, so every output word equals the oracle's float result, with
+    zeros (ROC's zero divisor), NaN and infinite bars mixed in."""
+    d = synthetic.ohlcv(9, 2500, seed=41)
+    d["close"][1, ::97] = 0.0
+    d["close"][2, 50:60] = np.nan
+    d["high"][3, 400:410] = np.nan
+    d["low"][4, 1000] = -np.inf
+    d["high"][5, :] = np.nan  # whole windows of NaN: MIDPRICE stays NaN there
+    dp = device_planes(d)
+    for p in FLOAT_KERNELS[name]:
+        got = to_np(call_batch_d(name, dp, p))[0]
+        ref = O.run(name, d, **p)[0].astype(np.float32)
+        np.testing.assert_array_equal(np.isnan(got), np.isnan(ref), err_msg=f"{name}{p}")
+        m = ~np.isnan(ref)
+        np.testing.assert_array_equal(got[m].view(np.uint32), ref[m].view(np.uint32), err_msg=f"{name}{p}")
+
+
+def test_rma_period_one_propagates_nan(mode):
+    """TA_RMA has no period-1 shortcut: fma(0, NaN, x) keeps a NaN from an
+    interior bar to the end of the row (unlike EMA(1), which copies)."""
+    x = np.array([[np.nan, 1.0, 2.0, np.nan, 3.0, 4.0]], np.float32)
+    got = to_np(call_batch_d("rma", device_planes({"close": x}), dict(period=1)))[0]
+    ref = O.run("rma", {"close": x}, period=1)[0]
+    np.testing.assert_array_equal(np.isnan(got), np.isnan(ref))
+    assert np.isnan(got[0, 3:]).all() and (got[0, 1:3] == [1.0, 2.0]).all()
+
+
+NEW_JOBS = [("roc", (10,), {"period": 10}), ("rma", (14,), {"period": 14}), ("medprice", (), {}),
+            ("typprice", (), {}), ("midprice", (14,), {"period": 14}), ("ema", (14,), {"period": 14})]
+
+
+def test_fused_pass_with_price_transforms_roc_rma(mode):
+    """ROC, RMA, MEDPRICE, TYPPRICE and MIDPRICE share one fused launch with an
+    EMA job on uniform rows (bit-equal to their single entry points) and on a
+    ragged plan (against the oracle)."""
+    S, T = 41, 900
+    d = synthetic.ohlcv(S, T, seed=43)
+    dp = device_planes(d)
+    outs = [torch.full((S, T), 777.0, device="cuda") for _ in NEW_JOBS]
+    jobs = [tb.make_job(fam, p, (), [o.data_ptr()]) for (fam, p, _), o in zip(NEW_JOBS, outs)]
+    series = tb.make_series({k: v.data_ptr() for k, v in dp.items() if k in tb.PLANE_ID}, S, T)
+    tb.fused_batch_d(series, jobs, 0)
+    torch.cuda.synchronize()
+    for (fam, _, kw), o in zip(NEW_JOBS, outs):
+        g = o.cpu().numpy()
+        compare(g, O.run(fam, d, **kw)[0], f"fused {fam}")
+        single = to_np(call_batch_d(fam, dp, kw))[0]
+        np.testing.assert_array_equal(g.view(np.uint32), single.view(np.uint32), err_msg=f"fused vs single {fam}")
+
+    lengths = synthetic.ragged_lengths(120, 1, 3000, seed=44)
+    lengths[:4] = [0, 1, 15, 2049]
+    planes, off = synthetic.ragged_ohlcv(lengths, seed=45)
+    rp = {k: torch.from_numpy(v).to("cuda") for k, v in planes.items()}
+    doff = torch.from_numpy(off).to("cuda")
+    N = int(off[-1])
+    routs = [torch.full((N,), 777.0, device="cuda") for _ in NEW_JOBS]
+    rjobs = [tb.make_job(fam, p, (), [o.data_ptr()]) for (fam, p, _), o in zip(NEW_JOBS, routs)]
+    plan = tb.Plan(rjobs, len(lengths), 0, off)
+    rseries = tb.make_series({k: v.data_ptr() for k, v in rp.items()}, len(lengths), 0, doff.data_ptr())
+    plan.execute(rseries, rjobs, 0)
+    torch.cuda.synchronize()
+    for (fam, _, kw), o in zip(NEW_JOBS, routs):
+        ref = O.run(fam, planes, offsets=off, **kw)[0]
+        g = o.cpu().numpy()
+        for s in range(len(lengths)):
+            a, b = off[s], off[s + 1]
+            if b > a:
+                compare(g[a:b], ref[a:b], f"ragged {fam} row {s} len {b - a}")
+    plan.close()

@@ -23,6 +23,7 @@ CASES = {
     "macd": dict(fast=12, slow=26, signal=9), "bbands": dict(period=20, up=2.0, dn=2.0),
     "atr": dict(period=14), "trange": {}, "stoch": dict(k=14, d=3), "obv": {}, "ad": {},
     "mfi": dict(period=14), "adosc": dict(fast=3, slow=10), "natr": dict(period=14),
+    "roc": dict(period=10), "rma": dict(period=14), "medprice": {}, "typprice": {}, "midprice": dict(period=14),
 }
 
 
@@ -149,3 +150,39 @@ def test_leading_nan_delays_recurrences():
         for u, v in zip(a, b):
             assert np.all(np.isnan(v[0, :7]))
             np.testing.assert_array_equal(u[0], v[0, 7:])
+
+
+def test_roc_zero_divisor_and_float_order():
+    # ROC.cu:18-20: 0 where the earlier bar is 0, float ((x - prev) / prev) * 100
+    x = np.array([[0.0, 1.0, 2.0, 3.0, 0.5, np.nan, 7.0]], np.float32)
+    got = O.run("roc", {"close": x}, period=2)[0][0]
+    assert np.isnan(got[:2]).all()
+    assert got[2] == 0.0
+    exp = np.float32((np.float32(3.0) - np.float32(1.0)) / np.float32(1.0)) * np.float32(100.0)
+    assert got[3] == exp
+    assert got[4] == np.float32(np.float32(np.float32(0.5) - np.float32(2.0)) / np.float32(2.0)) * np.float32(100.0)
+    assert np.isnan(got[5]) and got[6] == np.float32(np.float32(7.0 - 0.5) / np.float32(0.5)) * np.float32(100.0)
+
+
+def test_price_transforms_known_answers():
+    h = np.array([[3.0, 5.0, np.nan, 9.0]], np.float32)
+    l = np.array([[1.0, 2.0, 4.0, 1.0]], np.float32)
+    c = np.array([[2.0, 4.0, 4.0, 1.0]], np.float32)
+    med = O.run("medprice", {"high": h, "low": l})[0][0]
+    typ = O.run("typprice", {"high": h, "low": l, "close": c})[0][0]
+    np.testing.assert_array_equal(med[[0, 1, 3]], [2.0, 3.5, 5.0])
+    assert np.isnan(med[2]) and np.isnan(typ[2])
+    assert typ[0] == 2.0 and typ[1] == np.float32(np.float32(11.0) / np.float32(3.0))
+    # MIDPRICE: fmaxf/fminf skip the NaN high inside the window
+    mid = O.run("midprice", {"high": h, "low": l}, period=2)[0][0]
+    assert np.isnan(mid[0])
+    np.testing.assert_array_equal(mid[1:], [3.0, 3.5, 5.0])
+
+
+def test_rma_is_wilder_average():
+    x = np.array([[np.nan, np.nan, 1.0, 2.0, 3.0, 4.0, 5.0]], np.float32)
+    got = O.run("rma", {"close": x}, period=3)[0][0]
+    assert np.isnan(got[:4]).all()
+    assert got[4] == 2.0
+    # fma(wBeta, 2, wAlpha * 4) with wBeta = 2/3: 8/3 up to the coefficients' rounding
+    assert abs(got[5] - 8.0 / 3.0) < 1e-14
