@@ -84,6 +84,13 @@ CTAPI_EXPORT ctStatus_t ct_rma_batch_d(const float *d_inputs, float *d_outputs, 
 CTAPI_EXPORT ctStatus_t ct_typprice_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1300 */
 CTAPI_EXPORT ctStatus_t ct_medprice_batch_d(const float *d_highs, const float *d_lows, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1339 */
 CTAPI_EXPORT ctStatus_t ct_midprice_batch_d(const float *d_highs, const float *d_lows, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1727 */
+CTAPI_EXPORT ctStatus_t ct_rocp_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1016 */
+CTAPI_EXPORT ctStatus_t ct_rocr_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1026 */
+CTAPI_EXPORT ctStatus_t ct_rocr100_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1036 */
+CTAPI_EXPORT ctStatus_t ct_momentum_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:997 */
+CTAPI_EXPORT ctStatus_t ct_midpoint_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1516 */
+CTAPI_EXPORT ctStatus_t ct_wclprice_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1312 */
+CTAPI_EXPORT ctStatus_t ct_avgprice_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1428 */
 
 /* candlestick patterns: float signal (+-100/+-80/+-200), warm-up 0 */
 CTAPI_EXPORT ctStatus_t ct_cdl_doji_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1877 */
@@ -184,6 +191,13 @@ CTAPI_EXPORT ctStatus_t ct_medprice_d(const float* d_high, const float* d_low, f
 CTAPI_EXPORT ctStatus_t ct_typprice_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:345 */
 CTAPI_EXPORT ctStatus_t ct_midprice_d(const float* d_high, const float* d_low, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:511 */
 CTAPI_EXPORT ctStatus_t ct_rma_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:1212 */
+CTAPI_EXPORT ctStatus_t ct_rocp_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:177 */
+CTAPI_EXPORT ctStatus_t ct_rocr_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:180 */
+CTAPI_EXPORT ctStatus_t ct_rocr100_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:183 */
+CTAPI_EXPORT ctStatus_t ct_momentum_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:171 */
+CTAPI_EXPORT ctStatus_t ct_midpoint_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:447 */
+CTAPI_EXPORT ctStatus_t ct_wclprice_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:349 */
+CTAPI_EXPORT ctStatus_t ct_avgprice_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:338 */
 CTAPI_EXPORT ctStatus_t ct_cdl_doji_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:555 */
 CTAPI_EXPORT ctStatus_t ct_cdl_hammer_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:559 */
 CTAPI_EXPORT ctStatus_t ct_cdl_inverted_hammer_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:565 */
@@ -308,7 +322,9 @@ typedef enum ctB200Family {
   CT_B200_CCI, CT_B200_OBV, CT_B200_AD, CT_B200_ADOSC, CT_B200_MFI, CT_B200_WILLR,
   CT_B200_SUM, CT_B200_MIN, CT_B200_MAX, CT_B200_STDDEV, CT_B200_VAR, CT_B200_LINEARREG,
   CT_B200_CORREL, CT_B200_DEMA, CT_B200_TEMA, CT_B200_T3, CT_B200_CDL,
-  CT_B200_ROC, CT_B200_RMA, CT_B200_MEDPRICE, CT_B200_TYPPRICE, CT_B200_MIDPRICE
+  CT_B200_ROC, CT_B200_RMA, CT_B200_MEDPRICE, CT_B200_TYPPRICE, CT_B200_MIDPRICE,
+  CT_B200_ROCP, CT_B200_ROCR, CT_B200_ROCR100, CT_B200_MOM, CT_B200_AVGPRICE, CT_B200_WCLPRICE,
+  CT_B200_MIDPOINT
 } ctB200Family_t;
 
 /* Input planes of a batch. */

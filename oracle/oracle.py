@@ -55,6 +55,13 @@ FAMILIES = {
     "medprice": (30, ("high", "low"), ("out",), (), ()),
     "typprice": (31, ("high", "low", "close"), ("out",), (), ()),
     "midprice": (32, ("high", "low"), ("out",), ("period",), ()),
+    "rocp": (33, ("close",), ("out",), ("period",), ()),
+    "rocr": (34, ("close",), ("out",), ("period",), ()),
+    "rocr100": (35, ("close",), ("out",), ("period",), ()),
+    "momentum": (36, ("close",), ("out",), ("period",), ()),
+    "avgprice": (37, ("open", "high", "low", "close"), ("out",), (), ()),
+    "wclprice": (38, ("high", "low", "close"), ("out",), (), ()),
+    "midpoint": (39, ("close",), ("out",), ("period",), ()),
 }
 
 _P = ct.c_void_p
@@ -160,7 +167,7 @@ def _load_ref():
 
 
 _REF_SINGLE = {"sma": 0, "ema": 1, "wma": 2, "rsi": 3, "stddev": 4, "var": 5,
-               "linearreg": 6, "dema": 7, "tema": 8, "t3": 9, "roc": 10, "rma": 11}
+               "linearreg": 6, "dema": 7, "tema": 8, "t3": 9, "roc": 10, "rma": 11, "rocp": 12}
 _REF_STATES = {"obv": 0, "ad": 1, "mfi": 2, "adosc": 3, "natr": 4}
 _REF_PRICE = {"medprice": 0, "typprice": 1, "midprice": 2}
 REF_FAMILIES = (tuple(_REF_SINGLE) + ("macd", "bbands", "atr", "trange", "stoch") + tuple(_REF_STATES)

@@ -8,7 +8,8 @@
 //     TA-Lib 0.8.3 C (commit 62021c1d, third_party/ta_lib_0_8_3/PROVENANCE.json)
 //     in FP64: TA_SMA, TA_EMA, TA_WMA, TA_RSI, TA_MACD, TA_ATR, TA_BBANDS,
 //     TA_STOCH, TA_STDDEV, TA_VAR, TA_LINEARREG, TA_DEMA, TA_TEMA, TA_T3,
-//     TA_TRANGE, TA_ROC, TA_RMA, TA_MEDPRICE, TA_TYPPRICE, TA_MIDPRICE.
+//     TA_TRANGE, TA_ROC, TA_ROCP, TA_RMA, TA_MEDPRICE, TA_TYPPRICE,
+//     TA_MIDPRICE.
 //   * include/utils/StreamStates.h: ObvState, AdState, precise::MfiState,
 //     precise::AdoscState, precise::NatrState (the fused batch arithmetic).
 //   * include/utils/CandleUtils.h: the cdl_*_talib pattern decisions.
@@ -71,7 +72,7 @@ int ref_threads(void) { return omp_get_max_threads(); }
 
 // One-input, one-output TA-Lib families: 0 SMA, 1 EMA, 2 WMA, 3 RSI,
 // 4 STDDEV(nbdev=1), 5 VAR(nbdev=1), 6 LINEARREG, 7 DEMA, 8 TEMA, 9 T3(v=fparam),
-// 10 ROC, 11 RMA.
+// 10 ROC, 11 RMA, 12 ROCP.
 int ref_single(int fam, const float* x, int S, int T, int p, double fparam,
                double* out, int threads) {
   int rc_all = 0;
@@ -96,6 +97,7 @@ int ref_single(int fam, const float* x, int S, int T, int p, double fparam,
       case 9: rc = TA_T3(a, 0, T - 1, in, p, fparam, &beg, &nb, o); break;
       case 10: rc = TA_ROC(a, 0, T - 1, in, p, &beg, &nb, o); break;
       case 11: rc = TA_RMA(a, 0, T - 1, in, p, &beg, &nb, o); break;
+      case 12: rc = TA_ROCP(a, 0, T - 1, in, p, &beg, &nb, o); break;
       default: rc = TA_BAD_PARAM;
     }
     if (rc != TA_SUCCESS) { rc_all = static_cast<int>(rc); nb = 0; }

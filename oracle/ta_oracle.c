@@ -704,17 +704,33 @@ static void row_t3(RowCtx* r) { cascade_row(r->in[0], r->n, r->ip[0], 6, 1, r->f
 
 /* ------------------------------------------------- ROC, RMA, price transforms */
 
-/* src/indicators/ROC.cu:10-21: float ((x - prev) / prev) * 100 from bar p, 0
- * where prev == 0; the float arithmetic is kept (C float ops, no contraction). */
-static void row_roc(RowCtx* r) {
+/* The ROC kernels in float arithmetic (C float ops, no contraction), from bar
+ * p with prev = x[t-p]; the ratios give 0 where prev == 0:
+ *   0 ROC     src/indicators/ROC.cu:10-21      ((x - prev) / prev) * 100
+ *   1 ROCP    src/indicators/ROCP.cu:10-20     (x - prev) / prev
+ *   2 ROCR    src/indicators/ROCR.cu:10-20     x / prev
+ *   3 ROCR100 src/indicators/ROCR100.cu:10-21  (x / prev) * 100
+ *   4 MOM     src/indicators/Momentum.cu:10-18 x - prev */
+static void roc_row(RowCtx* r, int mode) {
   const float* x = r->in[0]; int n = r->n, p = r->ip[0]; double* o = r->out[0];
   fill_nan(o, n);
   for (int t = p; t < n; ++t) {
     const float prev = x[t - p], curr = x[t];
-    const float v = prev != 0.0f ? ((curr - prev) / prev) * 100.0f : 0.0f;
+    float v;
+    if (mode == 4) v = curr - prev;
+    else if (!(prev != 0.0f)) v = 0.0f;
+    else if (mode == 0) v = ((curr - prev) / prev) * 100.0f;
+    else if (mode == 1) v = (curr - prev) / prev;
+    else if (mode == 2) v = curr / prev;
+    else v = (curr / prev) * 100.0f;
     o[t] = (double)v;
   }
 }
+static void row_roc(RowCtx* r) { roc_row(r, 0); }
+static void row_rocp(RowCtx* r) { roc_row(r, 1); }
+static void row_rocr(RowCtx* r) { roc_row(r, 2); }
+static void row_rocr100(RowCtx* r) { roc_row(r, 3); }
+static void row_mom(RowCtx* r) { roc_row(r, 4); }
 
 /* talib08:13614-13683 TA_RMA (mean of the first p, then fma(wBeta, y,
  * wAlpha * x)); the reference's TA-Lib runner starts after the row's leading
@@ -741,6 +757,32 @@ static void row_medprice(RowCtx* r) {
 static void row_typprice(RowCtx* r) {
   for (int t = 0; t < r->n; ++t)
     r->out[0][t] = (double)((r->in[0][t] + r->in[1][t] + r->in[2][t]) / 3.0f);
+}
+
+/* src/indicators/AvgPrice.cu:16-18: (o + h + l + c) * 0.25f in float. */
+static void row_avgprice(RowCtx* r) {
+  for (int t = 0; t < r->n; ++t)
+    r->out[0][t] = (double)((r->in[0][t] + r->in[1][t] + r->in[2][t] + r->in[3][t]) * 0.25f);
+}
+
+/* src/indicators/WclPrice.cu:14-16: (h + l + 2.0f * c) * 0.25f in float. */
+static void row_wclprice(RowCtx* r) {
+  for (int t = 0; t < r->n; ++t)
+    r->out[0][t] = (double)((r->in[0][t] + r->in[1][t] + 2.0f * r->in[2][t]) * 0.25f);
+}
+
+/* src/indicators/MIDPOINT.cu:13-35: fmaxf / fminf over the window of one
+ * plane, 0.5f * (max + min) from bar p-1; a window starting inside the row's
+ * leading NaN run is NaN (LeadingNaN.cuh:22-28 in_leading_nan_prefix). */
+static void row_midpoint(RowCtx* r) {
+  const float* x = r->in[0]; int n = r->n, p = r->ip[0]; double* o = r->out[0];
+  fill_nan(o, n);
+  const int f = leading_nan(x, n);
+  for (int t = p - 1; t < n; ++t) {
+    float hi = x[t - p + 1], lo = hi;
+    for (int k = t - p + 2; k <= t; ++k) { hi = fmaxf(hi, x[k]); lo = fminf(lo, x[k]); }
+    o[t] = (t - p + 1 < f) ? kNaN : (double)(0.5f * (hi + lo));
+  }
 }
 
 /* src/indicators/MIDPRICE.cu:11-24: fmaxf / fminf over [t-p+1, t] (NaN
@@ -780,6 +822,10 @@ static const FamSpec kFam[ORC_FAMILY_COUNT] = {
   [ORC_ROC] = {1, 1, 1, 0, row_roc, 1},      [ORC_RMA] = {1, 1, 1, 0, row_rma, 1},
   [ORC_MEDPRICE] = {2, 1, 0, 0, row_medprice, 0}, [ORC_TYPPRICE] = {3, 1, 0, 0, row_typprice, 0},
   [ORC_MIDPRICE] = {2, 1, 1, 0, row_midprice, 1},
+  [ORC_ROCP] = {1, 1, 1, 0, row_rocp, 1},    [ORC_ROCR] = {1, 1, 1, 0, row_rocr, 1},
+  [ORC_ROCR100] = {1, 1, 1, 0, row_rocr100, 1}, [ORC_MOM] = {1, 1, 1, 0, row_mom, 1},
+  [ORC_AVGPRICE] = {4, 1, 0, 0, row_avgprice, 0}, [ORC_WCLPRICE] = {3, 1, 0, 0, row_wclprice, 0},
+  [ORC_MIDPOINT] = {1, 1, 1, 0, row_midpoint, 1},
 };
 
 static int check_params(int family, const int* ip) {

@@ -11,11 +11,14 @@
  * reference tree (oracle/_ref); OBV AD ADOSC MFI NATR and the candle patterns are
  * pinned against the reference's StreamStates.h / CandleUtils.h compiled on the
  * host. RMA is pinned against the vendored TA_RMA (the reference's device path
- * runs that same function). ROC MEDPRICE TYPPRICE MIDPRICE restate the
- * reference's float kernels (src/indicators/ROC.cu, MedPrice.cu, TypPrice.cu,
- * MIDPRICE.cu) operation for operation; they are pinned against the vendored
- * TA_ROC / TA_MEDPRICE / TA_TYPPRICE / TA_MIDPRICE within the float tolerance
- * and by known answers. ADX DX CCI WILLR CORREL SUM MIN MAX have no CPU code in
+ * runs that same function). ROC ROCP ROCR ROCR100 MOM MEDPRICE TYPPRICE
+ * AVGPRICE WCLPRICE MIDPRICE MIDPOINT restate the reference's float kernels
+ * (src/indicators/ROC*.cu, Momentum.cu, MedPrice.cu, TypPrice.cu, AvgPrice.cu,
+ * WclPrice.cu, MIDPRICE.cu, MIDPOINT.cu) operation for operation. ROC ROCP
+ * MEDPRICE TYPPRICE MIDPRICE are pinned against the vendored TA-Lib functions
+ * of the same names within the float tolerance; ROCR ROCR100 MOM AVGPRICE
+ * WCLPRICE MIDPOINT are not in the vendored set and are pinned by known
+ * answers only. ADX DX CCI WILLR CORREL SUM MIN MAX have no CPU code in
  * the reference: they are pinned by known-answer tests only ("parity partially
  * unpinned").
  */
@@ -30,7 +33,8 @@ enum OracleFamily {
   ORC_ADX, ORC_DX, ORC_BBANDS, ORC_STOCH, ORC_CCI, ORC_OBV, ORC_AD, ORC_ADOSC,
   ORC_MFI, ORC_WILLR, ORC_SUM, ORC_MIN, ORC_MAX, ORC_STDDEV, ORC_VAR, ORC_LINEARREG,
   ORC_CORREL, ORC_DEMA, ORC_TEMA, ORC_T3, ORC_ROC, ORC_RMA, ORC_MEDPRICE,
-  ORC_TYPPRICE, ORC_MIDPRICE, ORC_FAMILY_COUNT
+  ORC_TYPPRICE, ORC_MIDPRICE, ORC_ROCP, ORC_ROCR, ORC_ROCR100, ORC_MOM,
+  ORC_AVGPRICE, ORC_WCLPRICE, ORC_MIDPOINT, ORC_FAMILY_COUNT
 };
 
 /* ins: the family's input planes (see oracle/oracle.py INPUTS); outs: its output

@@ -34,7 +34,8 @@ CT_STATUS = {
 # ctB200Family / ctB200Plane (include/tacuda.h)
 FAMILIES = ("sma", "ema", "wma", "rsi", "macd", "atr", "natr", "trange", "adx", "dx", "bbands", "stoch",
             "cci", "obv", "ad", "adosc", "mfi", "willr", "sum", "min", "max", "stddev", "var", "linearreg",
-            "correl", "dema", "tema", "t3", "cdl", "roc", "rma", "medprice", "typprice", "midprice")
+            "correl", "dema", "tema", "t3", "cdl", "roc", "rma", "medprice", "typprice", "midprice",
+            "rocp", "rocr", "rocr100", "momentum", "avgprice", "wclprice", "midpoint")
 FAMILY_ID = {n: i for i, n in enumerate(FAMILIES)}
 PLANES = ("open", "high", "low", "close", "volume", "aux")
 PLANE_ID = {n: i for i, n in enumerate(PLANES)}

@@ -46,6 +46,7 @@ ctStatus_t cuda_fail(ctStatus_t st, const char* where, cudaError_t e) {
 int min_period(int family) {
   switch (family) {
     case tb::F_OBV: case tb::F_AD: case tb::F_TRANGE: case tb::F_CDL: case tb::F_MEDPRICE: case tb::F_TYPPRICE:
+    case tb::F_AVGPRICE: case tb::F_WCLPRICE:
       return 0;
     default: return 1;
   }
@@ -54,14 +55,14 @@ int min_period(int family) {
 int default_inputs(int family, int* in) {
   switch (family) {
     case tb::F_ATR: case tb::F_NATR: case tb::F_TRANGE: case tb::F_ADX: case tb::F_DX:
-    case tb::F_STOCH: case tb::F_WILLR: case tb::F_CCI: case tb::F_TYPPRICE:
+    case tb::F_STOCH: case tb::F_WILLR: case tb::F_CCI: case tb::F_TYPPRICE: case tb::F_WCLPRICE:
       in[0] = tb::P_HIGH; in[1] = tb::P_LOW; in[2] = tb::P_CLOSE; return 3;
     case tb::F_MEDPRICE: case tb::F_MIDPRICE: in[0] = tb::P_HIGH; in[1] = tb::P_LOW; return 2;
     case tb::F_AD: case tb::F_ADOSC: case tb::F_MFI:
       in[0] = tb::P_HIGH; in[1] = tb::P_LOW; in[2] = tb::P_CLOSE; in[3] = tb::P_VOLUME; return 4;
     case tb::F_OBV: in[0] = tb::P_CLOSE; in[1] = tb::P_VOLUME; return 2;
     case tb::F_CORREL: in[0] = tb::P_CLOSE; in[1] = tb::P_AUX; return 2;
-    case tb::F_CDL:
+    case tb::F_CDL: case tb::F_AVGPRICE:
       in[0] = tb::P_OPEN; in[1] = tb::P_HIGH; in[2] = tb::P_LOW; in[3] = tb::P_CLOSE; return 4;
     default: in[0] = tb::P_CLOSE; return 1;
   }
@@ -100,7 +101,8 @@ ctStatus_t make_job(const ctB200Job& u, Job& j, const char* who) {
   switch (f) {
     case tb::F_SMA: case tb::F_SUM: case tb::F_WMA: case tb::F_BBANDS: case tb::F_STDDEV: case tb::F_VAR:
     case tb::F_LINEARREG: case tb::F_MIN: case tb::F_MAX: case tb::F_WILLR: case tb::F_CCI: case tb::F_MFI:
-    case tb::F_CORREL: case tb::F_ROC: case tb::F_MIDPRICE:
+    case tb::F_CORREL: case tb::F_ROC: case tb::F_MIDPRICE: case tb::F_ROCP: case tb::F_ROCR: case tb::F_ROCR100:
+    case tb::F_MOM: case tb::F_MIDPOINT:
       if (u.params[0] > kMaxWindow) return fail(CT_STATUS_UNSUPPORTED, std::string(who) + ": window period above 4096");
       break;
     case tb::F_STOCH:
@@ -346,6 +348,11 @@ TB_S1(min, tb::F_MIN)
 TB_S1(linearreg, tb::F_LINEARREG)
 TB_S1(roc, tb::F_ROC)  // tacuda.h:1007, tacuda_device.h:174
 TB_S1(rma, tb::F_RMA)  // tacuda.h:4110, tacuda_device.h:1212
+TB_S1(rocp, tb::F_ROCP)  // tacuda.h:1016, tacuda_device.h:177
+TB_S1(rocr, tb::F_ROCR)  // tacuda.h:1026, tacuda_device.h:180
+TB_S1(rocr100, tb::F_ROCR100)  // tacuda.h:1036, tacuda_device.h:183
+TB_S1(momentum, tb::F_MOM)  // tacuda.h:997, tacuda_device.h:171
+TB_S1(midpoint, tb::F_MIDPOINT)  // tacuda.h:1516, tacuda_device.h:447
 #undef TB_S1
 
 #define TB_HLC(NAME, FAM)                                                                                  \
@@ -581,6 +588,36 @@ ctStatus_t ct_typprice_d(const float* d_high, const float* d_low, const float* d
   u.outputs[0] = d_output;
   const Planes P = hlc(d_high, d_low, d_close);
   return run_single(P.p, u, size, 1, stream, "ct_typprice_d");
+}
+
+ctStatus_t ct_wclprice_batch_d(const float* d_highs, const float* d_lows, const float* d_closes, float* d_outputs,
+                               int seriesLen, int numSeries, int, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_WCLPRICE);
+  u.outputs[0] = d_outputs;
+  const Planes P = hlc(d_highs, d_lows, d_closes);
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_wclprice_batch_d");
+}
+ctStatus_t ct_wclprice_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, int size,
+                         cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_WCLPRICE);
+  u.outputs[0] = d_output;
+  const Planes P = hlc(d_high, d_low, d_close);
+  return run_single(P.p, u, size, 1, stream, "ct_wclprice_d");
+}
+
+ctStatus_t ct_avgprice_batch_d(const float* d_opens, const float* d_highs, const float* d_lows, const float* d_closes,
+                               float* d_outputs, int seriesLen, int numSeries, int, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_AVGPRICE);
+  u.outputs[0] = d_outputs;
+  const Planes P = ohlc(d_opens, d_highs, d_lows, d_closes);
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_avgprice_batch_d");
+}
+ctStatus_t ct_avgprice_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close,
+                         float* d_output, int size, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_AVGPRICE);
+  u.outputs[0] = d_output;
+  const Planes P = ohlc(d_open, d_high, d_low, d_close);
+  return run_single(P.p, u, size, 1, stream, "ct_avgprice_d");
 }
 
 ctStatus_t ct_midprice_batch_d(const float* d_highs, const float* d_lows, float* d_outputs, int seriesLen,

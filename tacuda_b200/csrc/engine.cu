@@ -96,11 +96,18 @@ __device__ __forceinline__ void run_job(const Ctx<K>& c, const Job& j, Carry& cy
     case F_CCI: cci_round(c, j); break;
     case F_MFI: mfi_round(c, j); break;
     case F_CORREL: correl_round(c, j, cy); break;
-    case F_ROC: roc_round(c, j); break;
+    case F_ROC: roc_round(c, j, 0); break;
+    case F_ROCP: roc_round(c, j, 1); break;
+    case F_ROCR: roc_round(c, j, 2); break;
+    case F_ROCR100: roc_round(c, j, 3); break;
+    case F_MOM: roc_round(c, j, 4); break;
     case F_RMA: ema_round(c, j, cy); break;
-    case F_MEDPRICE: price_round(c, j, false); break;
-    case F_TYPPRICE: price_round(c, j, true); break;
+    case F_MEDPRICE: price_round(c, j, 0); break;
+    case F_TYPPRICE: price_round(c, j, 1); break;
+    case F_AVGPRICE: price_round(c, j, 2); break;
+    case F_WCLPRICE: price_round(c, j, 3); break;
     case F_MIDPRICE: midprice_round(c, j); break;
+    case F_MIDPOINT: midpoint_round(c, j, cy); break;
     default: break;
   }
 }
@@ -303,11 +310,18 @@ __device__ void sp_run_job(sp::Driver& drv, const Job& j, const sp::Stage& st, c
     case F_OBV: sp::sp_volume(drv, j, st, ln, lane, 0); break;
     case F_AD: sp::sp_volume(drv, j, st, ln, lane, 1); break;
     case F_ADOSC: sp::sp_volume(drv, j, st, ln, lane, 2); break;
-    case F_ROC: sp::sp_roc(drv, j, st, ln, lane); break;
+    case F_ROC: sp::sp_roc(drv, j, st, ln, lane, 0); break;
+    case F_ROCP: sp::sp_roc(drv, j, st, ln, lane, 1); break;
+    case F_ROCR: sp::sp_roc(drv, j, st, ln, lane, 2); break;
+    case F_ROCR100: sp::sp_roc(drv, j, st, ln, lane, 3); break;
+    case F_MOM: sp::sp_roc(drv, j, st, ln, lane, 4); break;
     case F_RMA: sp::sp_ema(drv, j, st, ln, lane); break;
-    case F_MEDPRICE: sp::sp_price(drv, j, st, ln, lane, false); break;
-    case F_TYPPRICE: sp::sp_price(drv, j, st, ln, lane, true); break;
+    case F_MEDPRICE: sp::sp_price(drv, j, st, ln, lane, 0); break;
+    case F_TYPPRICE: sp::sp_price(drv, j, st, ln, lane, 1); break;
+    case F_AVGPRICE: sp::sp_price(drv, j, st, ln, lane, 2); break;
+    case F_WCLPRICE: sp::sp_price(drv, j, st, ln, lane, 3); break;
     case F_MIDPRICE: sp::sp_midprice(drv, j, st, ln, lane); break;
+    case F_MIDPOINT: sp::sp_minmax(drv, j, st, ln, lane, false, true); break;
     default:
       for (int c = 0; c < drv.nchunks; ++c) { drv.begin(c); drv.end(c); }
   }
@@ -415,7 +429,7 @@ int lb_slots(const Job& j) {
     case F_DX: return 1;
     case F_OBV: case F_AD: return 1;
     case F_ADOSC: return 3;
-    case F_MIN: case F_MAX: case F_CORREL: return 1;
+    case F_MIN: case F_MAX: case F_CORREL: case F_MIDPOINT: return 1;
     default: return 0;
   }
 }
@@ -425,7 +439,8 @@ int job_halo(const Job& j) {
     case F_SMA: case F_SUM: case F_WMA: case F_BBANDS: case F_STDDEV: case F_VAR:
     case F_LINEARREG: case F_MIN: case F_MAX: case F_WILLR: case F_CCI: case F_CORREL:
       return j.ip[0] - 1;
-    case F_MFI: case F_ROC: return j.ip[0];
+    case F_MFI: case F_ROC: case F_ROCP: case F_ROCR: case F_ROCR100: case F_MOM: return j.ip[0];
+    case F_MIDPOINT: return j.ip[0] - 1;
     case F_MIDPRICE: return j.ip[0] - 1;
     case F_STOCH: return j.ip[0] - 1 + 2 * (j.ip[1] - 1);
     case F_CDL: return 16;  // 10-bar averages anchored up to 5 bars back
@@ -439,14 +454,15 @@ unsigned job_planes(const Job& j) {
   switch (j.family) {
     case F_SMA: case F_EMA: case F_WMA: case F_RSI: case F_MACD: case F_BBANDS: case F_SUM:
     case F_MIN: case F_MAX: case F_STDDEV: case F_VAR: case F_LINEARREG: case F_DEMA:
-    case F_TEMA: case F_T3: case F_ROC: case F_RMA:
+    case F_TEMA: case F_T3: case F_ROC: case F_RMA: case F_ROCP: case F_ROCR: case F_ROCR100:
+    case F_MOM: case F_MIDPOINT:
       n = 1; break;
     case F_OBV: case F_CORREL: case F_MEDPRICE: case F_MIDPRICE: n = 2; break;
     case F_ATR: case F_NATR: case F_TRANGE: case F_ADX: case F_DX: case F_STOCH: case F_WILLR:
-    case F_TYPPRICE:
+    case F_TYPPRICE: case F_WCLPRICE:
       n = 3; break;
     case F_CCI: n = 3; break;
-    case F_AD: case F_ADOSC: case F_MFI: case F_CDL: n = 4; break;
+    case F_AD: case F_ADOSC: case F_MFI: case F_CDL: case F_AVGPRICE: n = 4; break;
     default: n = 0;
   }
   for (int i = 0; i < n; ++i) m |= 1u << j.in[i];

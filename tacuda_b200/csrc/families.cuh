@@ -970,11 +970,27 @@ __device__ __forceinline__ void minmax_round(const Ctx<K>& c, const Job& j, Carr
   c.flush(0, (float*)j.out[0]);
 }
 
-// ROC(p): src/indicators/ROC.cu:10-21, the reference's float arithmetic:
-// ((x[t] - x[t-p]) / x[t-p]) * 100 from bar p, 0 where x[t-p] == 0 (NaN
-// inputs propagate: NaN != 0).
+// ROC family from bar p, the reference kernels' float arithmetic (NaN inputs
+// propagate: NaN != 0), prev = x[t-p]:
+//   mode 0 ROC      ((x - prev) / prev) * 100   src/indicators/ROC.cu:10-21
+//   mode 1 ROCP     (x - prev) / prev           src/indicators/ROCP.cu:10-20
+//   mode 2 ROCR     x / prev                    src/indicators/ROCR.cu:10-20
+//   mode 3 ROCR100  (x / prev) * 100            src/indicators/ROCR100.cu:10-21
+//   mode 4 MOM      x - prev                    src/indicators/Momentum.cu:10-18
+// ROC* give 0 where prev == 0.
+__device__ __forceinline__ float roc_value(float curr, float prev, int mode) {
+  if (mode == 4) return curr - prev;
+  if (!(prev != 0.0f)) return 0.0f;
+  switch (mode) {
+    case 0: return ((curr - prev) / prev) * 100.0f;
+    case 1: return (curr - prev) / prev;
+    case 2: return curr / prev;
+    default: return (curr / prev) * 100.0f;
+  }
+}
+
 template <int K>
-__device__ __forceinline__ void roc_round(const Ctx<K>& c, const Job& j) {
+__device__ __forceinline__ void roc_round(const Ctx<K>& c, const Job& j, int mode) {
   const int pl = j.in[0], p = j.ip[0];
   const int g0 = c.gb0();
 #pragma unroll
@@ -983,27 +999,34 @@ __device__ __forceinline__ void roc_round(const Ctx<K>& c, const Job& j) {
     if (!c.valid(t)) break;
     float o = qnan();
     if (t >= p) {
-      const float prev = c.x(pl, t - p), curr = c.x(pl, t);
-      o = prev != 0.0f ? ((curr - prev) / prev) * 100.0f : 0.0f;
+      o = roc_value(c.x(pl, t), c.x(pl, t - p), mode);
     }
     c.put(0, k, o);
   }
   c.flush(0, (float*)j.out[0]);
 }
 
-// MEDPRICE: src/indicators/MedPrice.cu:12-14, 0.5f * (h + l);
-// TYPPRICE: src/indicators/TypPrice.cu:13-15, (h + l + c) / 3.0f. Float
-// arithmetic in the reference's order; no warm-up.
+// Price transforms, float arithmetic in the reference's order, no warm-up:
+//   mode 0 MEDPRICE  0.5f * (h + l)             src/indicators/MedPrice.cu:12-14
+//   mode 1 TYPPRICE  (h + l + c) / 3.0f         src/indicators/TypPrice.cu:13-15
+//   mode 2 AVGPRICE  (o + h + l + c) * 0.25f    src/indicators/AvgPrice.cu:16-18
+//   mode 3 WCLPRICE  (h + l + 2.0f * c) * 0.25f src/indicators/WclPrice.cu:14-16
+// Inputs in[0..] are (h, l[, c]) for modes 0,1,3 and (o, h, l, c) for mode 2.
 template <int K>
-__device__ __forceinline__ void price_round(const Ctx<K>& c, const Job& j, bool typ) {
-  const int ph = j.in[0], plo = j.in[1], pc = j.in[2];
+__device__ __forceinline__ void price_round(const Ctx<K>& c, const Job& j, int mode) {
+  const int p0 = j.in[0], p1 = j.in[1], p2 = j.in[2], p3 = j.in[3];
   const int g0 = c.gb0();
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const int t = g0 + k;
     if (!c.valid(t)) break;
-    const float h = c.x(ph, t), l = c.x(plo, t);
-    c.put(0, k, typ ? (h + l + c.x(pc, t)) / 3.0f : 0.5f * (h + l));
+    const float a = c.x(p0, t), b = c.x(p1, t);
+    float o;
+    if (mode == 0) o = 0.5f * (a + b);
+    else if (mode == 1) o = (a + b + c.x(p2, t)) / 3.0f;
+    else if (mode == 2) o = (a + b + c.x(p2, t) + c.x(p3, t)) * 0.25f;
+    else o = (a + b + 2.0f * c.x(p2, t)) * 0.25f;
+    c.put(0, k, o);
   }
   c.flush(0, (float*)j.out[0]);
 }
@@ -1034,6 +1057,37 @@ __device__ __forceinline__ void midprice_round(const Ctx<K>& c, const Job& j) {
     }
     c.put(0, k, o);
   }
+  c.flush(0, (float*)j.out[0]);
+}
+
+// MIDPOINT(p): src/indicators/MIDPOINT.cu:13-35: fmaxf / fminf over the
+// window of one plane, 0.5f * (max + min) from bar p-1; a window starting in
+// the row's leading NaN run stays NaN (LeadingNaN.cuh:22-28, as MIN/MAX).
+template <int K>
+__device__ __forceinline__ void midpoint_round(const Ctx<K>& c, const Job& j, Carry& cy) {
+  const int pl = j.in[0], p = j.ip[0];
+  const int f = resolve_start(c, cy, pl, j.lb_slot);
+  const int g0 = c.gb0();
+  float his[K], los[K];
+  bool fast = p - 1 >= K;
+  if (fast) {
+    const bool n1 = lane_window_ext<K, true>(c, pl, p, his);
+    const bool n2 = lane_window_ext<K, false>(c, pl, p, los);
+    fast = !n1 && !n2;
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int t = g0 + k;
+    if (!c.valid(t)) break;
+    float o = qnan();
+    if (t >= p - 1 && f >= 0 && t - p + 1 >= f) {
+      const float hi = fast ? his[k] : win_max(c, pl, t, p);
+      const float lo = fast ? los[k] : win_min(c, pl, t, p);
+      o = 0.5f * (hi + lo);
+    }
+    c.put(0, k, o);
+  }
+  cy.f = f;
   c.flush(0, (float*)j.out[0]);
 }
 

@@ -283,7 +283,8 @@ __device__ void sp_correl(SP_ARGS) {
 }
 
 // MIN / MAX with the leading-NaN window rule
-__device__ void sp_minmax(SP_ARGS, bool is_max) {
+// MIN / MAX; mid: MIDPOINT = 0.5f * (max + min) (src/indicators/MIDPOINT.cu:24-34)
+__device__ void sp_minmax(SP_ARGS, bool is_max, bool mid = false) {
   const int pl = j.in[0], p = j.ip[0];
   long long f = -1;
   for (int c = 0; c < drv.nchunks; ++c) {
@@ -294,8 +295,17 @@ __device__ void sp_minmax(SP_ARGS, bool is_max) {
       if (f < 0 && !isnan(X_pl[r])) f = t;
       float o = qnan();
       if (t >= p - 1 && f >= 0 && t - p + 1 >= f) {
-        o = X_pl[r - p + 1];
-        for (int i = 1; i < p; ++i) o = is_max ? fmaxf(o, X_pl[r - p + 1 + i]) : fminf(o, X_pl[r - p + 1 + i]);
+        if (mid) {
+          float hi = X_pl[r - p + 1], lo = hi;
+          for (int i = 1; i < p; ++i) {
+            hi = fmaxf(hi, X_pl[r - p + 1 + i]);
+            lo = fminf(lo, X_pl[r - p + 1 + i]);
+          }
+          o = 0.5f * (hi + lo);
+        } else {
+          o = X_pl[r - p + 1];
+          for (int i = 1; i < p; ++i) o = is_max ? fmaxf(o, X_pl[r - p + 1 + i]) : fminf(o, X_pl[r - p + 1 + i]);
+        }
       }
       st.put(0, lane, r, o);
     });
@@ -344,8 +354,8 @@ __device__ void sp_willr(SP_ARGS) {
   }
 }
 
-// ROC (src/indicators/ROC.cu:10-21, float arithmetic)
-__device__ void sp_roc(SP_ARGS) {
+// ROC / ROCP / ROCR / ROCR100 / MOM (roc_value in families.cuh)
+__device__ void sp_roc(SP_ARGS, int mode) {
   const int pl = j.in[0], p = j.ip[0];
   for (int c = 0; c < drv.nchunks; ++c) {
     drv.begin(c);
@@ -353,10 +363,7 @@ __device__ void sp_roc(SP_ARGS) {
     const float* X_pl = drv.pptr(c, pl);
     for_chunk(rw, [&](int r, long long t) {
       float o = qnan();
-      if (t >= p) {
-        const float prev = X_pl[r - p], curr = X_pl[r];
-        o = prev != 0.0f ? ((curr - prev) / prev) * 100.0f : 0.0f;
-      }
+      if (t >= p) o = roc_value(X_pl[r], X_pl[r - p], mode);
       st.put(0, lane, r, o);
     });
     SP_FLUSH(0);
@@ -364,18 +371,23 @@ __device__ void sp_roc(SP_ARGS) {
   }
 }
 
-// MEDPRICE / TYPPRICE (src/indicators/MedPrice.cu:12-14, TypPrice.cu:13-15)
-__device__ void sp_price(SP_ARGS, bool typ) {
-  const int ph = j.in[0], plo = j.in[1], pc = j.in[2];
+// MEDPRICE / TYPPRICE / AVGPRICE / WCLPRICE (price_round modes in families.cuh)
+__device__ void sp_price(SP_ARGS, int mode) {
   for (int c = 0; c < drv.nchunks; ++c) {
     drv.begin(c);
     const Row rw = drv.row(c);
-    const float* X_ph = drv.pptr(c, ph);
-    const float* X_plo = drv.pptr(c, plo);
-    const float* X_pc = typ ? drv.pptr(c, pc) : X_ph;
+    const float* A = drv.pptr(c, j.in[0]);
+    const float* B = drv.pptr(c, j.in[1]);
+    const float* C2 = mode >= 1 ? drv.pptr(c, j.in[2]) : A;
+    const float* D = mode == 2 ? drv.pptr(c, j.in[3]) : A;
     for_chunk(rw, [&](int r, long long) {
-      const float h = X_ph[r], l = X_plo[r];
-      st.put(0, lane, r, typ ? (h + l + X_pc[r]) / 3.0f : 0.5f * (h + l));
+      const float a = A[r], b = B[r];
+      float o;
+      if (mode == 0) o = 0.5f * (a + b);
+      else if (mode == 1) o = (a + b + C2[r]) / 3.0f;
+      else if (mode == 2) o = (a + b + C2[r] + D[r]) * 0.25f;
+      else o = (a + b + 2.0f * C2[r]) * 0.25f;
+      st.put(0, lane, r, o);
     });
     SP_FLUSH(0);
     drv.end(c);

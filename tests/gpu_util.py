@@ -46,6 +46,13 @@ SPECS = {
     "medprice": ("ct_medprice_batch_d", ["high", "low"], 1, []),
     "typprice": ("ct_typprice_batch_d", HLC, 1, []),
     "midprice": ("ct_midprice_batch_d", ["high", "low"], 1, [("i", "period")]),
+    "rocp": ("ct_rocp_batch_d", ["close"], 1, [("i", "period")]),
+    "rocr": ("ct_rocr_batch_d", ["close"], 1, [("i", "period")]),
+    "rocr100": ("ct_rocr100_batch_d", ["close"], 1, [("i", "period")]),
+    "momentum": ("ct_momentum_batch_d", ["close"], 1, [("i", "period")]),
+    "avgprice": ("ct_avgprice_batch_d", ["open", "high", "low", "close"], 1, []),
+    "wclprice": ("ct_wclprice_batch_d", HLC, 1, []),
+    "midpoint": ("ct_midpoint_batch_d", ["close"], 1, [("i", "period")]),
 }
 
 DEFAULTS = {
@@ -57,6 +64,8 @@ DEFAULTS = {
     "macd": dict(fast=12, slow=26, signal=9), "bbands": dict(period=20, up=2.0, dn=2.0), "stoch": dict(k=14, d=3),
     "obv": {}, "mfi": dict(period=14), "ad": {}, "adosc": dict(fast=3, slow=10), "correl": dict(period=30),
     "roc": dict(period=10), "rma": dict(period=14), "medprice": {}, "typprice": {}, "midprice": dict(period=14),
+    "rocp": dict(period=10), "rocr": dict(period=10), "rocr100": dict(period=10), "momentum": dict(period=10),
+    "avgprice": {}, "wclprice": {}, "midpoint": dict(period=14),
 }
 
 

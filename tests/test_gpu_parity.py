@@ -80,6 +80,8 @@ VARIANTS = {
     "roc": [dict(period=1), dict(period=2), dict(period=300)],
     "rma": [dict(period=1), dict(period=2), dict(period=60)],
     "midprice": [dict(period=1), dict(period=2), dict(period=40)],
+    "midpoint": [dict(period=1), dict(period=2), dict(period=40)],
+    "momentum": [dict(period=1), dict(period=250)],
 }
 
 
@@ -179,7 +181,8 @@ def test_leading_nan_and_interior_nan_semantics(mode):
     d = oracle_data(d)
     dp = device_planes(d)
     for name in ("ema", "rsi", "macd", "sma", "bbands", "willr", "min", "max", "dema", "roc", "rma",
-                 "medprice", "typprice", "midprice"):
+                 "medprice", "typprice", "midprice", "rocp", "rocr", "rocr100", "momentum", "avgprice",
+                 "wclprice", "midpoint"):
         got = to_np(call_batch_d(name, dp, DEFAULTS[name]))
         ref = O.run(name, d, **DEFAULTS[name])
         for i, (g, r) in enumerate(zip(got, ref)):
@@ -239,8 +242,8 @@ def test_graph_capture_replay_equals_eager(mode):
 
 
 LOOKBACK_FAMILIES = ["ema", "dema", "tema", "t3", "rsi", "macd", "atr", "natr", "adx", "dx", "obv", "ad", "adosc",
-                     "min", "max", "correl", "sma", "stoch", "mfi", "rma", "roc", "midprice"]
-SINGLE_INPUT = {"ema", "dema", "tema", "t3", "rsi", "macd", "min", "max", "sma", "rma", "roc"}
+                     "min", "max", "correl", "sma", "stoch", "mfi", "rma", "roc", "midprice", "midpoint"]
+SINGLE_INPUT = {"ema", "dema", "tema", "t3", "rsi", "macd", "min", "max", "sma", "rma", "roc", "midpoint"}
 
 
 @pytest.mark.parametrize("bars", ["4", "16"])
@@ -389,17 +392,23 @@ def test_host_entry_matches_device_entry(S, T):
 
 
 FLOAT_KERNELS = {"roc": [dict(period=1), dict(period=10), dict(period=700)], "medprice": [{}], "typprice": [{}],
-                 "midprice": [dict(period=1), dict(period=7), dict(period=100)]}
+                 "midprice": [dict(period=1), dict(period=7), dict(period=100)],
+                 "rocp": [dict(period=1), dict(period=33)], "rocr": [dict(period=2), dict(period=64)],
+                 "rocr100": [dict(period=5)], "momentum": [dict(period=1), dict(period=9)],
+                 "avgprice": [{}], "wclprice": [{}],
+                 "midpoint": [dict(period=1), dict(period=7), dict(period=100)]}
 
 
 @pytest.mark.parametrize("name", sorted(FLOAT_KERNELS))
 def test_float_kernel_families_bit_exact(name, mode):
-    """ROC, MEDPRICE, TYPPRICE and MIDPRICE repeat the reference kernels' float
-    arithmetic, so every output word equals the oracle's float result, with
-    zeros (ROC's zero divisor), NaN and infinite bars mixed in."""
+    """The ROC family, MOM, the price transforms, MIDPRICE and MIDPOINT repeat
+    the reference kernels' float arithmetic, so every output word equals the
+    oracle's float result, with zeros (the ratios' zero divisor), NaN and
+    infinite bars and a leading NaN run mixed in."""
     d = synthetic.ohlcv(9, 2500, seed=41)
     d["close"][1, ::97] = 0.0
     d["close"][2, 50:60] = np.nan
+    d["close"][6, :300] = np.nan
     d["high"][3, 400:410] = np.nan
     d["low"][4, 1000] = -np.inf
     d["high"][5, :] = np.nan  # whole windows of NaN: MIDPRICE stays NaN there
@@ -423,7 +432,9 @@ def test_rma_period_one_propagates_nan(mode):
 
 
 NEW_JOBS = [("roc", (10,), {"period": 10}), ("rma", (14,), {"period": 14}), ("medprice", (), {}),
-            ("typprice", (), {}), ("midprice", (14,), {"period": 14}), ("ema", (14,), {"period": 14})]
+            ("typprice", (), {}), ("midprice", (14,), {"period": 14}), ("ema", (14,), {"period": 14}),
+            ("rocr100", (7,), {"period": 7}), ("momentum", (3,), {"period": 3}), ("avgprice", (), {}),
+            ("wclprice", (), {}), ("midpoint", (20,), {"period": 20})]
 
 
 def test_fused_pass_with_price_transforms_roc_rma(mode):

@@ -24,6 +24,7 @@ CASES = {
     "atr": dict(period=14), "trange": {}, "stoch": dict(k=14, d=3), "obv": {}, "ad": {},
     "mfi": dict(period=14), "adosc": dict(fast=3, slow=10), "natr": dict(period=14),
     "roc": dict(period=10), "rma": dict(period=14), "medprice": {}, "typprice": {}, "midprice": dict(period=14),
+    "rocp": dict(period=10),
 }
 
 
@@ -186,3 +187,27 @@ def test_rma_is_wilder_average():
     assert got[4] == 2.0
     # fma(wBeta, 2, wAlpha * 4) with wBeta = 2/3: 8/3 up to the coefficients' rounding
     assert abs(got[5] - 8.0 / 3.0) < 1e-14
+
+
+def test_ratio_momentum_and_price_known_answers():
+    # ROCR.cu / ROCR100.cu / Momentum.cu / AvgPrice.cu / WclPrice.cu / MIDPOINT.cu
+    f = np.float32
+    x = np.array([[np.nan, 0.0, 4.0, 3.0, 6.0, 1.5]], np.float32)
+    assert np.isnan(O.run("rocr", {"close": x}, period=1)[0][0, :2]).all()
+    np.testing.assert_array_equal(O.run("rocr", {"close": x}, period=1)[0][0, 2:], [0.0, f(3.0) / f(4.0), 2.0, 0.25])
+    np.testing.assert_array_equal(O.run("rocr100", {"close": x}, period=2)[0][0, 3:],
+                                  [0.0, f(f(6.0) / f(4.0)) * f(100.0), f(f(1.5) / f(3.0)) * f(100.0)])
+    mom = O.run("momentum", {"close": x}, period=2)[0][0]
+    assert np.isnan(mom[:3]).all() and (mom[3:] == [3.0, 2.0, -1.5]).all()
+    o = np.array([[1.0, 2.0]], np.float32)
+    h = np.array([[4.0, 3.0]], np.float32)
+    l = np.array([[0.5, 1.0]], np.float32)
+    c = np.array([[2.5, 2.0]], np.float32)
+    np.testing.assert_array_equal(O.run("avgprice", {"open": o, "high": h, "low": l, "close": c})[0][0], [2.0, 2.0])
+    np.testing.assert_array_equal(O.run("wclprice", {"high": h, "low": l, "close": c})[0][0],
+                                  [f(f(4.5) + f(5.0)) * f(0.25), 2.0])
+    # MIDPOINT: leading NaN windows stay NaN, interior NaN is skipped by fmaxf/fminf
+    y = np.array([[np.nan, np.nan, 1.0, 5.0, np.nan, 3.0]], np.float32)
+    mp = O.run("midpoint", {"close": y}, period=2)[0][0]
+    assert np.isnan(mp[:3]).all()
+    np.testing.assert_array_equal(mp[3:], [3.0, 5.0, 3.0])
