@@ -9,9 +9,11 @@
 // Outputs are staged per warp and written back with coalesced stores, so each
 // input byte is read from HBM once per launch and each output byte written once.
 //
-// This file is compiled twice: normally (FP64 engines, candles, entry-side
-// launch logic) and with TB_PREC_TU defined, which builds only the kernels of
-// the precision variants (launch_prec), so the two halves compile in parallel.
+// This file is compiled twice: normally (FP64 engines for the families up to
+// CDL, candles, entry-side launch logic) and with TB_PREC_TU defined, which
+// builds the kernels of the precision variants (launch_prec) and the FP64
+// kernels that also hold the families appended after CDL (launch_ext), so the
+// two halves compile in parallel and the common job sets keep lean kernels.
 #include "engine.h"
 #include "pool.h"
 #include "families.cuh"
@@ -62,11 +64,36 @@ __device__ __forceinline__ bool run_job_prec(const Ctx<K>& c, const Job& j, Carr
   }
 }
 
+// Families appended after CDL (ROC ... MIDPOINT): compiled only into the P = 4
+// kernels, so the kernels of the other job sets keep their code size and
+// register allocation.
+template <int K>
+__device__ __forceinline__ void run_job_ext(const Ctx<K>& c, const Job& j, Carry& cy) {
+  switch (j.family) {
+    case F_ROC: roc_round(c, j, 0); break;
+    case F_ROCP: roc_round(c, j, 1); break;
+    case F_ROCR: roc_round(c, j, 2); break;
+    case F_ROCR100: roc_round(c, j, 3); break;
+    case F_MOM: roc_round(c, j, 4); break;
+    case F_RMA: ema_round(c, j, cy); break;
+    case F_MEDPRICE: price_round(c, j, 0); break;
+    case F_TYPPRICE: price_round(c, j, 1); break;
+    case F_AVGPRICE: price_round(c, j, 2); break;
+    case F_WCLPRICE: price_round(c, j, 3); break;
+    case F_MIDPRICE: midprice_round(c, j); break;
+    case F_MIDPOINT: midpoint_round(c, j, cy); break;
+    default: break;
+  }
+}
+
+// P = 0: FP64 families up to CDL; P = 1..3: precision variants (a precision
+// launch holds only the families that have them, which the host validates);
+// P = 4: FP64, all families.
 template <int K, int P>
 __device__ __forceinline__ void run_job(const Ctx<K>& c, const Job& j, Carry& cy) {
-  if constexpr (P != 0) {
-    if (run_job_prec<K, P>(c, j, cy)) return;
-  }
+  if constexpr (P >= 1 && P <= 3) {
+    run_job_prec<K, P>(c, j, cy);
+  } else {
   switch (j.family) {
     case F_SMA: sum_window_round(c, j, 0); break;
     case F_SUM: sum_window_round(c, j, 1); break;
@@ -96,19 +123,10 @@ __device__ __forceinline__ void run_job(const Ctx<K>& c, const Job& j, Carry& cy
     case F_CCI: cci_round(c, j); break;
     case F_MFI: mfi_round(c, j); break;
     case F_CORREL: correl_round(c, j, cy); break;
-    case F_ROC: roc_round(c, j, 0); break;
-    case F_ROCP: roc_round(c, j, 1); break;
-    case F_ROCR: roc_round(c, j, 2); break;
-    case F_ROCR100: roc_round(c, j, 3); break;
-    case F_MOM: roc_round(c, j, 4); break;
-    case F_RMA: ema_round(c, j, cy); break;
-    case F_MEDPRICE: price_round(c, j, 0); break;
-    case F_TYPPRICE: price_round(c, j, 1); break;
-    case F_AVGPRICE: price_round(c, j, 2); break;
-    case F_WCLPRICE: price_round(c, j, 3); break;
-    case F_MIDPRICE: midprice_round(c, j); break;
-    case F_MIDPOINT: midpoint_round(c, j, cy); break;
-    default: break;
+    default:
+      if constexpr (P == 4) run_job_ext<K>(c, j, cy);
+      break;
+  }
   }
 }
 
@@ -515,7 +533,7 @@ struct OccEntry { int k, warps, smem, per_sm; };
 struct DeviceInfo {
   int sms = 0;
   int smem_optin = 0;
-  bool attr_set[3][4] = {};
+  bool attr_set[3][5] = {};
   bool sp_attr = false;
   int cdl_per_sm = 0;
   std::vector<OccEntry> occ;
@@ -786,9 +804,38 @@ cudaError_t launch_prec(Launch& L, const SchedulePlan& plan, long long total_bar
     default: return cudaErrorInvalidValue;
   }
 }
+
+// Job sets with a family appended after CDL: the P = 4 kernels.
+cudaError_t launch_ext_k(int k, Launch& L, const SchedulePlan& plan, cudaStream_t stream, LaunchStats* stats) {
+  switch (k) {
+    case 4: return launch_k<4, 4>(L, plan, stream, stats);
+    case 16: return launch_k<16, 4>(L, plan, stream, stats);
+    default: return launch_k<8, 4>(L, plan, stream, stats);
+  }
+}
+cudaError_t launch_ext(Launch& L, const SchedulePlan& plan, long long total_bars, cudaStream_t stream,
+                       LaunchStats* stats) {
+  if (plan.mode == 2) {
+    switch (plan.k) {
+      case 4: return launch_lookback<4, 4>(L, plan, total_bars, stream, stats);
+      case 16: return launch_lookback<16, 4>(L, plan, total_bars, stream, stats);
+      default: return launch_lookback<8, 4>(L, plan, total_bars, stream, stats);
+    }
+  }
+  return launch_ext_k(plan.k, L, plan, stream, stats);
+}
 #else
 cudaError_t launch_prec(Launch& L, const SchedulePlan& plan, long long total_bars, cudaStream_t stream,
                         LaunchStats* stats);
+cudaError_t launch_ext_k(int k, Launch& L, const SchedulePlan& plan, cudaStream_t stream, LaunchStats* stats);
+cudaError_t launch_ext(Launch& L, const SchedulePlan& plan, long long total_bars, cudaStream_t stream,
+                       LaunchStats* stats);
+
+bool has_ext_family(const Launch& L) {
+  for (int j = 0; j < L.njobs; ++j)
+    if (L.jobs[j].family > F_CDL) return true;
+  return false;
+}
 
 // Look-back scratch of the allocation-free entry point: a file-scope device
 // array (one copy per device, created when the module loads there). Its
@@ -843,7 +890,7 @@ cudaError_t launch_lookback_static_k(Launch& L, const SchedulePlan& plan, cudaSt
   L.lb_desc = reinterpret_cast<LbDesc*>(scratch + head);
   L.lb_nslots = nslots;
   L.lb_tiles = ntiles;
-  e = launch_k<K>(L, plan, stream, nullptr);
+  e = has_ext_family(L) ? launch_ext_k(K, L, plan, stream, nullptr) : launch_k<K>(L, plan, stream, nullptr);
   if (e == cudaSuccess && stream == 0) {
     int herr = 0;
     e = cudaMemcpyAsync(&herr, L.err, sizeof(int), cudaMemcpyDeviceToHost, stream);
@@ -903,6 +950,7 @@ cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, long long total_ba
   }
   L.lb = 0;
   if (L.njobs > 0 && L.jobs[0].prec != 0) return launch_prec(L, plan, total_bars, stream, stats);
+  if (has_ext_family(L)) return launch_ext(L, plan, total_bars, stream, stats);
   if (plan.mode == 2) {
     switch (plan.k) {
       case 4: return launch_lookback<4, 0>(L, plan, total_bars, stream, stats);
