@@ -62,6 +62,11 @@ FAMILIES = {
     "avgprice": (37, ("open", "high", "low", "close"), ("out",), (), ()),
     "wclprice": (38, ("high", "low", "close"), ("out",), (), ()),
     "midpoint": (39, ("close",), ("out",), ("period",), ()),
+    "change": (36, ("close",), ("out",), ("period",), ()),  # src/indicators/Change.cu: MOM's arithmetic
+    "rolling_mean": (40, ("close",), ("out",), ("period",), ()),
+    "rolling_max": (41, ("close",), ("out",), ("period",), ()),
+    "rolling_min": (42, ("close",), ("out",), ("period",), ()),
+    "rolling_std": (43, ("close",), ("out",), ("period",), ()),
 }
 
 _P = ct.c_void_p

@@ -785,6 +785,40 @@ static void row_midpoint(RowCtx* r) {
   }
 }
 
+/* src/indicators/ClubPack.cu:375-407 rollingStrictKernel: NaN-strict windows
+ * (any non-finite bar gives NaN), FP64 sums from the newest bar back; mode 0
+ * mean, 1 max, 2 min, 3 population std sqrt(max(0, sq/p - mean^2)) with the
+ * fma that nvcc's default contraction forms for sq/p - mean*mean. */
+static void rolling_row(RowCtx* r, int mode) {
+  const float* x = r->in[0]; int n = r->n, p = r->ip[0]; double* o = r->out[0];
+  fill_nan(o, n);
+  for (int t = p - 1; t < n; ++t) {
+    int ok = 1;
+    double sum = 0.0, sq = 0.0;
+    float mx = x[t], mn = x[t];
+    for (int k = 0; k < p; ++k) {
+      const float v = x[t - k];
+      if (!isfinite(v)) { ok = 0; break; }
+      sum += v;
+      sq = fma((double)v, (double)v, sq);
+      mx = fmaxf(mx, v);
+      mn = fminf(mn, v);
+    }
+    if (!ok) continue;
+    if (mode == 0) o[t] = (double)(float)(sum / p);
+    else if (mode == 1) o[t] = mx;
+    else if (mode == 2) o[t] = mn;
+    else {
+      const double mean = sum / p;
+      o[t] = (double)(float)sqrt(fmax(0.0, fma(-mean, mean, sq / p)));
+    }
+  }
+}
+static void row_rmean(RowCtx* r) { rolling_row(r, 0); }
+static void row_rmax(RowCtx* r) { rolling_row(r, 1); }
+static void row_rmin(RowCtx* r) { rolling_row(r, 2); }
+static void row_rstd(RowCtx* r) { rolling_row(r, 3); }
+
 /* src/indicators/MIDPRICE.cu:11-24: fmaxf / fminf over [t-p+1, t] (NaN
  * ignored unless the whole window is NaN), 0.5f * (max + min), from bar p-1. */
 static void row_midprice(RowCtx* r) {
@@ -826,6 +860,8 @@ static const FamSpec kFam[ORC_FAMILY_COUNT] = {
   [ORC_ROCR100] = {1, 1, 1, 0, row_rocr100, 1}, [ORC_MOM] = {1, 1, 1, 0, row_mom, 1},
   [ORC_AVGPRICE] = {4, 1, 0, 0, row_avgprice, 0}, [ORC_WCLPRICE] = {3, 1, 0, 0, row_wclprice, 0},
   [ORC_MIDPOINT] = {1, 1, 1, 0, row_midpoint, 1},
+  [ORC_RMEAN] = {1, 1, 1, 0, row_rmean, 1},  [ORC_RMAX] = {1, 1, 1, 0, row_rmax, 1},
+  [ORC_RMIN] = {1, 1, 1, 0, row_rmin, 1},    [ORC_RSTD] = {1, 1, 1, 0, row_rstd, 1},
 };
 
 static int check_params(int family, const int* ip) {

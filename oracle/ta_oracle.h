@@ -18,7 +18,7 @@
  * MEDPRICE TYPPRICE MIDPRICE are pinned against the vendored TA-Lib functions
  * of the same names within the float tolerance; ROCR ROCR100 MOM AVGPRICE
  * WCLPRICE MIDPOINT are not in the vendored set and are pinned by known
- * answers only. ADX DX CCI WILLR CORREL SUM MIN MAX have no CPU code in
+ * answers only, as are the NaN-strict rolling statistics (ClubPack.cu). ADX DX CCI WILLR CORREL SUM MIN MAX have no CPU code in
  * the reference: they are pinned by known-answer tests only ("parity partially
  * unpinned").
  */
@@ -34,7 +34,8 @@ enum OracleFamily {
   ORC_MFI, ORC_WILLR, ORC_SUM, ORC_MIN, ORC_MAX, ORC_STDDEV, ORC_VAR, ORC_LINEARREG,
   ORC_CORREL, ORC_DEMA, ORC_TEMA, ORC_T3, ORC_ROC, ORC_RMA, ORC_MEDPRICE,
   ORC_TYPPRICE, ORC_MIDPRICE, ORC_ROCP, ORC_ROCR, ORC_ROCR100, ORC_MOM,
-  ORC_AVGPRICE, ORC_WCLPRICE, ORC_MIDPOINT, ORC_FAMILY_COUNT
+  ORC_AVGPRICE, ORC_WCLPRICE, ORC_MIDPOINT, ORC_RMEAN, ORC_RMAX, ORC_RMIN,
+  ORC_RSTD, ORC_FAMILY_COUNT
 };
 
 /* ins: the family's input planes (see oracle/oracle.py INPUTS); outs: its output

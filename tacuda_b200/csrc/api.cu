@@ -102,7 +102,7 @@ ctStatus_t make_job(const ctB200Job& u, Job& j, const char* who) {
     case tb::F_SMA: case tb::F_SUM: case tb::F_WMA: case tb::F_BBANDS: case tb::F_STDDEV: case tb::F_VAR:
     case tb::F_LINEARREG: case tb::F_MIN: case tb::F_MAX: case tb::F_WILLR: case tb::F_CCI: case tb::F_MFI:
     case tb::F_CORREL: case tb::F_ROC: case tb::F_MIDPRICE: case tb::F_ROCP: case tb::F_ROCR: case tb::F_ROCR100:
-    case tb::F_MOM: case tb::F_MIDPOINT:
+    case tb::F_MOM: case tb::F_MIDPOINT: case tb::F_RMEAN: case tb::F_RMAX: case tb::F_RMIN: case tb::F_RSTD:
       if (u.params[0] > kMaxWindow) return fail(CT_STATUS_UNSUPPORTED, std::string(who) + ": window period above 4096");
       break;
     case tb::F_STOCH:
@@ -353,7 +353,39 @@ TB_S1(rocr, tb::F_ROCR)  // tacuda.h:1026, tacuda_device.h:180
 TB_S1(rocr100, tb::F_ROCR100)  // tacuda.h:1036, tacuda_device.h:183
 TB_S1(momentum, tb::F_MOM)  // tacuda.h:997, tacuda_device.h:171
 TB_S1(midpoint, tb::F_MIDPOINT)  // tacuda.h:1516, tacuda_device.h:447
+TB_S1(change, tb::F_MOM)  // tacuda.h:1506, tacuda_device.h:444; src/indicators/Change.cu is MOM's arithmetic
 #undef TB_S1
+
+// NaN-strict rolling statistics: a period above the row length is an invalid
+// argument (src/indicators/ClubPack.cu:409-413 check_period).
+#define TB_ROLL(NAME, FAM)                                                                            \
+  ctStatus_t ct_##NAME##_batch_d(const float* d_inputs, float* d_outputs, int seriesLen, int numSeries, \
+                                 int period, int, cudaStream_t stream) {                              \
+    if (period > seriesLen && seriesLen > 0) {                                                        \
+      clear_error();                                                                                  \
+      return fail(CT_STATUS_INVALID_ARGUMENT, "ct_" #NAME "_batch_d: invalid period");              \
+    }                                                                                                 \
+    ctB200Job u = job_of(FAM, period);                                                                \
+    u.outputs[0] = d_outputs;                                                                         \
+    const Planes P = close_only(d_inputs);                                                            \
+    return run_single(P.p, u, seriesLen, numSeries, stream, "ct_" #NAME "_batch_d");                  \
+  }                                                                                                   \
+  ctStatus_t ct_##NAME##_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream) { \
+    if (period > size && size > 0 && d_input && d_output) {                                           \
+      clear_error();                                                                                  \
+      return fail(CT_STATUS_INVALID_ARGUMENT, "ct_" #NAME "_d: invalid period");                    \
+    }                                                                                                 \
+    ctB200Job u = job_of(FAM, period);                                                                \
+    u.outputs[0] = d_output;                                                                          \
+    const Planes P = close_only(d_input);                                                             \
+    return run_single(P.p, u, size, 1, stream, "ct_" #NAME "_d");                                     \
+  }
+
+TB_ROLL(rolling_mean, tb::F_RMEAN)  // tacuda.h:3157, tacuda_device.h:981
+TB_ROLL(rolling_max, tb::F_RMAX)    // tacuda.h:3171, tacuda_device.h:985
+TB_ROLL(rolling_min, tb::F_RMIN)    // tacuda.h:3185, tacuda_device.h:988
+TB_ROLL(rolling_std, tb::F_RSTD)    // tacuda.h:3199, tacuda_device.h:991
+#undef TB_ROLL
 
 #define TB_HLC(NAME, FAM)                                                                                  \
   ctStatus_t ct_##NAME##_batch_d(const float* d_highs, const float* d_lows, const float* d_closes,         \

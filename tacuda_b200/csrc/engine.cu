@@ -82,6 +82,10 @@ __device__ __forceinline__ void run_job_ext(const Ctx<K>& c, const Job& j, Carry
     case F_WCLPRICE: price_round(c, j, 3); break;
     case F_MIDPRICE: midprice_round(c, j); break;
     case F_MIDPOINT: midpoint_round(c, j, cy); break;
+    case F_RMEAN: rolling_round(c, j, 0); break;
+    case F_RMAX: rolling_round(c, j, 1); break;
+    case F_RMIN: rolling_round(c, j, 2); break;
+    case F_RSTD: rolling_round(c, j, 3); break;
     default: break;
   }
 }
@@ -340,6 +344,10 @@ __device__ void sp_run_job(sp::Driver& drv, const Job& j, const sp::Stage& st, c
     case F_WCLPRICE: sp::sp_price(drv, j, st, ln, lane, 3); break;
     case F_MIDPRICE: sp::sp_midprice(drv, j, st, ln, lane); break;
     case F_MIDPOINT: sp::sp_minmax(drv, j, st, ln, lane, false, true); break;
+    case F_RMEAN: sp::sp_rolling(drv, j, st, ln, lane, 0); break;
+    case F_RMAX: sp::sp_rolling(drv, j, st, ln, lane, 1); break;
+    case F_RMIN: sp::sp_rolling(drv, j, st, ln, lane, 2); break;
+    case F_RSTD: sp::sp_rolling(drv, j, st, ln, lane, 3); break;
     default:
       for (int c = 0; c < drv.nchunks; ++c) { drv.begin(c); drv.end(c); }
   }
@@ -458,7 +466,7 @@ int job_halo(const Job& j) {
     case F_LINEARREG: case F_MIN: case F_MAX: case F_WILLR: case F_CCI: case F_CORREL:
       return j.ip[0] - 1;
     case F_MFI: case F_ROC: case F_ROCP: case F_ROCR: case F_ROCR100: case F_MOM: return j.ip[0];
-    case F_MIDPOINT: return j.ip[0] - 1;
+    case F_MIDPOINT: case F_RMEAN: case F_RMAX: case F_RMIN: case F_RSTD: return j.ip[0] - 1;
     case F_MIDPRICE: return j.ip[0] - 1;
     case F_STOCH: return j.ip[0] - 1 + 2 * (j.ip[1] - 1);
     case F_CDL: return 16;  // 10-bar averages anchored up to 5 bars back
@@ -473,7 +481,7 @@ unsigned job_planes(const Job& j) {
     case F_SMA: case F_EMA: case F_WMA: case F_RSI: case F_MACD: case F_BBANDS: case F_SUM:
     case F_MIN: case F_MAX: case F_STDDEV: case F_VAR: case F_LINEARREG: case F_DEMA:
     case F_TEMA: case F_T3: case F_ROC: case F_RMA: case F_ROCP: case F_ROCR: case F_ROCR100:
-    case F_MOM: case F_MIDPOINT:
+    case F_MOM: case F_MIDPOINT: case F_RMEAN: case F_RMAX: case F_RMIN: case F_RSTD:
       n = 1; break;
     case F_OBV: case F_CORREL: case F_MEDPRICE: case F_MIDPRICE: n = 2; break;
     case F_ATR: case F_NATR: case F_TRANGE: case F_ADX: case F_DX: case F_STOCH: case F_WILLR:

@@ -1091,6 +1091,48 @@ __device__ __forceinline__ void midpoint_round(const Ctx<K>& c, const Job& j, Ca
   c.flush(0, (float*)j.out[0]);
 }
 
+// NaN-strict rolling statistics (src/indicators/ClubPack.cu:375-407): a window
+// holding a NaN or an infinity gives NaN; otherwise FP64 sums accumulated from
+// the newest bar back, in the reference's order. mode 0 mean (sum / p), 1 max,
+// 2 min (fmaxf / fminf), 3 population standard deviation
+// sqrt(max(0, sq/p - mean^2)). The reference file is compiled with FMA
+// contraction on, which fuses sq/p - mean*mean into one fma; this library is
+// built without contraction, so the fma is written out.
+template <int K>
+__device__ __forceinline__ void rolling_round(const Ctx<K>& c, const Job& j, int mode) {
+  const int pl = j.in[0], p = j.ip[0];
+  const int g0 = c.gb0();
+  for (int k = 0; k < K; ++k) {
+    const int t = g0 + k;
+    if (!c.valid(t)) break;
+    float o = qnan();
+    if (t >= p - 1) {
+      bool ok = true;
+      double sum = 0.0, sq = 0.0;
+      float mx = c.x(pl, t), mn = mx;
+      for (int i = 0; i < p; ++i) {
+        const float v = c.x(pl, t - i);
+        if (!isfinite(v)) { ok = false; break; }
+        sum += v;
+        sq = fma((double)v, (double)v, sq);
+        mx = fmaxf(mx, v);
+        mn = fminf(mn, v);
+      }
+      if (ok) {
+        if (mode == 0) o = (float)(sum / p);
+        else if (mode == 1) o = mx;
+        else if (mode == 2) o = mn;
+        else {
+          const double mean = sum / p;
+          o = (float)sqrt(fmax(0.0, fma(-mean, mean, sq / p)));
+        }
+      }
+    }
+    c.put(0, k, o);
+  }
+  c.flush(0, (float*)j.out[0]);
+}
+
 // WILLR(p): src/indicators/WILLR.cu:11-30: float window extrema (strict
 // comparisons seeded with the current bar), ((HH - C)/(HH - LL)) * -100 in
 // FP64, clamped to [-100, 0]; 0 for a zero range.

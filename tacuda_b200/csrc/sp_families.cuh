@@ -419,6 +419,44 @@ __device__ void sp_midprice(SP_ARGS) {
   }
 }
 
+// NaN-strict rolling mean / max / min / std (rolling_round in families.cuh)
+__device__ void sp_rolling(SP_ARGS, int mode) {
+  const int pl = j.in[0], p = j.ip[0];
+  for (int c = 0; c < drv.nchunks; ++c) {
+    drv.begin(c);
+    const Row rw = drv.row(c);
+    const float* X_pl = drv.pptr(c, pl);
+    for_chunk(rw, [&](int r, long long t) {
+      float o = qnan();
+      if (t >= p - 1) {
+        bool ok = true;
+        double sum = 0.0, sq = 0.0;
+        float mx = X_pl[r], mn = mx;
+        for (int i = 0; i < p; ++i) {
+          const float v = X_pl[r - i];
+          if (!isfinite(v)) { ok = false; break; }
+          sum += v;
+          sq = fma((double)v, (double)v, sq);
+          mx = fmaxf(mx, v);
+          mn = fminf(mn, v);
+        }
+        if (ok) {
+          if (mode == 0) o = (float)(sum / p);
+          else if (mode == 1) o = mx;
+          else if (mode == 2) o = mn;
+          else {
+            const double mean = sum / p;
+            o = (float)sqrt(fmax(0.0, fma(-mean, mean, sq / p)));
+          }
+        }
+      }
+      st.put(0, lane, r, o);
+    });
+    SP_FLUSH(0);
+    drv.end(c);
+  }
+}
+
 // STOCH (talib08:16115-16302): fastK into the warp line for the chunk and the
 // 2(d-1) bars before it, then slowK / slowD as direct means.
 __device__ void sp_stoch(SP_ARGS) {

@@ -53,6 +53,11 @@ SPECS = {
     "avgprice": ("ct_avgprice_batch_d", ["open", "high", "low", "close"], 1, []),
     "wclprice": ("ct_wclprice_batch_d", HLC, 1, []),
     "midpoint": ("ct_midpoint_batch_d", ["close"], 1, [("i", "period")]),
+    "change": ("ct_change_batch_d", ["close"], 1, [("i", "period")]),
+    "rolling_mean": ("ct_rolling_mean_batch_d", ["close"], 1, [("i", "period")]),
+    "rolling_max": ("ct_rolling_max_batch_d", ["close"], 1, [("i", "period")]),
+    "rolling_min": ("ct_rolling_min_batch_d", ["close"], 1, [("i", "period")]),
+    "rolling_std": ("ct_rolling_std_batch_d", ["close"], 1, [("i", "period")]),
 }
 
 DEFAULTS = {
@@ -65,7 +70,9 @@ DEFAULTS = {
     "obv": {}, "mfi": dict(period=14), "ad": {}, "adosc": dict(fast=3, slow=10), "correl": dict(period=30),
     "roc": dict(period=10), "rma": dict(period=14), "medprice": {}, "typprice": {}, "midprice": dict(period=14),
     "rocp": dict(period=10), "rocr": dict(period=10), "rocr100": dict(period=10), "momentum": dict(period=10),
-    "avgprice": {}, "wclprice": {}, "midpoint": dict(period=14),
+    "avgprice": {}, "wclprice": {}, "midpoint": dict(period=14), "change": dict(period=10),
+    "rolling_mean": dict(period=20), "rolling_max": dict(period=20), "rolling_min": dict(period=20),
+    "rolling_std": dict(period=20),
 }
 
 

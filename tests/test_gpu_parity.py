@@ -29,6 +29,11 @@ def oracle_data(d):
 
 def run_case(name, params, shape, seed=6):
     d = oracle_data(synthetic.ohlcv(*shape, seed=seed))
+    if name.startswith("rolling_") and params["period"] > shape[1]:
+        # ClubPack.cu:409-413: a rolling period above the row length is an invalid argument
+        with pytest.raises(RuntimeError, match="code 4"):
+            call_batch_d(name, device_planes(d), params)
+        return []
     got = to_np(call_batch_d(name, device_planes(d), params))
     ref = O.run(name, d, **params)
     stats = []
@@ -396,7 +401,9 @@ FLOAT_KERNELS = {"roc": [dict(period=1), dict(period=10), dict(period=700)], "me
                  "rocp": [dict(period=1), dict(period=33)], "rocr": [dict(period=2), dict(period=64)],
                  "rocr100": [dict(period=5)], "momentum": [dict(period=1), dict(period=9)],
                  "avgprice": [{}], "wclprice": [{}],
-                 "midpoint": [dict(period=1), dict(period=7), dict(period=100)]}
+                 "midpoint": [dict(period=1), dict(period=7), dict(period=100)], "change": [dict(period=4)],
+                 "rolling_mean": [dict(period=1), dict(period=30)], "rolling_max": [dict(period=7)],
+                 "rolling_min": [dict(period=200)], "rolling_std": [dict(period=1), dict(period=25)]}
 
 
 @pytest.mark.parametrize("name", sorted(FLOAT_KERNELS))
@@ -409,6 +416,7 @@ def test_float_kernel_families_bit_exact(name, mode):
     d["close"][1, ::97] = 0.0
     d["close"][2, 50:60] = np.nan
     d["close"][6, :300] = np.nan
+    d["close"][7, 1500] = np.inf  # the rolling statistics are NaN wherever a window holds it
     d["high"][3, 400:410] = np.nan
     d["low"][4, 1000] = -np.inf
     d["high"][5, :] = np.nan  # whole windows of NaN: MIDPRICE stays NaN there
@@ -434,7 +442,8 @@ def test_rma_period_one_propagates_nan(mode):
 NEW_JOBS = [("roc", (10,), {"period": 10}), ("rma", (14,), {"period": 14}), ("medprice", (), {}),
             ("typprice", (), {}), ("midprice", (14,), {"period": 14}), ("ema", (14,), {"period": 14}),
             ("rocr100", (7,), {"period": 7}), ("momentum", (3,), {"period": 3}), ("avgprice", (), {}),
-            ("wclprice", (), {}), ("midpoint", (20,), {"period": 20})]
+            ("wclprice", (), {}), ("midpoint", (20,), {"period": 20}), ("rolling_std", (15,), {"period": 15}),
+            ("rolling_max", (9,), {"period": 9})]
 
 
 def test_fused_pass_with_price_transforms_roc_rma(mode):

@@ -211,3 +211,16 @@ def test_ratio_momentum_and_price_known_answers():
     mp = O.run("midpoint", {"close": y}, period=2)[0][0]
     assert np.isnan(mp[:3]).all()
     np.testing.assert_array_equal(mp[3:], [3.0, 5.0, 3.0])
+
+
+def test_rolling_strict_known_answers():
+    # ClubPack.cu:375-407: any non-finite bar in the window gives NaN
+    x = np.array([[1.0, 2.0, np.inf, 4.0, 5.0, 6.0]], np.float32)
+    mean = O.run("rolling_mean", {"close": x}, period=2)[0][0]
+    assert np.isnan(mean[[0, 2, 3]]).all()
+    np.testing.assert_array_equal(mean[[1, 4, 5]], [1.5, 4.5, 5.5])
+    np.testing.assert_array_equal(O.run("rolling_max", {"close": x}, period=2)[0][0, 4:], [5.0, 6.0])
+    np.testing.assert_array_equal(O.run("rolling_min", {"close": x}, period=2)[0][0, 4:], [4.0, 5.0])
+    std = O.run("rolling_std", {"close": x}, period=2)[0][0]
+    np.testing.assert_array_equal(std[[1, 4, 5]], [0.5, 0.5, 0.5])
+    np.testing.assert_array_equal(O.run("change", {"close": x}, period=1)[0][0, 4:], [1.0, 1.0])
