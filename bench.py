@@ -63,16 +63,19 @@ class ClockSampler:
         self._stop = threading.Event()
         self._t = None
 
+    def _sample(self):
+        try:
+            out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                  "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+            line = out.stdout.strip().splitlines()[0] if out.stdout.strip() else ""
+            if line:
+                self.samples.append([x.strip() for x in line.split(",")])
+        except Exception:
+            pass
+
     def _run(self):
         while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                line = out.stdout.strip().splitlines()[0] if out.stdout.strip() else ""
-                if line:
-                    self.samples.append([x.strip() for x in line.split(",")])
-            except Exception:
-                pass
+            self._sample()
             self._stop.wait(0.1)
 
     def __enter__(self):
@@ -84,6 +87,9 @@ class ClockSampler:
         self._stop.set()
         if self._t:
             self._t.join(timeout=10)
+        # one more sample right at the end of the region (a region of a few
+        # milliseconds is shorter than one nvidia-smi query)
+        self._sample()
 
     def summary(self):
         if not self.samples:
@@ -255,7 +261,7 @@ def _event_ms(fn, reps, warm=2, stream=None):
 
 def run_extras(dev, peak):
     """The other measured workloads, each timed with CUDA events (inputs larger
-    than L2 where the workload is; config 1 is latency-bound and L2-resident)."""
+    than L2 where the workload is; the single 100,000-bar series is latency-bound and L2-resident)."""
     import torch
     import tacuda_b200 as tb
     from tacuda_b200 import synthetic, workloads
@@ -263,7 +269,7 @@ def run_extras(dev, peak):
     out = {}
     torch.cuda.synchronize()
 
-    # config 1: one 100,000-bar close series, SMA20 EMA30 RSI14 MACD12/26/9
+    # one 100,000-bar close series, SMA20 EMA30 RSI14 MACD12/26/9
     x = torch.from_numpy(synthetic.single_close(100_000, seed=11).astype(np.float32)).to(dev).reshape(1, -1)
     o1 = {n: torch.empty_like(x) for n in ("sma", "ema", "rsi", "macd", "sig", "hist")}
     j1 = [tb.make_job("sma", (20,), (), [o1["sma"].data_ptr()]), tb.make_job("ema", (30,), (), [o1["ema"].data_ptr()]),
@@ -273,13 +279,13 @@ def run_extras(dev, peak):
     st = torch.cuda.current_stream().cuda_stream
     f_ms = _event_ms(lambda: tb.fused_batch_d(s1, j1, st), 20)
     p_ms = _event_ms(lambda: [tb.fused_batch_d(s1, [j], st) for j in j1], 20)
-    out["config1_single_100k"] = {"workload": "1 series x 100,000 bars: SMA20 EMA30 RSI14 MACD12/26/9 (6 outputs)",
+    out["single_series_100k"] = {"workload": "1 series x 100,000 bars: SMA20 EMA30 RSI14 MACD12/26/9 (6 outputs)",
                                   "fused_us": f_ms * 1e3, "plain_us": p_ms * 1e3,
                                   "value": 4 * 100_000 / (f_ms * 1e-3), "unit": "indicator-bars/s",
                                   "bound": "latency"}
     del x, o1
 
-    # config 3: 10,000 ragged series (log-uniform 50..20,000 bars), 13-pass + 61 CDL int32
+    # 10,000 ragged series (log-uniform 50..20,000 bars), 13-pass + 61 CDL int32
     lengths = synthetic.ragged_lengths(10_000, 50, 20_000, seed=7)
     planes, off = synthetic.ragged_ohlcv(lengths, seed=4)
     N = int(off[-1])
@@ -299,7 +305,7 @@ def run_extras(dev, peak):
     ncdl = bin(mask).count("1")
     bytes3 = N * (20 + 4 * len(workloads.PASS13_OUTPUTS) + 4 * ncdl)
     gbs = bytes3 / (fused * 1e-3) / 1e9
-    out["config3_ragged_13_plus_cdl61"] = {
+    out["ragged_10k_13pass_cdl61"] = {
         "workload": f"10,000 ragged series (sum {N} bars), 13-indicator pass + 61 CDL int32, one plan (2 launches)",
         "ms": fused, "plain_ms": plain, "fused_speedup": plain / fused,
         "value": (13 + ncdl) * N / (fused * 1e-3), "unit": "indicator-bars/s",
@@ -311,7 +317,7 @@ def run_extras(dev, peak):
     plan.close()
     del dp, doff, outs, cdl
 
-    # config 4: per-series alpha EMA/MACD/RSI, forward and adjoint, 4096 x 2048
+    # per-series alpha EMA/MACD/RSI, forward and adjoint, 4096 x 2048
     rng = np.random.default_rng(4)
     c4 = torch.from_numpy(synthetic.ohlcv(4096, 2048, seed=4)["close"]).to(dev)
     a4 = torch.from_numpy(rng.uniform(0.01, 0.5, 4096).astype(np.float32)).to(dev)
@@ -320,7 +326,7 @@ def run_extras(dev, peak):
     fwd = _event_ms(lambda: TA.alpha_forward(c4, a4), 5)
     bwd = _event_ms(lambda: TA.alpha_backward(c4, a4, ck, w4), 5)
     n4 = 4096 * 2048
-    out["config4_alpha_adjoint"] = {
+    out["alpha_adjoint_4096x2048"] = {
         "workload": "4096 series x 2048 bars, EMA14 MACD12/26/9 RSI14 with per-series alpha; adjoint of a "
                     "N(0,1)-weighted sum of the 5 outputs; checkpoints every 256 bars",
         "forward_ms": fwd, "adjoint_ms": bwd, "adjoint_over_forward": bwd / fwd,
@@ -360,7 +366,7 @@ def run_extras(dev, peak):
         "ema14_ms_per_append": ema_ms, "macd_ms_per_append": macd_ms,
         "ema14_bars_per_s": Ss * n / (ema_ms * 1e-3), "macd_bars_per_s": Ss * n / (macd_ms * 1e-3)}
 
-    # config 5: 4 series x 50,000,000 bars with a +1e4 level, look-back across tiles
+    # 4 series x 50,000,000 bars with a +1e4 level, look-back across tiles
     T5 = 50_000_000
     x5 = torch.from_numpy(synthetic.level_walk(4, T5, seed=5)).to(dev)
     y5 = torch.from_numpy(synthetic.level_walk(4, T5, seed=6)).to(dev)
@@ -375,7 +381,7 @@ def run_extras(dev, peak):
     ms5 = _event_ms(lambda: tb.fused_batch_d(s5, j5, st), 3, warm=1)
     bytes5 = 4 * T5 * (8 + 4 * len(o5))
     g5 = bytes5 / (ms5 * 1e-3) / 1e9
-    out["config5_long_4x50M"] = {
+    out["long_rows_4x50M"] = {
         "workload": "4 series x 50,000,000 bars (+1e4 level): SMA/STDDEV/VAR/LINEARREG 200, CORREL30, EMA500, "
                     "FP64 carries, decoupled look-back",
         "ms": ms5, "value": 6 * 4 * T5 / (ms5 * 1e-3), "unit": "indicator-bars/s",
