@@ -11,7 +11,8 @@
  * reference tree (oracle/_ref); OBV AD ADOSC MFI NATR and the candle patterns are
  * pinned against the reference's StreamStates.h / CandleUtils.h compiled on the
  * host. RMA is pinned against the vendored TA_RMA (the reference's device path
- * runs that same function). ROC ROCP ROCR ROCR100 MOM MEDPRICE TYPPRICE
+ * runs that same function) and, bit for bit, against the reference's TA-Lib
+ * 0.8.3 fixture tests/fixtures/talib08_typed.json (RMA(close, 14)). ROC ROCP ROCR ROCR100 MOM MEDPRICE TYPPRICE
  * AVGPRICE WCLPRICE MIDPRICE MIDPOINT restate the reference's float kernels
  * (src/indicators/ROC*.cu, Momentum.cu, MedPrice.cu, TypPrice.cu, AvgPrice.cu,
  * WclPrice.cu, MIDPRICE.cu, MIDPOINT.cu) operation for operation. ROC ROCP

@@ -6,6 +6,7 @@ reference build itself (oracle/_ref) on fresh seeded data when it is present.
 Families without reference CPU code (ADX, DX, CCI, WILLR, CORREL, SUM, MIN,
 MAX) are pinned by known-answer tests.
 """
+import os
 from pathlib import Path
 
 import numpy as np
@@ -224,3 +225,23 @@ def test_rolling_strict_known_answers():
     std = O.run("rolling_std", {"close": x}, period=2)[0][0]
     np.testing.assert_array_equal(std[[1, 4, 5]], [0.5, 0.5, 0.5])
     np.testing.assert_array_equal(O.run("change", {"close": x}, period=1)[0][0, 4:], [1.0, 1.0])
+
+
+# The reference's own TA-Lib 0.8.3 fixture for RMA(close, 14) on a 96-bar OHLC
+# series (tests/fixtures/talib08_typed.json, checked by its Node binding test
+# tests/node/talib08_typed.js:36). Read from the reference tree where it exists.
+REF_TREE = Path(os.environ.get("TACUDA_REFERENCE_TREE", "/root/reference"))
+RMA_FIXTURE = REF_TREE / "tests" / "fixtures" / "talib08_typed.json"
+
+
+@pytest.mark.skipif(not RMA_FIXTURE.exists(), reason="reference tree not present")
+def test_rma_matches_reference_talib_fixture():
+    import json
+    f = json.loads(RMA_FIXTURE.read_text())
+    close = np.array([f["close"]], np.float64)
+    assert np.array_equal(close.astype(np.float32).astype(np.float64), close)  # float32 values
+    want = np.array([[np.nan if v is None else v for v in f["rma"]]])
+    got = O.run("rma", {"close": close.astype(np.float32)}, period=14)[0]
+    np.testing.assert_array_equal(np.isnan(got), np.isnan(want))
+    m = ~np.isnan(want)
+    np.testing.assert_allclose(got[m], want[m], rtol=1e-14, atol=0)
