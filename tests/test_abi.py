@@ -73,3 +73,27 @@ def test_fused_job_validation():
     with pytest.raises(RuntimeError, match="bad candle mask"):
         tb.fused_batch_d(tb.make_series({k: 0x1000 for k in ("open", "high", "low", "close")}, 4, 100),
                          [tb.make_job("cdl", (), (), [0x2000], cdl_mask=0)])
+
+
+def test_appended_families_validate_like_the_reference():
+    lib = tb.get_lib()
+    P, I = ct.c_void_p, ct.c_int
+    fake = P(0x1000)
+    # ROC.cu / Momentum.cu / MIDPRICE.cu / MIDPOINT.cu: period <= 0 is invalid
+    for name in ("roc", "rocp", "rocr", "rocr100", "momentum", "change", "rma", "midpoint"):
+        assert getattr(lib, f"ct_{name}_batch_d")(fake, fake, I(10), I(2), I(0), I(0), P(0)) == 4, name
+        assert "invalid period" in tb.get_last_error()
+    assert lib.ct_midprice_batch_d(fake, fake, fake, I(10), I(2), I(-3), I(0), P(0)) == 4
+    # TA_RMA's period range ends at 100000
+    assert lib.ct_rma_batch_d(fake, fake, I(10), I(2), I(100001), I(0), P(0)) == 4
+    # staged windows end at 4096 bars
+    assert lib.ct_roc_batch_d(fake, fake, I(10), I(2), I(4097), I(0), P(0)) == 6
+    # ClubPack.cu:409-413: a rolling period above the row length is invalid
+    for name in ("rolling_mean", "rolling_max", "rolling_min", "rolling_std"):
+        assert getattr(lib, f"ct_{name}_batch_d")(fake, fake, I(10), I(2), I(11), I(0), P(0)) == 4, name
+        assert getattr(lib, f"ct_{name}_d")(fake, fake, I(10), I(11), P(0)) == 4, name
+    # null pointers, as for every entry
+    assert lib.ct_medprice_batch_d(P(0), fake, fake, I(10), I(2), I(0), P(0)) == 4
+    assert lib.ct_avgprice_batch_d(fake, fake, P(0), fake, fake, I(10), I(2), I(0), P(0)) == 4
+    assert lib.ct_typprice_d(fake, fake, fake, P(0), I(10), P(0)) == 4
+    assert lib.ct_wclprice_batch_d(fake, fake, fake, fake, I(0), I(2), I(0), P(0)) == 4
