@@ -9,7 +9,7 @@
 //     in FP64: TA_SMA, TA_EMA, TA_WMA, TA_RSI, TA_MACD, TA_ATR, TA_BBANDS,
 //     TA_STOCH, TA_STDDEV, TA_VAR, TA_LINEARREG, TA_DEMA, TA_TEMA, TA_T3,
 //     TA_TRANGE, TA_ROC, TA_ROCP, TA_RMA, TA_MEDPRICE, TA_TYPPRICE,
-//     TA_MIDPRICE.
+//     TA_MIDPRICE, TA_IBS, TA_MARKETFI.
 //   * include/utils/StreamStates.h: ObvState, AdState, precise::MfiState,
 //     precise::AdoscState, precise::NatrState (the fused batch arithmetic).
 //   * include/utils/CandleUtils.h: the cdl_*_talib pattern decisions.
@@ -171,7 +171,8 @@ int ref_hlc(int fam, const float* h, const float* l, const float* c, int S, int 
   return rc_all;
 }
 
-// Price transforms: 0 MEDPRICE(h,l), 1 TYPPRICE(h,l,c), 2 MIDPRICE(h,l; p).
+// Price transforms and per-bar functions: 0 MEDPRICE(h,l), 1 TYPPRICE(h,l,c),
+// 2 MIDPRICE(h,l; p), 3 IBS(h,l,c), 4 MARKETFI(h,l,v) (c carries v).
 int ref_price(int fam, const float* h, const float* l, const float* c, int S, int T, int p,
               double* out, int threads) {
   int rc_all = 0;
@@ -179,7 +180,7 @@ int ref_price(int fam, const float* h, const float* l, const float* c, int S, in
     Row r(T);
     const size_t o = static_cast<size_t>(s) * T;
     load(r.buf[0], h + o, T); load(r.buf[1], l + o, T);
-    if (fam == 1) load(r.buf[2], c + o, T);
+    if (fam == 1 || fam == 3 || fam == 4) load(r.buf[2], c + o, T);
     Arena a = r.make_arena();
     int beg = 0, nb = 0;
     TA_RetCode rc = TA_SUCCESS;
@@ -188,6 +189,9 @@ int ref_price(int fam, const float* h, const float* l, const float* c, int S, in
       case 1: rc = TA_TYPPRICE(a, 0, T - 1, r.buf[0].data(), r.buf[1].data(), r.buf[2].data(), &beg, &nb,
                                r.out[0].data()); break;
       case 2: rc = TA_MIDPRICE(a, 0, T - 1, r.buf[0].data(), r.buf[1].data(), p, &beg, &nb, r.out[0].data()); break;
+      case 3: rc = TA_IBS(a, 0, T - 1, r.buf[0].data(), r.buf[1].data(), r.buf[2].data(), &beg, &nb, r.out[0].data()); break;
+      case 4: rc = TA_MARKETFI(a, 0, T - 1, r.buf[0].data(), r.buf[1].data(), r.buf[2].data(), &beg, &nb,
+                               r.out[0].data()); break;
       default: rc = TA_BAD_PARAM;
     }
     if (rc != TA_SUCCESS) { rc_all = static_cast<int>(rc); nb = 0; }

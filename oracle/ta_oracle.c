@@ -819,6 +819,31 @@ static void row_rmax(RowCtx* r) { rolling_row(r, 1); }
 static void row_rmin(RowCtx* r) { rolling_row(r, 2); }
 static void row_rstd(RowCtx* r) { rolling_row(r, 3); }
 
+/* The reference's TA-Lib device runner (src/compat/Talib08.cu:72-97) starts a
+ * row at the first bar where no input is NaN (the last bar when none is
+ * complete); TA_IBS: (c - l) / (h - l), 0.5 where h - l <= 0; TA_MARKETFI:
+ * (h - l) / v, 0 where v == 0 (talib08 TA_IBS, TA_MARKETFI). */
+static void talib_bar_row(RowCtx* r, int mode) {
+  const float* a = r->in[0]; const float* b = r->in[1]; const float* z = r->in[2];
+  int n = r->n; double* o = r->out[0];
+  fill_nan(o, n);
+  int f = 0;
+  while (f < n - 1 && (isnan(a[f]) || isnan(b[f]) || isnan(z[f]))) ++f;
+  for (int t = f; t < n; ++t) {
+    double v;
+    if (mode == 0) {
+      const double range = (double)a[t] - (double)b[t];
+      v = ((double)z[t] - (double)b[t]) / range;
+      if (range <= 0.0) v = 0.5;
+    } else {
+      v = (double)z[t] != 0.0 ? ((double)a[t] - (double)b[t]) / (double)z[t] : 0.0;
+    }
+    o[t] = (double)(float)v;
+  }
+}
+static void row_ibs(RowCtx* r) { talib_bar_row(r, 0); }
+static void row_marketfi(RowCtx* r) { talib_bar_row(r, 1); }
+
 /* src/indicators/MIDPRICE.cu:11-24: fmaxf / fminf over [t-p+1, t] (NaN
  * ignored unless the whole window is NaN), 0.5f * (max + min), from bar p-1. */
 static void row_midprice(RowCtx* r) {
@@ -862,6 +887,7 @@ static const FamSpec kFam[ORC_FAMILY_COUNT] = {
   [ORC_MIDPOINT] = {1, 1, 1, 0, row_midpoint, 1},
   [ORC_RMEAN] = {1, 1, 1, 0, row_rmean, 1},  [ORC_RMAX] = {1, 1, 1, 0, row_rmax, 1},
   [ORC_RMIN] = {1, 1, 1, 0, row_rmin, 1},    [ORC_RSTD] = {1, 1, 1, 0, row_rstd, 1},
+  [ORC_IBS] = {3, 1, 0, 0, row_ibs, 0},      [ORC_MARKETFI] = {3, 1, 0, 0, row_marketfi, 0},
 };
 
 static int check_params(int family, const int* ip) {

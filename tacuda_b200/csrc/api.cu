@@ -46,7 +46,7 @@ ctStatus_t cuda_fail(ctStatus_t st, const char* where, cudaError_t e) {
 int min_period(int family) {
   switch (family) {
     case tb::F_OBV: case tb::F_AD: case tb::F_TRANGE: case tb::F_CDL: case tb::F_MEDPRICE: case tb::F_TYPPRICE:
-    case tb::F_AVGPRICE: case tb::F_WCLPRICE:
+    case tb::F_AVGPRICE: case tb::F_WCLPRICE: case tb::F_IBS: case tb::F_MARKETFI:
       return 0;
     default: return 1;
   }
@@ -55,8 +55,9 @@ int min_period(int family) {
 int default_inputs(int family, int* in) {
   switch (family) {
     case tb::F_ATR: case tb::F_NATR: case tb::F_TRANGE: case tb::F_ADX: case tb::F_DX:
-    case tb::F_STOCH: case tb::F_WILLR: case tb::F_CCI: case tb::F_TYPPRICE: case tb::F_WCLPRICE:
+    case tb::F_STOCH: case tb::F_WILLR: case tb::F_CCI: case tb::F_TYPPRICE: case tb::F_WCLPRICE: case tb::F_IBS:
       in[0] = tb::P_HIGH; in[1] = tb::P_LOW; in[2] = tb::P_CLOSE; return 3;
+    case tb::F_MARKETFI: in[0] = tb::P_HIGH; in[1] = tb::P_LOW; in[2] = tb::P_VOLUME; return 3;
     case tb::F_MEDPRICE: case tb::F_MIDPRICE: in[0] = tb::P_HIGH; in[1] = tb::P_LOW; return 2;
     case tb::F_AD: case tb::F_ADOSC: case tb::F_MFI:
       in[0] = tb::P_HIGH; in[1] = tb::P_LOW; in[2] = tb::P_CLOSE; in[3] = tb::P_VOLUME; return 4;
@@ -620,6 +621,38 @@ ctStatus_t ct_typprice_d(const float* d_high, const float* d_low, const float* d
   u.outputs[0] = d_output;
   const Planes P = hlc(d_high, d_low, d_close);
   return run_single(P.p, u, size, 1, stream, "ct_typprice_d");
+}
+
+ctStatus_t ct_ibs_batch_d(const float* d_highs, const float* d_lows, const float* d_closes, float* d_outputs,
+                          int seriesLen, int numSeries, int, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_IBS);
+  u.outputs[0] = d_outputs;
+  const Planes P = hlc(d_highs, d_lows, d_closes);
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_ibs_batch_d");
+}
+ctStatus_t ct_ibs_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, int size,
+                    cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_IBS);
+  u.outputs[0] = d_output;
+  const Planes P = hlc(d_high, d_low, d_close);
+  return run_single(P.p, u, size, 1, stream, "ct_ibs_d");
+}
+
+ctStatus_t ct_marketfi_batch_d(const float* d_highs, const float* d_lows, const float* d_volumes, float* d_outputs,
+                               int seriesLen, int numSeries, int, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_MARKETFI);
+  u.outputs[0] = d_outputs;
+  Planes P;
+  P.p[tb::P_HIGH] = d_highs; P.p[tb::P_LOW] = d_lows; P.p[tb::P_VOLUME] = d_volumes;
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_marketfi_batch_d");
+}
+ctStatus_t ct_marketfi_d(const float* d_high, const float* d_low, const float* d_volume, float* d_output, int size,
+                         cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_MARKETFI);
+  u.outputs[0] = d_output;
+  Planes P;
+  P.p[tb::P_HIGH] = d_high; P.p[tb::P_LOW] = d_low; P.p[tb::P_VOLUME] = d_volume;
+  return run_single(P.p, u, size, 1, stream, "ct_marketfi_d");
 }
 
 ctStatus_t ct_wclprice_batch_d(const float* d_highs, const float* d_lows, const float* d_closes, float* d_outputs,

@@ -86,6 +86,8 @@ __device__ __forceinline__ void run_job_ext(const Ctx<K>& c, const Job& j, Carry
     case F_RMAX: rolling_round(c, j, 1); break;
     case F_RMIN: rolling_round(c, j, 2); break;
     case F_RSTD: rolling_round(c, j, 3); break;
+    case F_IBS: talib_bar_round(c, j, cy, 0); break;
+    case F_MARKETFI: talib_bar_round(c, j, cy, 1); break;
     default: break;
   }
 }
@@ -348,6 +350,8 @@ __device__ void sp_run_job(sp::Driver& drv, const Job& j, const sp::Stage& st, c
     case F_RMAX: sp::sp_rolling(drv, j, st, ln, lane, 1); break;
     case F_RMIN: sp::sp_rolling(drv, j, st, ln, lane, 2); break;
     case F_RSTD: sp::sp_rolling(drv, j, st, ln, lane, 3); break;
+    case F_IBS: sp::sp_talib_bar(drv, j, st, ln, lane, 0); break;
+    case F_MARKETFI: sp::sp_talib_bar(drv, j, st, ln, lane, 1); break;
     default:
       for (int c = 0; c < drv.nchunks; ++c) { drv.begin(c); drv.end(c); }
   }
@@ -455,7 +459,7 @@ int lb_slots(const Job& j) {
     case F_DX: return 1;
     case F_OBV: case F_AD: return 1;
     case F_ADOSC: return 3;
-    case F_MIN: case F_MAX: case F_CORREL: case F_MIDPOINT: return 1;
+    case F_MIN: case F_MAX: case F_CORREL: case F_MIDPOINT: case F_IBS: case F_MARKETFI: return 1;
     default: return 0;
   }
 }
@@ -485,7 +489,7 @@ unsigned job_planes(const Job& j) {
       n = 1; break;
     case F_OBV: case F_CORREL: case F_MEDPRICE: case F_MIDPRICE: n = 2; break;
     case F_ATR: case F_NATR: case F_TRANGE: case F_ADX: case F_DX: case F_STOCH: case F_WILLR:
-    case F_TYPPRICE: case F_WCLPRICE:
+    case F_TYPPRICE: case F_WCLPRICE: case F_IBS: case F_MARKETFI:
       n = 3; break;
     case F_CCI: n = 3; break;
     case F_AD: case F_ADOSC: case F_MFI: case F_CDL: case F_AVGPRICE: n = 4; break;

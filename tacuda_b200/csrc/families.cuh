@@ -1133,6 +1133,55 @@ __device__ __forceinline__ void rolling_round(const Ctx<K>& c, const Job& j, int
   c.flush(0, (float*)j.out[0]);
 }
 
+// Per-bar TA-Lib functions run by the reference's TA-Lib 0.8.3 device runner
+// (src/compat/Talib08.cu:72-97): the row starts at the first bar where no input
+// is NaN (the last bar when there is none), earlier bars stay NaN; FP64, then
+// rounded to float.
+//   mode 0 IBS (h, l, c)       talib08 TA_IBS: (c - l) / (h - l), 0.5 where h - l <= 0
+//   mode 1 MARKETFI (h, l, v)  talib08 TA_MARKETFI: (h - l) / v, 0 where v == 0
+template <int K>
+__device__ __forceinline__ void talib_bar_round(const Ctx<K>& c, const Job& j, Carry& cy, int mode) {
+  const int p0 = j.in[0], p1 = j.in[1], p2 = j.in[2];
+  // first bar of the row with every input present (warp-uniform; look-back
+  // mode resolves it across tiles like the single-input start)
+  int f;
+  if (!c.lb && cy.f >= 0) {
+    f = cy.f;
+  } else {
+    int first = 0x7fffffff;
+    for (int k = 0; k < K; ++k) {
+      const int t = c.gb0() + k;
+      if (c.valid(t) && !isnan(c.x(p0, t)) && !isnan(c.x(p1, t)) && !isnan(c.x(p2, t))) { first = t; break; }
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) first = min(first, __shfl_xor_sync(kFull, first, d));
+    const int local = first == 0x7fffffff ? -1 : first;
+    f = c.lb ? lb_first_index(c.lbd + j.lb_slot, c.lbs, c.tile, local, c.err, c.lane) : local;
+  }
+  const int g0 = c.gb0();
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int t = g0 + k;
+    if (!c.valid(t)) break;
+    float o = qnan();
+    if ((f >= 0 && t >= f) || (f < 0 && t == c.n - 1)) {
+      const double a = c.x(p0, t), b = c.x(p1, t), z = c.x(p2, t);
+      double v;
+      if (mode == 0) {
+        const double range = a - b;
+        v = (z - b) / range;
+        if (range <= 0.0) v = 0.5;
+      } else {
+        v = z != 0.0 ? (a - b) / z : 0.0;
+      }
+      o = (float)v;
+    }
+    c.put(0, k, o);
+  }
+  cy.f = f;
+  c.flush(0, (float*)j.out[0]);
+}
+
 // WILLR(p): src/indicators/WILLR.cu:11-30: float window extrema (strict
 // comparisons seeded with the current bar), ((HH - C)/(HH - LL)) * -100 in
 // FP64, clamped to [-100, 0]; 0 for a zero range.

@@ -457,6 +457,38 @@ __device__ void sp_rolling(SP_ARGS, int mode) {
   }
 }
 
+// IBS / MARKETFI (talib_bar_round in families.cuh)
+__device__ void sp_talib_bar(SP_ARGS, int mode) {
+  const int p0 = j.in[0], p1 = j.in[1], p2 = j.in[2];
+  long long f = -1;
+  for (int c = 0; c < drv.nchunks; ++c) {
+    drv.begin(c);
+    const Row rw = drv.row(c);
+    const float* A = drv.pptr(c, p0);
+    const float* B = drv.pptr(c, p1);
+    const float* Z = drv.pptr(c, p2);
+    for_chunk(rw, [&](int r, long long t) {
+      if (f < 0 && !isnan(A[r]) && !isnan(B[r]) && !isnan(Z[r])) f = t;
+      float o = qnan();
+      if (f >= 0 || t == rw.n - 1) {
+        const double a = A[r], b = B[r], z = Z[r];
+        double v;
+        if (mode == 0) {
+          const double range = a - b;
+          v = (z - b) / range;
+          if (range <= 0.0) v = 0.5;
+        } else {
+          v = z != 0.0 ? (a - b) / z : 0.0;
+        }
+        o = (float)v;
+      }
+      st.put(0, lane, r, o);
+    });
+    SP_FLUSH(0);
+    drv.end(c);
+  }
+}
+
 // STOCH (talib08:16115-16302): fastK into the warp line for the chunk and the
 // 2(d-1) bars before it, then slowK / slowD as direct means.
 __device__ void sp_stoch(SP_ARGS) {

@@ -58,6 +58,8 @@ SPECS = {
     "rolling_max": ("ct_rolling_max_batch_d", ["close"], 1, [("i", "period")]),
     "rolling_min": ("ct_rolling_min_batch_d", ["close"], 1, [("i", "period")]),
     "rolling_std": ("ct_rolling_std_batch_d", ["close"], 1, [("i", "period")]),
+    "ibs": ("ct_ibs_batch_d", HLC, 1, []),
+    "marketfi": ("ct_marketfi_batch_d", ["high", "low", "volume"], 1, []),
 }
 
 DEFAULTS = {
@@ -72,7 +74,7 @@ DEFAULTS = {
     "rocp": dict(period=10), "rocr": dict(period=10), "rocr100": dict(period=10), "momentum": dict(period=10),
     "avgprice": {}, "wclprice": {}, "midpoint": dict(period=14), "change": dict(period=10),
     "rolling_mean": dict(period=20), "rolling_max": dict(period=20), "rolling_min": dict(period=20),
-    "rolling_std": dict(period=20),
+    "rolling_std": dict(period=20), "ibs": {}, "marketfi": {},
 }
 
 

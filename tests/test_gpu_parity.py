@@ -187,7 +187,7 @@ def test_leading_nan_and_interior_nan_semantics(mode):
     dp = device_planes(d)
     for name in ("ema", "rsi", "macd", "sma", "bbands", "willr", "min", "max", "dema", "roc", "rma",
                  "medprice", "typprice", "midprice", "rocp", "rocr", "rocr100", "momentum", "avgprice",
-                 "wclprice", "midpoint"):
+                 "wclprice", "midpoint", "ibs", "marketfi"):
         got = to_np(call_batch_d(name, dp, DEFAULTS[name]))
         ref = O.run(name, d, **DEFAULTS[name])
         for i, (g, r) in enumerate(zip(got, ref)):
@@ -247,7 +247,7 @@ def test_graph_capture_replay_equals_eager(mode):
 
 
 LOOKBACK_FAMILIES = ["ema", "dema", "tema", "t3", "rsi", "macd", "atr", "natr", "adx", "dx", "obv", "ad", "adosc",
-                     "min", "max", "correl", "sma", "stoch", "mfi", "rma", "roc", "midprice", "midpoint"]
+                     "min", "max", "correl", "sma", "stoch", "mfi", "rma", "roc", "midprice", "midpoint", "ibs"]
 SINGLE_INPUT = {"ema", "dema", "tema", "t3", "rsi", "macd", "min", "max", "sma", "rma", "roc", "midpoint"}
 
 
@@ -403,7 +403,8 @@ FLOAT_KERNELS = {"roc": [dict(period=1), dict(period=10), dict(period=700)], "me
                  "avgprice": [{}], "wclprice": [{}],
                  "midpoint": [dict(period=1), dict(period=7), dict(period=100)], "change": [dict(period=4)],
                  "rolling_mean": [dict(period=1), dict(period=30)], "rolling_max": [dict(period=7)],
-                 "rolling_min": [dict(period=200)], "rolling_std": [dict(period=1), dict(period=25)]}
+                 "rolling_min": [dict(period=200)], "rolling_std": [dict(period=1), dict(period=25)],
+                 "ibs": [{}], "marketfi": [{}]}
 
 
 @pytest.mark.parametrize("name", sorted(FLOAT_KERNELS))
@@ -484,3 +485,21 @@ def test_fused_pass_with_price_transforms_roc_rma(mode):
             if b > a:
                 compare(g[a:b], ref[a:b], f"ragged {fam} row {s} len {b - a}")
     plan.close()
+
+
+def test_talib_runner_prefix_rule(mode):
+    """IBS and MARKETFI start at the first bar where no input is NaN; a row
+    with no complete bar evaluates its last bar only (src/compat/Talib08.cu:72-84)."""
+    d = synthetic.ohlcv(6, 700, seed=47)
+    d["close"][1, :40] = np.nan
+    d["volume"][2, :333] = np.nan
+    d["close"][3, :] = np.nan
+    d["high"][3, -1] = d["low"][3, -1]  # zero range on the last bar: IBS gives 0.5 there
+    d["volume"][4, :] = np.nan
+    d["volume"][5, 100] = 0.0
+    dp = device_planes(d)
+    for name in ("ibs", "marketfi"):
+        got = to_np(call_batch_d(name, dp, {}))[0]
+        ref = O.run(name, d)[0]
+        compare(got, ref, f"prefix {name}")
+    assert to_np(call_batch_d("ibs", dp, {}))[0][3, -1] == 0.5
