@@ -97,6 +97,7 @@ CTAPI_EXPORT ctStatus_t ct_rolling_min_batch_d(const float *d_inputs, float *d_o
 CTAPI_EXPORT ctStatus_t ct_rolling_std_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:3199 */
 CTAPI_EXPORT ctStatus_t ct_ibs_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:3742 */
 CTAPI_EXPORT ctStatus_t ct_marketfi_batch_d(const float *d_highs, const float *d_lows, const float *d_volumes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:3932 */
+CTAPI_EXPORT ctStatus_t ct_qstick_batch_d(const float *d_opens, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:4096 */
 CTAPI_EXPORT ctStatus_t ct_avgprice_batch_d(const float *d_opens, const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1428 */
 
 /* candlestick patterns: float signal (+-100/+-80/+-200), warm-up 0 */
@@ -211,6 +212,7 @@ CTAPI_EXPORT ctStatus_t ct_rolling_min_d(const float* d_input, float* d_output, 
 CTAPI_EXPORT ctStatus_t ct_rolling_std_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:991 */
 CTAPI_EXPORT ctStatus_t ct_ibs_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:1120 */
 CTAPI_EXPORT ctStatus_t ct_marketfi_d(const float* d_high, const float* d_low, const float* d_volume, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:1169 */
+CTAPI_EXPORT ctStatus_t ct_qstick_d(const float* d_open, const float* d_close, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:1209 */
 CTAPI_EXPORT ctStatus_t ct_avgprice_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:338 */
 CTAPI_EXPORT ctStatus_t ct_cdl_doji_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:555 */
 CTAPI_EXPORT ctStatus_t ct_cdl_hammer_d(const float* d_open, const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:559 */
@@ -339,7 +341,7 @@ typedef enum ctB200Family {
   CT_B200_ROC, CT_B200_RMA, CT_B200_MEDPRICE, CT_B200_TYPPRICE, CT_B200_MIDPRICE,
   CT_B200_ROCP, CT_B200_ROCR, CT_B200_ROCR100, CT_B200_MOM, CT_B200_AVGPRICE, CT_B200_WCLPRICE,
   CT_B200_MIDPOINT, CT_B200_ROLLING_MEAN, CT_B200_ROLLING_MAX, CT_B200_ROLLING_MIN, CT_B200_ROLLING_STD,
-  CT_B200_IBS, CT_B200_MARKETFI
+  CT_B200_IBS, CT_B200_MARKETFI, CT_B200_QSTICK
 } ctB200Family_t;
 
 /* Input planes of a batch. */

@@ -69,6 +69,7 @@ FAMILIES = {
     "rolling_std": (43, ("close",), ("out",), ("period",), ()),
     "ibs": (44, ("high", "low", "close"), ("out",), (), ()),
     "marketfi": (45, ("high", "low", "volume"), ("out",), (), ()),
+    "qstick": (46, ("open", "close"), ("out",), ("period",), ()),
 }
 
 _P = ct.c_void_p
@@ -176,7 +177,7 @@ def _load_ref():
 _REF_SINGLE = {"sma": 0, "ema": 1, "wma": 2, "rsi": 3, "stddev": 4, "var": 5,
                "linearreg": 6, "dema": 7, "tema": 8, "t3": 9, "roc": 10, "rma": 11, "rocp": 12}
 _REF_STATES = {"obv": 0, "ad": 1, "mfi": 2, "adosc": 3, "natr": 4}
-_REF_PRICE = {"medprice": 0, "typprice": 1, "midprice": 2, "ibs": 3, "marketfi": 4}
+_REF_PRICE = {"medprice": 0, "typprice": 1, "midprice": 2, "ibs": 3, "marketfi": 4, "qstick": 5}
 REF_FAMILIES = (tuple(_REF_SINGLE) + ("macd", "bbands", "atr", "trange", "stoch") + tuple(_REF_STATES)
                 + tuple(_REF_PRICE))
 
@@ -206,6 +207,8 @@ def ref_run(name: str, data: dict, threads: int = 0, **params):
                             float(params["dn"]), *(o.ctypes.data for o in outs), threads)
         return tuple(outs) if rc == 0 else None
     h, l = _f4(data.get("high", c)), _f4(data.get("low", c))
+    if name == "qstick":
+        h, l = _f4(data["open"]), c
     if name in _REF_PRICE:
         out = np.empty(shape, np.float64)
         third = _f4(data["volume"]) if name == "marketfi" else c

@@ -9,7 +9,7 @@
 //     in FP64: TA_SMA, TA_EMA, TA_WMA, TA_RSI, TA_MACD, TA_ATR, TA_BBANDS,
 //     TA_STOCH, TA_STDDEV, TA_VAR, TA_LINEARREG, TA_DEMA, TA_TEMA, TA_T3,
 //     TA_TRANGE, TA_ROC, TA_ROCP, TA_RMA, TA_MEDPRICE, TA_TYPPRICE,
-//     TA_MIDPRICE, TA_IBS, TA_MARKETFI.
+//     TA_MIDPRICE, TA_IBS, TA_MARKETFI, TA_QSTICK.
 //   * include/utils/StreamStates.h: ObvState, AdState, precise::MfiState,
 //     precise::AdoscState, precise::NatrState (the fused batch arithmetic).
 //   * include/utils/CandleUtils.h: the cdl_*_talib pattern decisions.
@@ -172,7 +172,8 @@ int ref_hlc(int fam, const float* h, const float* l, const float* c, int S, int 
 }
 
 // Price transforms and per-bar functions: 0 MEDPRICE(h,l), 1 TYPPRICE(h,l,c),
-// 2 MIDPRICE(h,l; p), 3 IBS(h,l,c), 4 MARKETFI(h,l,v) (c carries v).
+// 2 MIDPRICE(h,l; p), 3 IBS(h,l,c), 4 MARKETFI(h,l,v) (c carries v),
+// 5 QSTICK(open, close; p) (h carries open, l close).
 int ref_price(int fam, const float* h, const float* l, const float* c, int S, int T, int p,
               double* out, int threads) {
   int rc_all = 0;
@@ -190,6 +191,7 @@ int ref_price(int fam, const float* h, const float* l, const float* c, int S, in
                                r.out[0].data()); break;
       case 2: rc = TA_MIDPRICE(a, 0, T - 1, r.buf[0].data(), r.buf[1].data(), p, &beg, &nb, r.out[0].data()); break;
       case 3: rc = TA_IBS(a, 0, T - 1, r.buf[0].data(), r.buf[1].data(), r.buf[2].data(), &beg, &nb, r.out[0].data()); break;
+      case 5: rc = TA_QSTICK(a, 0, T - 1, r.buf[0].data(), r.buf[1].data(), p, &beg, &nb, r.out[0].data()); break;
       case 4: rc = TA_MARKETFI(a, 0, T - 1, r.buf[0].data(), r.buf[1].data(), r.buf[2].data(), &beg, &nb,
                                r.out[0].data()); break;
       default: rc = TA_BAD_PARAM;

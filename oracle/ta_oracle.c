@@ -844,6 +844,27 @@ static void talib_bar_row(RowCtx* r, int mode) {
 static void row_ibs(RowCtx* r) { talib_bar_row(r, 0); }
 static void row_marketfi(RowCtx* r) { talib_bar_row(r, 1); }
 
+/* talib08 TA_QSTICK (running FP64 sum of close - open, mean over p bars)
+ * after the runner's start at the first bar with open and close present
+ * (src/compat/Talib08.cu:72-84); a NaN difference stays in the running sum. */
+static void row_qstick(RowCtx* r) {
+  const float* op = r->in[0]; const float* cl = r->in[1];
+  int n = r->n, p = r->ip[0]; double* o = r->out[0];
+  fill_nan(o, n);
+  int f = 0;
+  while (f < n - 1 && (isnan(op[f]) || isnan(cl[f]))) ++f;
+  if (n - f < p) return;
+  double total = 0.0;
+  int trailing = f, i = f;
+  for (; i < f + p - 1; ++i) total += (double)cl[i] - (double)op[i];
+  for (; i < n; ++i) {
+    total += (double)cl[i] - (double)op[i];
+    o[i] = (double)(float)(total / (double)p);
+    total -= (double)cl[trailing] - (double)op[trailing];
+    ++trailing;
+  }
+}
+
 /* src/indicators/MIDPRICE.cu:11-24: fmaxf / fminf over [t-p+1, t] (NaN
  * ignored unless the whole window is NaN), 0.5f * (max + min), from bar p-1. */
 static void row_midprice(RowCtx* r) {
@@ -888,6 +909,7 @@ static const FamSpec kFam[ORC_FAMILY_COUNT] = {
   [ORC_RMEAN] = {1, 1, 1, 0, row_rmean, 1},  [ORC_RMAX] = {1, 1, 1, 0, row_rmax, 1},
   [ORC_RMIN] = {1, 1, 1, 0, row_rmin, 1},    [ORC_RSTD] = {1, 1, 1, 0, row_rstd, 1},
   [ORC_IBS] = {3, 1, 0, 0, row_ibs, 0},      [ORC_MARKETFI] = {3, 1, 0, 0, row_marketfi, 0},
+  [ORC_QSTICK] = {2, 1, 1, 0, row_qstick, 1},
 };
 
 static int check_params(int family, const int* ip) {

@@ -13,7 +13,8 @@
  * host. RMA is pinned against the vendored TA_RMA (the reference's device path
  * runs that same function) and, bit for bit, against the reference's TA-Lib
  * 0.8.3 fixture tests/fixtures/talib08_typed.json (RMA(close, 14)). IBS and
- * MARKETFI are pinned against the vendored TA_IBS / TA_MARKETFI. ROC ROCP ROCR ROCR100 MOM MEDPRICE TYPPRICE
+ * MARKETFI and QSTICK are pinned against the vendored TA_IBS / TA_MARKETFI /
+ * TA_QSTICK. ROC ROCP ROCR ROCR100 MOM MEDPRICE TYPPRICE
  * AVGPRICE WCLPRICE MIDPRICE MIDPOINT restate the reference's float kernels
  * (src/indicators/ROC*.cu, Momentum.cu, MedPrice.cu, TypPrice.cu, AvgPrice.cu,
  * WclPrice.cu, MIDPRICE.cu, MIDPOINT.cu) operation for operation. ROC ROCP
@@ -37,7 +38,7 @@ enum OracleFamily {
   ORC_CORREL, ORC_DEMA, ORC_TEMA, ORC_T3, ORC_ROC, ORC_RMA, ORC_MEDPRICE,
   ORC_TYPPRICE, ORC_MIDPRICE, ORC_ROCP, ORC_ROCR, ORC_ROCR100, ORC_MOM,
   ORC_AVGPRICE, ORC_WCLPRICE, ORC_MIDPOINT, ORC_RMEAN, ORC_RMAX, ORC_RMIN,
-  ORC_RSTD, ORC_IBS, ORC_MARKETFI, ORC_FAMILY_COUNT
+  ORC_RSTD, ORC_IBS, ORC_MARKETFI, ORC_QSTICK, ORC_FAMILY_COUNT
 };
 
 /* ins: the family's input planes (see oracle/oracle.py INPUTS); outs: its output

@@ -36,7 +36,7 @@ FAMILIES = ("sma", "ema", "wma", "rsi", "macd", "atr", "natr", "trange", "adx", 
             "cci", "obv", "ad", "adosc", "mfi", "willr", "sum", "min", "max", "stddev", "var", "linearreg",
             "correl", "dema", "tema", "t3", "cdl", "roc", "rma", "medprice", "typprice", "midprice",
             "rocp", "rocr", "rocr100", "momentum", "avgprice", "wclprice", "midpoint",
-            "rolling_mean", "rolling_max", "rolling_min", "rolling_std", "ibs", "marketfi")
+            "rolling_mean", "rolling_max", "rolling_min", "rolling_std", "ibs", "marketfi", "qstick")
 FAMILY_ID = {n: i for i, n in enumerate(FAMILIES)}
 PLANES = ("open", "high", "low", "close", "volume", "aux")
 PLANE_ID = {n: i for i, n in enumerate(PLANES)}

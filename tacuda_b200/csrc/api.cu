@@ -58,6 +58,7 @@ int default_inputs(int family, int* in) {
     case tb::F_STOCH: case tb::F_WILLR: case tb::F_CCI: case tb::F_TYPPRICE: case tb::F_WCLPRICE: case tb::F_IBS:
       in[0] = tb::P_HIGH; in[1] = tb::P_LOW; in[2] = tb::P_CLOSE; return 3;
     case tb::F_MARKETFI: in[0] = tb::P_HIGH; in[1] = tb::P_LOW; in[2] = tb::P_VOLUME; return 3;
+    case tb::F_QSTICK: in[0] = tb::P_OPEN; in[1] = tb::P_CLOSE; return 2;
     case tb::F_MEDPRICE: case tb::F_MIDPRICE: in[0] = tb::P_HIGH; in[1] = tb::P_LOW; return 2;
     case tb::F_AD: case tb::F_ADOSC: case tb::F_MFI:
       in[0] = tb::P_HIGH; in[1] = tb::P_LOW; in[2] = tb::P_CLOSE; in[3] = tb::P_VOLUME; return 4;
@@ -104,6 +105,7 @@ ctStatus_t make_job(const ctB200Job& u, Job& j, const char* who) {
     case tb::F_LINEARREG: case tb::F_MIN: case tb::F_MAX: case tb::F_WILLR: case tb::F_CCI: case tb::F_MFI:
     case tb::F_CORREL: case tb::F_ROC: case tb::F_MIDPRICE: case tb::F_ROCP: case tb::F_ROCR: case tb::F_ROCR100:
     case tb::F_MOM: case tb::F_MIDPOINT: case tb::F_RMEAN: case tb::F_RMAX: case tb::F_RMIN: case tb::F_RSTD:
+    case tb::F_QSTICK:
       if (u.params[0] > kMaxWindow) return fail(CT_STATUS_UNSUPPORTED, std::string(who) + ": window period above 4096");
       break;
     case tb::F_STOCH:
@@ -653,6 +655,23 @@ ctStatus_t ct_marketfi_d(const float* d_high, const float* d_low, const float* d
   Planes P;
   P.p[tb::P_HIGH] = d_high; P.p[tb::P_LOW] = d_low; P.p[tb::P_VOLUME] = d_volume;
   return run_single(P.p, u, size, 1, stream, "ct_marketfi_d");
+}
+
+ctStatus_t ct_qstick_batch_d(const float* d_opens, const float* d_closes, float* d_outputs, int seriesLen,
+                             int numSeries, int period, int, cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_QSTICK, period);
+  u.outputs[0] = d_outputs;
+  Planes P;
+  P.p[tb::P_OPEN] = d_opens; P.p[tb::P_CLOSE] = d_closes;
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_qstick_batch_d");
+}
+ctStatus_t ct_qstick_d(const float* d_open, const float* d_close, float* d_output, int size, int period,
+                       cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_QSTICK, period);
+  u.outputs[0] = d_output;
+  Planes P;
+  P.p[tb::P_OPEN] = d_open; P.p[tb::P_CLOSE] = d_close;
+  return run_single(P.p, u, size, 1, stream, "ct_qstick_d");
 }
 
 ctStatus_t ct_wclprice_batch_d(const float* d_highs, const float* d_lows, const float* d_closes, float* d_outputs,

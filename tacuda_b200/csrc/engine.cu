@@ -88,6 +88,7 @@ __device__ __forceinline__ void run_job_ext(const Ctx<K>& c, const Job& j, Carry
     case F_RSTD: rolling_round(c, j, 3); break;
     case F_IBS: talib_bar_round(c, j, cy, 0); break;
     case F_MARKETFI: talib_bar_round(c, j, cy, 1); break;
+    case F_QSTICK: qstick_round(c, j, cy); break;
     default: break;
   }
 }
@@ -352,6 +353,7 @@ __device__ void sp_run_job(sp::Driver& drv, const Job& j, const sp::Stage& st, c
     case F_RSTD: sp::sp_rolling(drv, j, st, ln, lane, 3); break;
     case F_IBS: sp::sp_talib_bar(drv, j, st, ln, lane, 0); break;
     case F_MARKETFI: sp::sp_talib_bar(drv, j, st, ln, lane, 1); break;
+    case F_QSTICK: sp::sp_qstick(drv, j, st, ln, lane); break;
     default:
       for (int c = 0; c < drv.nchunks; ++c) { drv.begin(c); drv.end(c); }
   }
@@ -448,7 +450,7 @@ namespace {
 // recurrence stage, in the order the round functions address them.
 int lb_slots(const Job& j) {
   switch (j.family) {
-    case F_EMA: case F_RMA: return 2;
+    case F_EMA: case F_RMA: case F_QSTICK: return 2;
     case F_DEMA: return 3;
     case F_TEMA: return 4;
     case F_T3: return 7;
@@ -470,7 +472,7 @@ int job_halo(const Job& j) {
     case F_LINEARREG: case F_MIN: case F_MAX: case F_WILLR: case F_CCI: case F_CORREL:
       return j.ip[0] - 1;
     case F_MFI: case F_ROC: case F_ROCP: case F_ROCR: case F_ROCR100: case F_MOM: return j.ip[0];
-    case F_MIDPOINT: case F_RMEAN: case F_RMAX: case F_RMIN: case F_RSTD: return j.ip[0] - 1;
+    case F_MIDPOINT: case F_RMEAN: case F_RMAX: case F_RMIN: case F_RSTD: case F_QSTICK: return j.ip[0] - 1;
     case F_MIDPRICE: return j.ip[0] - 1;
     case F_STOCH: return j.ip[0] - 1 + 2 * (j.ip[1] - 1);
     case F_CDL: return 16;  // 10-bar averages anchored up to 5 bars back
@@ -487,7 +489,7 @@ unsigned job_planes(const Job& j) {
     case F_TEMA: case F_T3: case F_ROC: case F_RMA: case F_ROCP: case F_ROCR: case F_ROCR100:
     case F_MOM: case F_MIDPOINT: case F_RMEAN: case F_RMAX: case F_RMIN: case F_RSTD:
       n = 1; break;
-    case F_OBV: case F_CORREL: case F_MEDPRICE: case F_MIDPRICE: n = 2; break;
+    case F_OBV: case F_CORREL: case F_MEDPRICE: case F_MIDPRICE: case F_QSTICK: n = 2; break;
     case F_ATR: case F_NATR: case F_TRANGE: case F_ADX: case F_DX: case F_STOCH: case F_WILLR:
     case F_TYPPRICE: case F_WCLPRICE: case F_IBS: case F_MARKETFI:
       n = 3; break;

@@ -489,6 +489,31 @@ __device__ void sp_talib_bar(SP_ARGS, int mode) {
   }
 }
 
+// QSTICK (qstick_round in families.cuh)
+__device__ void sp_qstick(SP_ARGS) {
+  const int po = j.in[0], pc = j.in[1], p = j.ip[0];
+  long long f = -1, g = -1;
+  for (int c = 0; c < drv.nchunks; ++c) {
+    drv.begin(c);
+    const Row rw = drv.row(c);
+    const float* O = drv.pptr(c, po);
+    const float* C2 = drv.pptr(c, pc);
+    for_chunk(rw, [&](int r, long long t) {
+      if (f < 0 && !isnan(O[r]) && !isnan(C2[r])) f = t;
+      if (f >= 0 && g < 0 && isnan((double)C2[r] - (double)O[r])) g = t;
+      float o = qnan();
+      if (f >= 0 && t >= f + p - 1 && g < 0) {
+        double s = 0.0;
+        for (int i = r - p + 1; i <= r; ++i) s += (double)C2[i] - (double)O[i];
+        o = (float)(s / (double)p);
+      }
+      st.put(0, lane, r, o);
+    });
+    SP_FLUSH(0);
+    drv.end(c);
+  }
+}
+
 // STOCH (talib08:16115-16302): fastK into the warp line for the chunk and the
 // 2(d-1) bars before it, then slowK / slowD as direct means.
 __device__ void sp_stoch(SP_ARGS) {

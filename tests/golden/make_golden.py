@@ -30,7 +30,7 @@ CASES = {
     "atr": dict(period=14), "trange": {}, "stoch": dict(k=14, d=3), "obv": {}, "ad": {},
     "mfi": dict(period=14), "adosc": dict(fast=3, slow=10), "natr": dict(period=14),
     "roc": dict(period=10), "rma": dict(period=14), "medprice": {}, "typprice": {}, "midprice": dict(period=14),
-    "rocp": dict(period=10), "ibs": {}, "marketfi": {},
+    "rocp": dict(period=10), "ibs": {}, "marketfi": {}, "qstick": dict(period=10),
 }
 
 

@@ -60,6 +60,7 @@ SPECS = {
     "rolling_std": ("ct_rolling_std_batch_d", ["close"], 1, [("i", "period")]),
     "ibs": ("ct_ibs_batch_d", HLC, 1, []),
     "marketfi": ("ct_marketfi_batch_d", ["high", "low", "volume"], 1, []),
+    "qstick": ("ct_qstick_batch_d", ["open", "close"], 1, [("i", "period")]),
 }
 
 DEFAULTS = {
@@ -74,7 +75,7 @@ DEFAULTS = {
     "rocp": dict(period=10), "rocr": dict(period=10), "rocr100": dict(period=10), "momentum": dict(period=10),
     "avgprice": {}, "wclprice": {}, "midpoint": dict(period=14), "change": dict(period=10),
     "rolling_mean": dict(period=20), "rolling_max": dict(period=20), "rolling_min": dict(period=20),
-    "rolling_std": dict(period=20), "ibs": {}, "marketfi": {},
+    "rolling_std": dict(period=20), "ibs": {}, "marketfi": {}, "qstick": dict(period=10),
 }
 
 

@@ -87,6 +87,7 @@ VARIANTS = {
     "midprice": [dict(period=1), dict(period=2), dict(period=40)],
     "midpoint": [dict(period=1), dict(period=2), dict(period=40)],
     "momentum": [dict(period=1), dict(period=250)],
+    "qstick": [dict(period=1), dict(period=2), dict(period=64)],
 }
 
 
@@ -187,7 +188,7 @@ def test_leading_nan_and_interior_nan_semantics(mode):
     dp = device_planes(d)
     for name in ("ema", "rsi", "macd", "sma", "bbands", "willr", "min", "max", "dema", "roc", "rma",
                  "medprice", "typprice", "midprice", "rocp", "rocr", "rocr100", "momentum", "avgprice",
-                 "wclprice", "midpoint", "ibs", "marketfi"):
+                 "wclprice", "midpoint", "ibs", "marketfi", "qstick"):
         got = to_np(call_batch_d(name, dp, DEFAULTS[name]))
         ref = O.run(name, d, **DEFAULTS[name])
         for i, (g, r) in enumerate(zip(got, ref)):
@@ -247,7 +248,7 @@ def test_graph_capture_replay_equals_eager(mode):
 
 
 LOOKBACK_FAMILIES = ["ema", "dema", "tema", "t3", "rsi", "macd", "atr", "natr", "adx", "dx", "obv", "ad", "adosc",
-                     "min", "max", "correl", "sma", "stoch", "mfi", "rma", "roc", "midprice", "midpoint", "ibs"]
+                     "min", "max", "correl", "sma", "stoch", "mfi", "rma", "roc", "midprice", "midpoint", "ibs", "qstick"]
 SINGLE_INPUT = {"ema", "dema", "tema", "t3", "rsi", "macd", "min", "max", "sma", "rma", "roc", "midpoint"}
 
 
@@ -498,8 +499,11 @@ def test_talib_runner_prefix_rule(mode):
     d["volume"][4, :] = np.nan
     d["volume"][5, 100] = 0.0
     dp = device_planes(d)
-    for name in ("ibs", "marketfi"):
-        got = to_np(call_batch_d(name, dp, {}))[0]
-        ref = O.run(name, d)[0]
+    d["open"][4, 500] = np.nan  # QSTICK: NaN from here to the end of the row
+    dp = device_planes(d)
+    for name, p in (("ibs", {}), ("marketfi", {}), ("qstick", dict(period=10))):
+        got = to_np(call_batch_d(name, dp, p))[0]
+        ref = O.run(name, d, **p)[0]
         compare(got, ref, f"prefix {name}")
+    assert np.isnan(to_np(call_batch_d("qstick", dp, dict(period=10)))[0][4, 500:]).all()
     assert to_np(call_batch_d("ibs", dp, {}))[0][3, -1] == 0.5
