@@ -23,7 +23,7 @@ OUT = PKG / "libtacuda_b200.so"
 # (source, object name, extra defines): engine.cu is compiled twice, the second
 # time for the kernels of the precision variants only
 SOURCES = [("engine.cu", "engine.cu.o", []), ("engine.cu", "engine_prec.cu.o", ["-DTB_PREC_TU"]),
-           ("adjoint.cu", "adjoint.cu.o", []), ("api.cu", "api.cu.o", []),
+           ("rows.cu", "rows.cu.o", []), ("adjoint.cu", "adjoint.cu.o", []), ("api.cu", "api.cu.o", []),
            ("scheduler.cpp", "scheduler.cpp.o", []), ("pool.cpp", "pool.cpp.o", [])]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -39,11 +39,24 @@ def _run(cmd):
     subprocess.run(cmd, check=True)
 
 
+def _includes(src: Path, seen: set) -> set:
+    """Project headers a source includes, directly or through other headers."""
+    import re
+    for name in re.findall(r'^\s*#\s*include\s+"([^"]+)"', src.read_text(), re.M):
+        for d in (src.parent, CSRC, ROOT / "include"):
+            h = d / name
+            if h.exists():
+                if h not in seen:
+                    seen.add(h)
+                    _includes(h, seen)
+                break
+    return seen
+
+
 def build_library(verbose: bool = False) -> Path:
     from concurrent.futures import ThreadPoolExecutor
     objdir = ROOT / "_build"
     objdir.mkdir(exist_ok=True)
-    deps = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(CSRC.glob("*.inc")) + [ROOT / "include" / "tacuda.h"]
     jobs, objs = [], []
     for src_name, obj_name, defines in SOURCES:
         src = CSRC / src_name
@@ -51,6 +64,7 @@ def build_library(verbose: bool = False) -> Path:
             continue
         obj = objdir / obj_name
         objs.append(str(obj))
+        deps = sorted(_includes(src, set()))
         if not obj.exists() or any(d.stat().st_mtime > obj.stat().st_mtime for d in deps + [src]):
             cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC,-fvisibility=hidden",
                    f"-I{ROOT / 'include'}", f"-I{CSRC}", *defines, "-c", str(src), "-o", str(obj)]

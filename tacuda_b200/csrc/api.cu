@@ -199,6 +199,7 @@ ctStatus_t finish(cudaStream_t stream, const char* who) {
 ctStatus_t launch(Launch& L, long long total, long long maxlen, const tb::SchedulePlan* forced, cudaStream_t stream,
                   const char* who, tb::LaunchStats* stats = nullptr) {
   const tb::SchedulePlan plan = forced ? *forced : tb::plan_for(L, total, maxlen);
+  L.max_len = maxlen;
   const cudaError_t e = tb::launch_batch(L, plan, total, stream, stats);
   if (e != cudaSuccess) return cuda_fail(CT_STATUS_KERNEL_FAILED, who, e);
   g_launches.fetch_add(1, std::memory_order_relaxed);

@@ -90,4 +90,14 @@ __device__ __forceinline__ double true_range(double hi, double lo, double yc) {
   return g;
 }
 
+// TA-Lib's EMA coefficients (talib08:5546-5627 TA_EMA): beta = (p-1)/(p+1),
+// k = 1 - beta, and beta = 1 - k when beta < 0.5.
+__host__ __device__ inline void talib_ema_coeffs(int p, double& beta, double& k) {
+  double b = (double)(p - 1) / (double)(p + 1);
+  double kk = 1.0 - b;
+  if (b < 0.5) b = 1.0 - kk;
+  beta = b;
+  k = kk;
+}
+
 }  // namespace tb

@@ -19,6 +19,7 @@
 #include "families.cuh"
 #include "families_prec.cuh"
 #include "scheduler.h"
+#include "jobs.h"
 #ifndef TB_PREC_TU
 #include "candles.cuh"
 #include "sp_candles.cuh"
@@ -302,117 +303,6 @@ __global__ void __launch_bounds__(256, (K <= 8 ? 2 : 1)) batch_kernel(const __gr
   }
 }
 
-#ifndef TB_PREC_TU
-// ------------------------------------------------------- series-parallel
-
-__device__ void sp_run_job(sp::Driver& drv, const Job& j, const sp::Stage& st, const sp::Line& ln, int lane) {
-  switch (j.family) {
-    case F_SMA: sp::sp_sum_window(drv, j, st, ln, lane, 0); break;
-    case F_SUM: sp::sp_sum_window(drv, j, st, ln, lane, 1); break;
-    case F_WMA: sp::sp_sum_window(drv, j, st, ln, lane, 2); break;
-    case F_BBANDS: sp::sp_moment_window(drv, j, st, ln, lane, 0); break;
-    case F_STDDEV: sp::sp_moment_window(drv, j, st, ln, lane, 1); break;
-    case F_VAR: sp::sp_moment_window(drv, j, st, ln, lane, 2); break;
-    case F_LINEARREG: sp::sp_linreg(drv, j, st, ln, lane); break;
-    case F_CORREL: sp::sp_correl(drv, j, st, ln, lane); break;
-    case F_MIN: sp::sp_minmax(drv, j, st, ln, lane, false); break;
-    case F_MAX: sp::sp_minmax(drv, j, st, ln, lane, true); break;
-    case F_WILLR: sp::sp_willr(drv, j, st, ln, lane); break;
-    case F_STOCH: sp::sp_stoch(drv, j, st, ln, lane); break;
-    case F_CCI: sp::sp_cci(drv, j, st, ln, lane); break;
-    case F_MFI: sp::sp_mfi(drv, j, st, ln, lane); break;
-    case F_EMA: sp::sp_ema(drv, j, st, ln, lane); break;
-    case F_DEMA: sp::sp_cascade(drv, j, st, ln, lane, 2); break;
-    case F_TEMA: sp::sp_cascade(drv, j, st, ln, lane, 3); break;
-    case F_T3: sp::sp_cascade(drv, j, st, ln, lane, 6); break;
-    case F_RSI: sp::sp_rsi(drv, j, st, ln, lane); break;
-    case F_MACD: sp::sp_macd(drv, j, st, ln, lane); break;
-    case F_ATR: sp::sp_atr(drv, j, st, ln, lane, 0); break;
-    case F_NATR: sp::sp_atr(drv, j, st, ln, lane, 1); break;
-    case F_TRANGE: sp::sp_atr(drv, j, st, ln, lane, 2); break;
-    case F_ADX: sp::sp_adx(drv, j, st, ln, lane, true); break;
-    case F_DX: sp::sp_adx(drv, j, st, ln, lane, false); break;
-    case F_OBV: sp::sp_volume(drv, j, st, ln, lane, 0); break;
-    case F_AD: sp::sp_volume(drv, j, st, ln, lane, 1); break;
-    case F_ADOSC: sp::sp_volume(drv, j, st, ln, lane, 2); break;
-    case F_ROC: sp::sp_roc(drv, j, st, ln, lane, 0); break;
-    case F_ROCP: sp::sp_roc(drv, j, st, ln, lane, 1); break;
-    case F_ROCR: sp::sp_roc(drv, j, st, ln, lane, 2); break;
-    case F_ROCR100: sp::sp_roc(drv, j, st, ln, lane, 3); break;
-    case F_MOM: sp::sp_roc(drv, j, st, ln, lane, 4); break;
-    case F_RMA: sp::sp_ema(drv, j, st, ln, lane); break;
-    case F_MEDPRICE: sp::sp_price(drv, j, st, ln, lane, 0); break;
-    case F_TYPPRICE: sp::sp_price(drv, j, st, ln, lane, 1); break;
-    case F_AVGPRICE: sp::sp_price(drv, j, st, ln, lane, 2); break;
-    case F_WCLPRICE: sp::sp_price(drv, j, st, ln, lane, 3); break;
-    case F_MIDPRICE: sp::sp_midprice(drv, j, st, ln, lane); break;
-    case F_MIDPOINT: sp::sp_minmax(drv, j, st, ln, lane, false, true); break;
-    case F_RMEAN: sp::sp_rolling(drv, j, st, ln, lane, 0); break;
-    case F_RMAX: sp::sp_rolling(drv, j, st, ln, lane, 1); break;
-    case F_RMIN: sp::sp_rolling(drv, j, st, ln, lane, 2); break;
-    case F_RSTD: sp::sp_rolling(drv, j, st, ln, lane, 3); break;
-    case F_IBS: sp::sp_talib_bar(drv, j, st, ln, lane, 0); break;
-    case F_MARKETFI: sp::sp_talib_bar(drv, j, st, ln, lane, 1); break;
-    case F_QSTICK: sp::sp_qstick(drv, j, st, ln, lane); break;
-    default:
-      for (int c = 0; c < drv.nchunks; ++c) { drv.begin(c); drv.end(c); }
-  }
-}
-
-__global__ void __launch_bounds__(768) sp_kernel(const __grid_constant__ Launch L, const sp::Layout lay) {
-  // Layout fields used here: warp_off/warp_tp per warp, cdl_* for candle jobs.
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int rows = lay.G * 32;
-  long long* rows_base = reinterpret_cast<long long*>(smem + 2 * (size_t)lay.in_bytes);
-  long long* rows_n = rows_base + rows;
-  int* maxlen_slot = reinterpret_cast<int*>(rows_n + rows);
-  const int group = warp / lay.J;
-  const Job& job = L.jobs[warp % lay.J];
-  sp::Stage st{reinterpret_cast<float*>(smem + lay.warp_off[warp])};
-  sp::Line ln{lay.warp_tp[warp] ? reinterpret_cast<double*>(smem + lay.warp_line[warp]) : nullptr, lay.RS, lay.H};
-  const bool is_cdl = job.family == F_CDL;
-  sp::CdlTable tbl{is_cdl ? reinterpret_cast<double*>(smem + lay.cdl_table_off + (size_t)group * lay.cdl_table_bytes)
-                          : nullptr,
-                   sp::C + sp::kCdlBack};
-  const long long ngs = ((long long)L.S + rows - 1) / rows;
-  for (long long gs = blockIdx.x; gs < ngs; gs += gridDim.x) {
-    __syncthreads();
-    if (threadIdx.x == 0) *maxlen_slot = 0;
-    __syncthreads();
-    for (int i = threadIdx.x; i < rows; i += blockDim.x) {
-      const long long idx = gs * rows + i;
-      long long b = -1, n = 0;
-      if (idx < L.S) {
-        const int s = L.order ? L.order[idx] : (int)idx;
-        if (L.offsets) { b = L.offsets[s]; n = L.offsets[s + 1] - b; }
-        else { b = (long long)s * L.T; n = L.T; }
-      }
-      rows_base[i] = b;
-      rows_n[i] = n;
-      atomicMax(maxlen_slot, (int)min(n, (long long)0x7fffffff));
-    }
-    __syncthreads();
-    sp::Driver drv;
-    drv.L = &L;
-    drv.lay = &lay;
-    drv.smem = smem;
-    drv.rows_base = rows_base;
-    drv.rows_n = rows_n;
-    drv.nchunks = (*maxlen_slot + sp::C - 1) / sp::C;
-    drv.group = group;
-    drv.lane = lane;
-    drv.my_base = rows_base[group * 32 + lane];
-    drv.my_n = rows_n[group * 32 + lane];
-    if (is_cdl)
-      sp::sp_cdl_job(drv, job, st, lane, tbl, (warp % lay.J) == lay.cdl_first, 1 + group, 32 * lay.cdl_count);
-    else
-      sp_run_job(drv, job, st, ln, lane);
-  }
-}
-
-#endif  // TB_PREC_TU
-
 // First look-back tile of every ragged series: tile_start[s] = sum over
 // earlier series of ceil(n / tile), tile_start[S] = total. One block.
 static __global__ void __launch_bounds__(1024) lb_tile_start_kernel(const long long* offsets, int S, int tile,
@@ -445,72 +335,6 @@ static __global__ void __launch_bounds__(1024) lb_tile_start_kernel(const long l
 // ------------------------------------------------------------------ host side
 
 namespace {
-
-// Look-back descriptor slots of a job: one per first-index carry and one per
-// recurrence stage, in the order the round functions address them.
-int lb_slots(const Job& j) {
-  switch (j.family) {
-    case F_EMA: case F_RMA: case F_QSTICK: return 2;
-    case F_DEMA: return 3;
-    case F_TEMA: return 4;
-    case F_T3: return 7;
-    case F_RSI: return 2;
-    case F_MACD: return 4;
-    case F_ATR: case F_NATR: return 1;
-    case F_ADX: return 2;
-    case F_DX: return 1;
-    case F_OBV: case F_AD: return 1;
-    case F_ADOSC: return 3;
-    case F_MIN: case F_MAX: case F_CORREL: case F_MIDPOINT: case F_IBS: case F_MARKETFI: return 1;
-    default: return 0;
-  }
-}
-
-int job_halo(const Job& j) {
-  switch (j.family) {
-    case F_SMA: case F_SUM: case F_WMA: case F_BBANDS: case F_STDDEV: case F_VAR:
-    case F_LINEARREG: case F_MIN: case F_MAX: case F_WILLR: case F_CCI: case F_CORREL:
-      return j.ip[0] - 1;
-    case F_MFI: case F_ROC: case F_ROCP: case F_ROCR: case F_ROCR100: case F_MOM: return j.ip[0];
-    case F_MIDPOINT: case F_RMEAN: case F_RMAX: case F_RMIN: case F_RSTD: case F_QSTICK: return j.ip[0] - 1;
-    case F_MIDPRICE: return j.ip[0] - 1;
-    case F_STOCH: return j.ip[0] - 1 + 2 * (j.ip[1] - 1);
-    case F_CDL: return 16;  // 10-bar averages anchored up to 5 bars back
-    default: return 1;  // previous bar
-  }
-}
-
-unsigned job_planes(const Job& j) {
-  unsigned m = 0;
-  int n = 0;
-  switch (j.family) {
-    case F_SMA: case F_EMA: case F_WMA: case F_RSI: case F_MACD: case F_BBANDS: case F_SUM:
-    case F_MIN: case F_MAX: case F_STDDEV: case F_VAR: case F_LINEARREG: case F_DEMA:
-    case F_TEMA: case F_T3: case F_ROC: case F_RMA: case F_ROCP: case F_ROCR: case F_ROCR100:
-    case F_MOM: case F_MIDPOINT: case F_RMEAN: case F_RMAX: case F_RMIN: case F_RSTD:
-      n = 1; break;
-    case F_OBV: case F_CORREL: case F_MEDPRICE: case F_MIDPRICE: case F_QSTICK: n = 2; break;
-    case F_ATR: case F_NATR: case F_TRANGE: case F_ADX: case F_DX: case F_STOCH: case F_WILLR:
-    case F_TYPPRICE: case F_WCLPRICE: case F_IBS: case F_MARKETFI:
-      n = 3; break;
-    case F_CCI: n = 3; break;
-    case F_AD: case F_ADOSC: case F_MFI: case F_CDL: case F_AVGPRICE: n = 4; break;
-    default: n = 0;
-  }
-  for (int i = 0; i < n; ++i) m |= 1u << j.in[i];
-  return m;
-}
-
-int job_lines(const Job& j) {
-  switch (j.family) {
-    case F_MACD: case F_ADX: case F_DX: case F_STOCH: return 1;
-    case F_ADOSC: return 2;
-    case F_DEMA: return 2;
-    case F_TEMA: return 3;
-    case F_T3: return 4;
-    default: return 0;
-  }
-}
 
 template <int K>
 SmemLayout make_layout(const Launch& L, int warps) {
@@ -617,94 +441,6 @@ cudaError_t launch_k(Launch& L, const SchedulePlan& plan, cudaStream_t stream, L
   }
   return cudaGetLastError();
 }
-
-#ifndef TB_PREC_TU
-cudaError_t launch_sp(Launch& L, const SchedulePlan& plan, cudaStream_t stream, LaunchStats* stats) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  DeviceInfo& di = device_info(dev);
-  const int J = L.njobs;
-  int G = plan.groups > 0 ? plan.groups : std::max(1, 8 / J);
-  while (G > 1 && G * J > 24) --G;
-  if (G * J > 24) return cudaErrorInvalidConfiguration;
-  sp::Layout lay{};
-  lay.J = J;
-  lay.H = max_lookback_halo(L);
-  lay.RS = lay.H + sp::C + 1;
-  if ((lay.RS & 1) == 0) lay.RS += 1;
-  int slots = 0;
-  for (int p = 0; p < P_COUNT; ++p) {
-    lay.plane_slot[p] = (L.plane_mask & (1u << p)) ? slots : -1;
-    if (L.plane_mask & (1u << p)) lay.slot_plane[slots++] = p;
-  }
-  lay.nplanes = slots;
-  lay.cdl_first = -1;
-  lay.cdl_count = 0;
-  for (int j = 0; j < J; ++j)
-    if (L.jobs[j].family == F_CDL) {
-      if (lay.cdl_first < 0) lay.cdl_first = j;
-      ++lay.cdl_count;
-    }
-  for (;;) {
-    lay.G = G;
-    lay.in_bytes = G * lay.nplanes * 32 * lay.RS * 4;
-    int off = 2 * lay.in_bytes + G * 32 * 16 + 16;
-    off = (off + 15) & ~15;
-    lay.cdl_table_bytes = lay.cdl_count > 0 ? 4 * 32 * (sp::C + sp::kCdlBack) * 8 : 0;
-    lay.cdl_table_off = off;
-    off += G * lay.cdl_table_bytes;
-    for (int w = 0; w < G * J; ++w) {
-      const Job& jb = L.jobs[w % J];
-      const bool line = jb.family == F_STOCH || jb.family == F_CCI || jb.family == F_MFI;
-      const int nout = jb.family == F_CDL ? 1 : (jb.family == F_MACD || jb.family == F_BBANDS ? 3 : (jb.family == F_STOCH ? 2 : 1));
-      lay.warp_off[w] = off;
-      lay.warp_tp[w] = line ? 1 : 0;
-      off += nout * 32 * (sp::C + 1) * 4;
-      off = (off + 15) & ~15;
-      lay.warp_line[w] = off;
-      if (line) off += 32 * lay.RS * 8;
-      off = (off + 15) & ~15;
-    }
-    lay.total = off;
-    if (lay.total <= di.smem_optin || G == 1) break;
-    G = std::max(1, G / 2);
-  }
-  if (lay.total > di.smem_optin) return cudaErrorInvalidConfiguration;
-  const int threads = 32 * G * J;
-  int per_sm = -1;
-  {
-    std::lock_guard<std::mutex> lk(g_mutex);
-    if (!di.sp_attr) {
-      e = cudaFuncSetAttribute(sp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, di.smem_optin);
-      if (e != cudaSuccess) return e;
-      di.sp_attr = true;
-    }
-    for (const OccEntry& o : di.occ)
-      if (o.k == -1 && o.warps == G * J && o.smem == lay.total) per_sm = o.per_sm;
-    if (per_sm < 0) {
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sp_kernel, threads, lay.total);
-      if (e != cudaSuccess) return e;
-      di.occ.push_back({-1, G * J, lay.total, per_sm});
-    }
-  }
-  if (per_sm < 1) return cudaErrorInvalidConfiguration;
-  const long long ngs = ((long long)L.S + 32 * G - 1) / (32 * G);
-  long long cap = (long long)per_sm * di.sms;
-  if (plan.max_blocks > 0) cap = std::min<long long>(cap, plan.max_blocks);
-  const int blocks = (int)std::max<long long>(1, std::min(ngs, cap));
-  sp_kernel<<<blocks, threads, lay.total, stream>>>(L, lay);
-  if (stats) {
-    stats->blocks = blocks;
-    stats->warps_per_block = G * J;
-    stats->smem_per_block = lay.total;
-    stats->k = 0;
-    stats->blocks_per_sm = per_sm;
-  }
-  return cudaGetLastError();
-}
-
-#endif  // TB_PREC_TU
 
 }  // namespace
 
@@ -946,7 +682,6 @@ cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, long long total_ba
   L.need_tp = need_tp;
   const int h = max_lookback_halo(L);
   L.halo = ((h + 31) / 32) * 32;
-  if (plan.mode == 1 && !(L.njobs > 0 && L.jobs[0].prec != 0)) return launch_sp(L, plan, stream, stats);
   // candle jobs go to the bar-parallel tile kernel, the rest to the engine
   int ncdl = 0;
   Job cdl_jobs[kMaxJobs];
@@ -963,6 +698,8 @@ cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, long long total_ba
     return launch_candles(L, cdl_jobs, ncdl, stream);
   }
   L.lb = 0;
+  // row-parallel engine; job sets it does not take run on the warp-scan engine
+  if (plan.mode == 1 && rows::supports(L, L.max_len)) return rows::launch(L, L.max_len, stream, stats);
   if (L.njobs > 0 && L.jobs[0].prec != 0) return launch_prec(L, plan, total_bars, stream, stats);
   if (has_ext_family(L)) return launch_ext(L, plan, total_bars, stream, stats);
   if (plan.mode == 2) {

@@ -49,6 +49,7 @@ struct Launch {
   const long long* offsets;  // ragged row starts (S+1 entries) or nullptr
   const int* order;          // processing order of series (longest first) or nullptr
   long long T;               // uniform row length when offsets == nullptr
+  long long max_len;         // longest row of the batch
   int S;
   int njobs;
   int halo;                  // multiple of 32, >= every job's halo

@@ -229,14 +229,6 @@ __device__ __forceinline__ double stage_round(const Ctx<K>& c, int f, const Stag
   return tail;
 }
 
-__host__ __device__ inline void talib_ema_coeffs(int p, double& beta, double& k) {
-  double b = (double)(p - 1) / (double)(p + 1);
-  double kk = 1.0 - b;
-  if (b < 0.5) b = 1.0 - kk;
-  beta = b;
-  k = kk;
-}
-
 // EMA(p): talib08:5546-5627 TA_EMA; leading NaNs skipped (BatchFused.cu:34-41).
 // fp[0] = beta, fp[1] = k (host-precomputed TA-Lib coefficients).
 // RMA(p) is the same stage (talib08:13614-13683 TA_RMA: mean seed, then

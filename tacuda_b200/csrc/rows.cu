@@ -1,0 +1,324 @@
+// Row-parallel engine: kernel and launcher (see rows.cuh for the design).
+#include "rows.cuh"
+
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "jobs.h"
+#include "scheduler.h"
+
+namespace tb {
+namespace rows {
+
+// Per-warp history line (entries per lane, a power of two; 0: none).
+__host__ __device__ inline int line_entries(const Job& j) {
+  int need = 0;
+  switch (j.family) {
+    case F_WILLR: need = j.ip[0]; break;
+    case F_STOCH: need = j.ip[0] > j.ip[1] ? j.ip[0] : j.ip[1]; break;
+    case F_CCI: case F_MFI: need = j.ip[0] + 1; break;
+    default: return 0;
+  }
+  int cap = 1;
+  while (cap < need) cap <<= 1;
+  return cap;
+}
+
+__host__ __device__ inline int line_bytes(const Job& j) {
+  const int cap = line_entries(j);
+  switch (j.family) {
+    case F_WILLR: return 2 * 32 * cap * 4;
+    case F_STOCH: return 4 * 32 * cap * 4;
+    case F_CCI: return 32 * cap * 8;
+    case F_MFI: return 2 * 32 * cap * 8;
+    default: return 0;
+  }
+}
+
+__host__ __device__ inline int out_count(int family) {
+  return family == F_MACD || family == F_BBANDS ? 3 : (family == F_STOCH ? 2 : 1);
+}
+
+__device__ void run_job(const Warp& w, const Job& j, unsigned char* line) {
+  const int cap = line_entries(j);
+  const bool f32 = j.ip[0] <= kFp32MaxPeriod;
+  switch (j.family) {
+    case F_SMA: w_sum_window(w, j, 0); break;
+    case F_SUM: w_sum_window(w, j, 1); break;
+    case F_WMA: w_sum_window(w, j, 2); break;
+    case F_BBANDS: w_moment_window(w, j, 0); break;
+    case F_STDDEV: w_moment_window(w, j, 1); break;
+    case F_VAR: w_moment_window(w, j, 2); break;
+    case F_WILLR: w_willr(w, j, reinterpret_cast<float*>(line), cap); break;
+    case F_STOCH: w_stoch(w, j, reinterpret_cast<float*>(line), cap); break;
+    case F_CCI: w_cci(w, j, reinterpret_cast<double*>(line), cap); break;
+    case F_MFI: w_mfi(w, j, reinterpret_cast<double*>(line), cap); break;
+    case F_EMA: case F_RMA:
+      if (f32) w_ema<float>(w, j); else w_ema<double>(w, j);
+      break;
+    case F_RSI:
+      if (f32) w_rsi<float>(w, j); else w_rsi<double>(w, j);
+      break;
+    case F_MACD: w_macd(w, j); break;
+    case F_ATR:
+      if (f32) w_atr<float>(w, j, 0); else w_atr<double>(w, j, 0);
+      break;
+    case F_NATR:
+      if (f32) w_atr<float>(w, j, 1); else w_atr<double>(w, j, 1);
+      break;
+    case F_TRANGE: w_atr<float>(w, j, 2); break;
+    case F_ADX:
+      if (f32) w_adx<float>(w, j, true); else w_adx<double>(w, j, true);
+      break;
+    case F_DX: w_adx<double>(w, j, false); break;
+    case F_OBV: w_volume(w, j, 0); break;
+    case F_AD: w_volume(w, j, 1); break;
+    case F_ADOSC: w_volume(w, j, 2); break;
+    case F_DEMA: w_cascade(w, j, 2); break;
+    case F_TEMA: w_cascade(w, j, 3); break;
+    case F_T3: w_cascade(w, j, 6); break;
+    case F_LINEARREG: w_linreg(w, j); break;
+    case F_CORREL: w_correl(w, j); break;
+    case F_MIN: w_minmax(w, j, false, false); break;
+    case F_MAX: w_minmax(w, j, true, false); break;
+    case F_MIDPOINT: w_minmax(w, j, false, true); break;
+    case F_ROC: w_roc(w, j, 0); break;
+    case F_ROCP: w_roc(w, j, 1); break;
+    case F_ROCR: w_roc(w, j, 2); break;
+    case F_ROCR100: w_roc(w, j, 3); break;
+    case F_MOM: w_roc(w, j, 4); break;
+    case F_MEDPRICE: w_price(w, j, 0); break;
+    case F_TYPPRICE: w_price(w, j, 1); break;
+    case F_AVGPRICE: w_price(w, j, 2); break;
+    case F_WCLPRICE: w_price(w, j, 3); break;
+    case F_MIDPRICE: w_midprice(w, j); break;
+    case F_RMEAN: w_rolling(w, j, 0); break;
+    case F_RMAX: w_rolling(w, j, 1); break;
+    case F_RMIN: w_rolling(w, j, 2); break;
+    case F_RSTD: w_rolling(w, j, 3); break;
+    case F_IBS: w_talib_bar(w, j, 0); break;
+    case F_MARKETFI: w_talib_bar(w, j, 1); break;
+    case F_QSTICK: w_qstick(w, j); break;
+    default:
+      // unreachable: the launcher admits only the families above
+      for (int c = 0; c < w.nchunks; ++c) {
+        if (!w.wait(c)) return;
+        w.release(c);
+      }
+  }
+}
+
+// Producer warp: stages chunk c of every plane for the 32 rows once the job
+// warps have released the chunk that last used its slot.
+__device__ void produce(const Launch& L, const Layout& lay, unsigned char* smem, uint64_t* full, uint64_t* empty,
+                        const long long* tbase, const long long* tn, volatile int* abort_flag, int* err,
+                        int nchunks, int lane) {
+  float* ring = reinterpret_cast<float*>(smem + lay.ring_off);
+  const int NS = lay.NS, Hs = lay.Hs, RS = lay.RS;
+  for (int c = 0; c < nchunks; ++c) {
+    const int s = c % NS, use = c / NS;
+    if (use > 0 && !mbar_wait(&empty[s], (unsigned)((use - 1) & 1), abort_flag, err, lane)) break;
+    const long long t = (long long)c * C + lane;
+    const bool mir = s >= NS - Hs;
+    const int off = (Hs + s) * C + lane, moff = (s - (NS - Hs)) * C + lane;
+    for (int q = 0; q < lay.nplanes; ++q) {
+      const float* src = L.plane[lay.slot_plane[q]];
+      float* dst = ring + (size_t)q * 32 * RS;
+#pragma unroll 4
+      for (int i = 0; i < 32; ++i) {
+        const long long b = tbase[i];
+        const bool ok = b >= 0 && t < tn[i];
+        const float* sp = ok ? src + b + t : src;
+        cp_async4(dst + i * RS + off, sp, ok);
+        if (mir) cp_async4(dst + i * RS + moff, sp, ok);
+      }
+    }
+    cp_async_arrive(&full[s]);
+  }
+  cp_async_wait_all();
+}
+
+__device__ int g_rows_err;  // sticky: a wait of the engine ran out on this device
+
+__global__ void __launch_bounds__(32 * (kMaxConsumers + 1), 1) rows_kernel(const __grid_constant__ Launch L, const __grid_constant__ Layout lay) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + lay.bar_off);
+  uint64_t* empty = full + lay.NS;
+  long long* tbase = reinterpret_cast<long long*>(smem + lay.tab_off);
+  long long* tn = tbase + 32;
+  int* misc = reinterpret_cast<int*>(tn + 32);  // [0] longest row of the group, [1] abort
+  int* err = L.err ? L.err : &g_rows_err;
+  if (warp == 0) {
+    const long long idx = (long long)blockIdx.x * 32 + lane;
+    long long b = -1, n = 0;
+    if (idx < L.S) {
+      const int s = L.order ? L.order[idx] : (int)idx;
+      if (L.offsets) {
+        b = L.offsets[s];
+        n = L.offsets[s + 1] - b;
+      } else {
+        b = (long long)s * L.T;
+        n = L.T;
+      }
+    }
+    tbase[lane] = b;
+    tn[lane] = n;
+    const int m = warp_max_int((int)min(n, (long long)INT_MAX));
+    if (lane == 0) {
+      misc[0] = m;
+      misc[1] = 0;
+      for (int s = 0; s < lay.NS; ++s) {
+        mbar_init(&full[s], 32);
+        mbar_init(&empty[s], (unsigned)lay.nconsumers);
+      }
+      asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+  }
+  __syncthreads();
+  const int maxn = misc[0];
+  const int nchunks = (maxn + C - 1) / C;
+  volatile int* abort_flag = misc + 1;
+  if (warp == lay.nconsumers) {
+    produce(L, lay, smem, full, empty, tbase, tn, abort_flag, err, nchunks, lane);
+    return;
+  }
+  if (warp > lay.nconsumers) return;
+  Warp w;
+  w.smem = smem;
+  w.lay = &lay;
+  w.full = full;
+  w.empty = empty;
+  w.tbase = tbase;
+  w.tn = tn;
+  w.abort_flag = abort_flag;
+  w.err = err;
+  w.stage = reinterpret_cast<float*>(smem + lay.stage_off[warp]);
+  w.lane = lane;
+  w.nchunks = nchunks;
+  w.maxn = maxn;
+  w.Hs = lay.Hs;
+  w.NS = lay.NS;
+  w.RS = lay.RS;
+  w.n = tn[lane];
+  run_job(w, L.jobs[lay.warp_job[warp]], smem + lay.line_off[warp]);
+}
+
+namespace {
+
+bool family_supported(int f) {
+  switch (f) {
+    case F_SMA: case F_SUM: case F_WMA: case F_BBANDS: case F_STDDEV: case F_VAR: case F_WILLR: case F_STOCH:
+    case F_CCI: case F_MFI: case F_EMA: case F_RMA: case F_RSI: case F_MACD: case F_ATR: case F_NATR:
+    case F_TRANGE: case F_ADX: case F_DX: case F_OBV: case F_AD: case F_ADOSC: case F_DEMA: case F_TEMA:
+    case F_T3: case F_LINEARREG: case F_CORREL: case F_MIN: case F_MAX: case F_MIDPOINT: case F_ROC:
+    case F_ROCP: case F_ROCR: case F_ROCR100: case F_MOM: case F_MEDPRICE: case F_TYPPRICE: case F_AVGPRICE:
+    case F_WCLPRICE: case F_MIDPRICE: case F_RMEAN: case F_RMAX: case F_RMIN: case F_RSTD: case F_IBS:
+    case F_MARKETFI: case F_QSTICK:
+      return true;
+    default:
+      return false;
+  }
+}
+
+// bars of history a job reads before a chunk: one more than its lookback halo
+// (the bar leaving a running window, the previous close)
+int rows_halo(const Job& j) { return job_halo(j) + 1; }
+
+struct DevState {
+  int sms = 0, smem_optin = 0;
+  bool attr = false;
+};
+std::mutex g_mutex;
+std::vector<DevState> g_dev;
+
+}  // namespace
+
+bool supports(const Launch& L, long long max_len) {
+  if (L.njobs < 1 || L.njobs > kMaxConsumers || L.st_carry) return false;
+  if (max_len > (1ll << 30)) return false;
+  for (int j = 0; j < L.njobs; ++j) {
+    const Job& jb = L.jobs[j];
+    if (jb.prec != 0 || !family_supported(jb.family)) return false;
+    if (rows_halo(jb) > kMaxHalo) return false;
+    if (line_entries(jb) > kMaxLine) return false;
+  }
+  return true;
+}
+
+cudaError_t launch(Launch& L, long long max_len, cudaStream_t stream, LaunchStats* stats) {
+  if (!supports(L, max_len)) return cudaErrorNotSupported;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  DevState* ds;
+  {
+    std::lock_guard<std::mutex> lk(g_mutex);
+    if ((int)g_dev.size() <= dev) g_dev.resize(dev + 1);
+    ds = &g_dev[dev];
+    if (ds->sms == 0) {
+      cudaDeviceGetAttribute(&ds->sms, cudaDevAttrMultiProcessorCount, dev);
+      cudaDeviceGetAttribute(&ds->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    }
+    if (!ds->attr) {
+      e = cudaFuncSetAttribute(rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, ds->smem_optin);
+      if (e != cudaSuccess) return e;
+      ds->attr = true;
+    }
+  }
+  Layout lay;
+  std::memset(&lay, 0, sizeof(lay));
+  unsigned mask = 0;
+  int H = 1;
+  for (int j = 0; j < L.njobs; ++j) {
+    mask |= job_planes(L.jobs[j]);
+    H = std::max(H, rows_halo(L.jobs[j]));
+  }
+  int np = 0;
+  for (int p = 0; p < P_COUNT; ++p) {
+    lay.plane_slot[p] = (mask & (1u << p)) ? np : -1;
+    if (mask & (1u << p)) lay.slot_plane[np++] = p;
+  }
+  lay.nplanes = np;
+  lay.Hs = std::max(1, (H + C - 1) / C);
+  lay.NS = lay.Hs + 2;
+  lay.RS = (lay.Hs + lay.NS) * C + 1;
+  int off = 0;
+  lay.ring_off = off;
+  off += np * 32 * lay.RS * 4;
+  off = (off + 15) & ~15;
+  lay.bar_off = off;
+  off += 2 * lay.NS * 8;
+  lay.tab_off = off;
+  off += 64 * 8 + 16;
+  lay.nconsumers = L.njobs;
+  for (int w = 0; w < L.njobs; ++w) {
+    lay.warp_job[w] = w;
+    off = (off + 15) & ~15;
+    lay.stage_off[w] = off;
+    off += out_count(L.jobs[w].family) * 32 * (C + 1) * 4;
+    off = (off + 15) & ~15;
+    lay.line_off[w] = off;
+    off += line_bytes(L.jobs[w]);
+  }
+  lay.total = (off + 127) & ~127;
+  if (lay.total > ds->smem_optin) return cudaErrorNotSupported;
+  const long long groups = ((long long)L.S + 31) / 32;
+  if (groups > INT_MAX) return cudaErrorInvalidValue;
+  const int threads = 32 * (L.njobs + 1);
+  rows_kernel<<<(unsigned)groups, threads, lay.total, stream>>>(L, lay);
+  if (stats) {
+    stats->blocks = (int)groups;
+    stats->warps_per_block = L.njobs + 1;
+    stats->smem_per_block = lay.total;
+    stats->k = 0;
+    stats->blocks_per_sm = 1;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace rows
+}  // namespace tb

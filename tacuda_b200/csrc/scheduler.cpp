@@ -1,11 +1,10 @@
 // Launch planner and autotuner cache for the batch engine.
 //
-// The heuristic picks the round width from the batch shape: rows of at most
-// 128 bars use K = 4 bars per lane, others K = 8 (two blocks per SM), and the
-// look-back engine for few long rows K = 16 (K = 4 when the batch holds fewer
-// than 1024 tiles of 512 bars).
-// Candle jobs run on their own bar-parallel kernel unless the series-parallel
-// engine is forced (it evaluates them in the same pass).
+// The heuristic picks the engine from the batch shape: the row-parallel engine
+// when the rows are at most 4x as long as there are rows, the look-back engine
+// for few long rows (K = 16 bars per lane, K = 4 for uniform rows of up to
+// 2^17 bars), the warp-scan engine (K = 8) otherwise.
+// Candle jobs run on their own bar-parallel kernel.
 // Measured plans (ct_b200_autotune) override it; they are keyed by a coarse
 // shape histogram (log2 of the series count, mean and max length) plus a hash
 // of the job set, kept in memory and optionally in the file named by
@@ -74,26 +73,32 @@ SchedulePlan plan_for(const Launch& L, long long total_bars, long long max_len) 
       if (e.first == key) return e.second;
   }
   SchedulePlan p;
-  const long long mean = L.S > 0 ? total_bars / L.S : 0;
-  // K = 8 runs two blocks per SM and beat K = 16 on long ragged rows too
-  p.k = max_len <= 128 ? 4 : 8;
-  (void)mean;
+  // Engine by batch shape, as the reference's dispatcher picks its fused path
+  // when seriesLen <= 4 * numSeries (src/api/BatchFused.cu:158-176):
+  //  * row-parallel: a thread per row and job; every row walks its bars in
+  //    TA-Lib's order, with no scans;
+  //  * look-back: few long rows, rounds of one row on different warps chained
+  //    by decoupled look-back;
+  //  * warp-scan otherwise: a warp per row, a round's bars split over lanes.
+  // Within an engine the round width is fixed (the look-back engine's depends
+  // on the row length of a uniform batch only), so a row's bits depend on the
+  // engine and its own data, never on the other rows of the batch.
+  p.k = 8;
   p.warps_per_block = 8;
-  // A warp per series splitting each round across its lanes; when there are
-  // too few series to fill the GPU and they span many rounds, rounds of one
-  // series go to different warps chained by decoupled look-back (512-bar
-  // rounds: fewer tiles and hops).
   p.mode = 0;
-  if (L.S < 1024 && max_len >= 8ll * 32 * 16) {
+  if (max_len <= 4ll * L.S) {
+    p.mode = 1;
+  } else if (L.S < 1024 && max_len >= 8ll * 32 * 16) {
     p.mode = 2;
     p.k = 16;
-    // Fewer than 1024 tiles of 512 bars leave the GPU nearly idle and the
-    // call latency-bound: 128-bar tiles put 4x more warps on it
-    // (1 x 100,000 bars, SMA EMA RSI MACD: 123 -> 113 us).
-    if (total_bars < 1024ll * 512) p.k = 4;
+    // One row of up to 2^17 bars per series of a uniform batch is latency-
+    // bound: 128-bar tiles put 4x more warps on it (1 x 100,000 bars,
+    // SMA EMA RSI MACD: 123 -> 113 us).
+    const bool uniform = total_bars == max_len * (long long)L.S;
+    if (uniform && max_len <= (1ll << 17)) p.k = 4;
   }
   if (const char* e = std::getenv("TACUDA_B200_MODE")) {
-    if (std::strcmp(e, "sp") == 0) p.mode = 1;
+    if (std::strcmp(e, "sp") == 0 || std::strcmp(e, "rows") == 0) p.mode = 1;
     if (std::strcmp(e, "ws") == 0) p.mode = 0;
     if (std::strcmp(e, "lb") == 0) p.mode = 2;
   }

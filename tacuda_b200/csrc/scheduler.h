@@ -42,6 +42,13 @@ cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, long long total_ba
                          LaunchStats* stats);
 int max_lookback_halo(const Launch& L);
 
+namespace rows {
+// Row-parallel engine (rows.cu): whether it takes this job set and batch, and
+// its launch. Returns cudaErrorNotSupported for job sets it does not take.
+bool supports(const Launch& L, long long max_len);
+cudaError_t launch(Launch& L, long long max_len, cudaStream_t stream, LaunchStats* stats);
+}  // namespace rows
+
 // Look-back launch with its scratch in a static device array of
 // kStaticLookbackBytes per device (allocation-free). Uniform rows, no candle
 // jobs. Returns cudaErrorInvalidValue when the scratch it needs (*need bytes)
