@@ -470,6 +470,17 @@ CTAPI_EXPORT ctStatus_t ct_b200_alpha_backward_d(const float* d_close, const flo
  * (diagnostics; the batch entry points issue one each). */
 CTAPI_EXPORT unsigned long long ct_b200_launch_count(void);
 
+/* Errors of asynchronous calls (no counterpart in the reference, whose
+ * asynchronous calls report nothing after their launch). Every wait inside
+ * this library's kernels is bounded; one that runs out sets an error word of
+ * the current device and the kernel returns with outputs that are not valid.
+ * Calls with stream == 0 (and the host-matrix calls) read the word after
+ * their synchronisation and fail with CT_STATUS_KERNEL_FAILED. For calls on
+ * other streams: synchronise them, then this call stores the word in *flags
+ * (0: no wait ran out; bit 0: a wait ran out) and clears it. The word is per
+ * device, shared by all threads and streams using it. */
+CTAPI_EXPORT ctStatus_t ct_b200_take_device_error(int* flags);
+
 #ifdef __cplusplus
 }
 #endif

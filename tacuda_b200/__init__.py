@@ -74,6 +74,7 @@ def _load() -> ct.CDLL:
     lib.ct_b200_cdl_name.argtypes = [_I]
     lib.ct_b200_cdl_lookback.argtypes = [_I]
     lib.ct_b200_launch_count.restype = ct.c_ulonglong
+    lib.ct_b200_take_device_error.argtypes = [ct.POINTER(_I)]
     lib.ct_b200_fused_batch_d.argtypes = [ct.POINTER(ctB200Series), ct.POINTER(ctB200Job), _I, _P]
     lib.ct_b200_fused_batch.argtypes = [ct.POINTER(ctB200Series), ct.POINTER(ctB200Job), _I, _P]
     lib.ct_b200_plan_create.argtypes = [ct.POINTER(ctB200Job), _I, _P, _I, ct.c_int64, ct.POINTER(_P)]
@@ -134,6 +135,14 @@ def cdl_lookback(k: int) -> int:
 
 def launch_count() -> int:
     return int(get_lib().ct_b200_launch_count())
+
+
+def take_device_error() -> int:
+    """Read and clear the current device's error word (bit 0: a bounded wait
+    of an engine ran out since the last read); ct_b200_take_device_error."""
+    flags = ct.c_int(0)
+    call_status(get_lib().ct_b200_take_device_error(ct.byref(flags)), "ct_b200_take_device_error")
+    return int(flags.value)
 
 
 def stream_arg(value: Any) -> ct.c_void_p:

@@ -79,8 +79,16 @@ def build_library(verbose: bool = False) -> Path:
     return OUT
 
 
+# The reference tree the oracle's reference builds compile from, where it exists
+# (only in the build container; the GPU box uses the prebuilt oracle/_ref files).
+REFERENCE_TREE = Path(os.environ.get("TACUDA_REFERENCE_TREE", "/root/reference"))
+
+
 def build_oracle() -> None:
-    _run(["make", "-s", "-C", str(ROOT / "oracle")])
+    cmd = ["make", "-s", "-C", str(ROOT / "oracle")]
+    if REFERENCE_TREE.is_dir():
+        cmd.append(f"REF={REFERENCE_TREE}")
+    _run(cmd)
 
 
 if __name__ == "__main__":

@@ -188,11 +188,30 @@ ctStatus_t check_planes(const Launch& L, const char* who) {
   return CT_STATUS_SUCCESS;
 }
 
-ctStatus_t finish(cudaStream_t stream, const char* who) {
-  if (stream == 0) {
-    const cudaError_t e = cudaStreamSynchronize(0);
+// Synchronise `stream` and report a bounded wait of an engine that ran out
+// meanwhile: the per-device error word is read into a pinned per-thread slot
+// on the same stream, before the synchronisation, and cleared when set.
+ctStatus_t sync_and_check(cudaStream_t stream, const char* who) {
+  thread_local int* slot = nullptr;
+  if (!slot && cudaMallocHost(reinterpret_cast<void**>(&slot), sizeof(int)) != cudaSuccess) slot = nullptr;
+  int* sticky = tb::sticky_word();
+  if (slot && sticky) {
+    *slot = 0;
+    const cudaError_t e = cudaMemcpyAsync(slot, sticky, sizeof(int), cudaMemcpyDeviceToHost, stream);
     if (e != cudaSuccess) return cuda_fail(CT_STATUS_DEVICE_ERROR, who, e);
   }
+  const cudaError_t e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return cuda_fail(CT_STATUS_DEVICE_ERROR, who, e);
+  if (slot && sticky && *slot != 0) {
+    cudaMemset(sticky, 0, sizeof(int));
+    return fail(CT_STATUS_KERNEL_FAILED,
+                std::string(who) + ": a bounded wait of the engine ran out; the outputs are not valid");
+  }
+  return CT_STATUS_SUCCESS;
+}
+
+ctStatus_t finish(cudaStream_t stream, const char* who) {
+  if (stream == 0) return sync_and_check(0, who);
   return CT_STATUS_SUCCESS;
 }
 
@@ -200,6 +219,9 @@ ctStatus_t launch(Launch& L, long long total, long long maxlen, const tb::Schedu
                   const char* who, tb::LaunchStats* stats = nullptr) {
   const tb::SchedulePlan plan = forced ? *forced : tb::plan_for(L, total, maxlen);
   L.max_len = maxlen;
+  // test knob: one bounded wait of the launch is made to run out (see
+  // Launch::stall_test); the call then reports CT_STATUS_KERNEL_FAILED
+  if (const char* e = std::getenv("TACUDA_B200_TEST_STALL")) L.stall_test = std::atoi(e) != 0;
   const cudaError_t e = tb::launch_batch(L, plan, total, stream, stats);
   if (e != cudaSuccess) return cuda_fail(CT_STATUS_KERNEL_FAILED, who, e);
   g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -320,6 +342,14 @@ const char* ct_status_string(ctStatus_t s) {
 const char* ct_get_last_error(void) { return t_last_error.c_str(); }
 const char* ct_version(void) { return "0.9.3-b200"; }
 unsigned long long ct_b200_launch_count(void) { return g_launches.load(); }
+
+ctStatus_t ct_b200_take_device_error(int* flags) {
+  clear_error();
+  if (!flags) return fail(CT_STATUS_INVALID_ARGUMENT, "ct_b200_take_device_error: null pointer");
+  const cudaError_t e = tb::take_sticky_error(flags);
+  if (e != cudaSuccess) return cuda_fail(CT_STATUS_DEVICE_ERROR, "ct_b200_take_device_error", e);
+  return CT_STATUS_SUCCESS;
+}
 
 // ------------------------------------------------------------ batch API
 
@@ -806,6 +836,7 @@ ctStatus_t ct_b200_fused_lookback_static_d(const ctB200Series* series, const ctB
   }
   tb::SchedulePlan plan = tb::plan_for(L, L.T * (long long)L.S, L.T);
   plan.mode = 2;
+  if (const char* e = std::getenv("TACUDA_B200_TEST_STALL")) L.stall_test = std::atoi(e) != 0;
   size_t need = 0;
   const cudaError_t e = tb::launch_lookback_static(L, plan, stream, &need);
   if (e == cudaErrorInvalidValue && need > tb::kStaticLookbackBytes) {
@@ -1018,9 +1049,7 @@ ctStatus_t ct_b200_fused_batch(const ctB200Series* hs, const ctB200Job* hjobs, i
   release();
   if (st != CT_STATUS_SUCCESS) return st;
   if (copy_err) return fail(CT_STATUS_COPY_FAILED, std::string(who) + copy_err);
-  const cudaError_t e = cudaStreamSynchronize(stream);
-  if (e != cudaSuccess) return cuda_fail(CT_STATUS_DEVICE_ERROR, who, e);
-  return CT_STATUS_SUCCESS;
+  return sync_and_check(stream, who);
 }
 
 // ------------------------------------------------------------ stream batches
@@ -1203,8 +1232,8 @@ ctStatus_t stream_append(ctStreamBatch* b, int family, const float* const* ins, 
     return fail(CT_STATUS_COPY_FAILED, std::string(who) + ": history copy failed");
   }
   tb::scratch_free(dout, stream);
-  const cudaError_t es = cudaStreamSynchronize(stream);
-  if (es != cudaSuccess) return cuda_fail(CT_STATUS_DEVICE_ERROR, who, es);
+  const ctStatus_t ss = sync_and_check(stream, who);
+  if (ss != CT_STATUS_SUCCESS) return ss;
   b->cur ^= 1;
   b->seen += n;
   return CT_STATUS_SUCCESS;
@@ -1571,9 +1600,7 @@ static ctStatus_t host_run(const std::vector<const float*>& hin, const std::vect
   for (size_t i = 0; i < hout.size(); ++i)
     if (cudaMemcpyAsync(hout[i], dout[i], n * 4, cudaMemcpyDeviceToHost, s2) != cudaSuccess) { release(); return fail(CT_STATUS_COPY_FAILED, std::string(who) + ": copy failed"); }
   release();
-  const cudaError_t e = cudaStreamSynchronize(s2);
-  if (e != cudaSuccess) return cuda_fail(CT_STATUS_DEVICE_ERROR, who, e);
-  return CT_STATUS_SUCCESS;
+  return sync_and_check(s2, who);
 }
 
 struct HostArgs { int len, n, p0, p1, p2, p3; float f0, f1; };

@@ -487,6 +487,22 @@ cudaError_t launch_candles(const Launch& L, const Job* jobs, int n, cudaStream_t
 
 #endif  // TB_PREC_TU
 
+// A look-back wait that ran out in this launch also sets the per-device error
+// word, so that calls on any stream can report it.
+static __global__ void fold_error_kernel(const int* err, int* sticky) {
+  if (*err) atomicOr(sticky, 1);
+}
+
+// Test knob (Launch::stall_test): tile 0 is never taken, so the tiles that
+// wait for it run out after a short limit instead of two seconds.
+static cudaError_t lookback_stall(unsigned long long* counter, int* err, cudaStream_t stream) {
+  static const unsigned long long one = 1;
+  static const int limit = 64;
+  cudaError_t e = cudaMemcpyAsync(counter, &one, sizeof(one), cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(err + 1, &limit, sizeof(limit), cudaMemcpyHostToDevice, stream);
+  return e;
+}
+
 template <int K, int P>
 cudaError_t launch_lookback(Launch& L, const SchedulePlan& plan, long long total_bars, cudaStream_t stream,
                             LaunchStats* stats) {
@@ -529,13 +545,11 @@ cudaError_t launch_lookback(Launch& L, const SchedulePlan& plan, long long total
       lb_tile_start_kernel<<<1, 1024, 0, stream>>>(L.offsets, L.S, TILE, L.lb_tile_start);
       e = cudaGetLastError();
     }
+    if (e == cudaSuccess && L.stall_test) e = lookback_stall(L.lb_counter, L.err, stream);
     if (e == cudaSuccess) e = launch_k<K, P>(L, plan, stream, stats);
-    if (e == cudaSuccess && stream == 0) {
-      // synchronous calls report a look-back wait that ran out
-      int herr = 0;
-      e = cudaMemcpyAsync(&herr, L.err, sizeof(int), cudaMemcpyDeviceToHost, stream);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-      if (e == cudaSuccess && herr != 0) e = cudaErrorLaunchTimeout;
+    if (e == cudaSuccess && L.sticky) {
+      fold_error_kernel<<<1, 1, 0, stream>>>(L.err, L.sticky);
+      e = cudaGetLastError();
     }
   }
   const cudaError_t ef = scratch_free(scratch, stream);
@@ -585,6 +599,41 @@ bool has_ext_family(const Launch& L) {
   for (int j = 0; j < L.njobs; ++j)
     if (L.jobs[j].family > F_CDL) return true;
   return false;
+}
+
+// Per-device error word: every engine sets bit 0 when one of its bounded
+// waits runs out (the look-back engine through fold_error_kernel, the
+// row-parallel engine directly). Synchronous calls read and clear it after
+// their synchronisation; ct_b200_take_device_error does for any caller.
+__device__ int g_sticky_err;
+
+namespace {
+std::mutex g_sticky_mutex;
+std::vector<int*> g_sticky_ptr;  // per device
+}  // namespace
+
+int* sticky_word() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lk(g_sticky_mutex);
+  if ((int)g_sticky_ptr.size() <= dev) g_sticky_ptr.resize(dev + 1, nullptr);
+  if (!g_sticky_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_sticky_err) != cudaSuccess) return nullptr;
+    g_sticky_ptr[dev] = static_cast<int*>(p);
+  }
+  return g_sticky_ptr[dev];
+}
+
+cudaError_t take_sticky_error(int* value) {
+  *value = 0;
+  int* p = sticky_word();
+  if (!p) return cudaErrorInvalidDevice;
+  int v = 0;
+  cudaError_t e = cudaMemcpy(&v, p, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && v != 0) e = cudaMemset(p, 0, sizeof(int));
+  *value = v;
+  return e;
 }
 
 // Look-back scratch of the allocation-free entry point: a file-scope device
@@ -640,18 +689,19 @@ cudaError_t launch_lookback_static_k(Launch& L, const SchedulePlan& plan, cudaSt
   L.lb_desc = reinterpret_cast<LbDesc*>(scratch + head);
   L.lb_nslots = nslots;
   L.lb_tiles = ntiles;
+  if (L.stall_test) e = lookback_stall(L.lb_counter, L.err, stream);
+  if (e != cudaSuccess) return e;
   e = has_ext_family(L) ? launch_ext_k(K, L, plan, stream, nullptr) : launch_k<K>(L, plan, stream, nullptr);
-  if (e == cudaSuccess && stream == 0) {
-    int herr = 0;
-    e = cudaMemcpyAsync(&herr, L.err, sizeof(int), cudaMemcpyDeviceToHost, stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    if (e == cudaSuccess && herr != 0) e = cudaErrorLaunchTimeout;
+  if (e == cudaSuccess && L.sticky) {
+    fold_error_kernel<<<1, 1, 0, stream>>>(L.err, L.sticky);
+    e = cudaGetLastError();
   }
   return e;
 }
 }  // namespace
 
 cudaError_t launch_lookback_static(Launch& L, const SchedulePlan& plan, cudaStream_t stream, size_t* need) {
+  if (!L.sticky) L.sticky = sticky_word();
   unsigned mask = 0;
   int need_tp = 0;
   for (int j = 0; j < L.njobs; ++j) {
@@ -671,6 +721,7 @@ cudaError_t launch_lookback_static(Launch& L, const SchedulePlan& plan, cudaStre
 
 cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, long long total_bars, cudaStream_t stream,
                          LaunchStats* stats) {
+  if (!L.sticky) L.sticky = sticky_word();
   unsigned mask = 0;
   int need_tp = 0;
   for (int j = 0; j < L.njobs; ++j) {

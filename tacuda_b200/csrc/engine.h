@@ -57,7 +57,9 @@ struct Launch {
   int need_tp;               // stage the FP64 typical price ((h+l)+c)/3
   int* sched;                // [0] series counter, [1] finished warps (self-resetting)
   int total_warps;
-  int* err;                  // device error word (0 = ok)
+  int* err;                  // look-back error word of this launch (0 = ok), or nullptr
+  int* sticky;               // per-device error word: bit 0 set when a bounded wait ran out
+  int stall_test;            // test knob: one wait of the launch is made to run out (short limit)
   // look-back mode: series split into one-round tiles taken in order
   int lb;
   unsigned long long* lb_counter;  // next tile (zeroed before the launch)

@@ -35,6 +35,13 @@ constexpr int kLbSpan = 1024;  // 32 groups
 constexpr int kLbAgg = 1, kLbInc = 2;
 constexpr long long kLbSpinLimit = 1ll << 26;  // polls / 32 at up to 1 us each: about two seconds
 
+// The polls a wait makes before giving up: err[1] when the host set it (a test
+// that makes a wait run out), else kLbSpinLimit / 32.
+__device__ __forceinline__ long long lb_spin_limit(const int* err) {
+  const int v = *reinterpret_cast<const volatile int*>(err + 1);
+  return v > 0 ? (long long)v : (kLbSpinLimit >> 5);
+}
+
 __device__ __forceinline__ int lb_load_flag(const LbDesc* d) {
   return *reinterpret_cast<const volatile int*>(&d->flag);
 }
@@ -50,7 +57,7 @@ __device__ __forceinline__ int lb_wait_on(const int* flag, int want, int* err) {
   unsigned ns = 32;
   int v;
   while ((v = *reinterpret_cast<const volatile int*>(flag)) < want) {
-    if (++spins > (kLbSpinLimit >> 5)) {
+    if (++spins > lb_spin_limit(err)) {
       atomicExch(err, 1);
       return 0;
     }
@@ -70,7 +77,7 @@ __device__ __forceinline__ bool lb_wait_all(const int* flag, int want, bool acti
   for (;;) {
     const bool ok = !active || *reinterpret_cast<const volatile int*>(flag) >= want;
     if (__all_sync(kFull, ok)) break;
-    if (++spins > (kLbSpinLimit >> 5)) {
+    if (++spins > lb_spin_limit(err)) {
       if (active) atomicExch(err, 1);
       return false;
     }
@@ -86,7 +93,7 @@ __device__ __forceinline__ int lb_wait(const LbDesc* d, int want, int* err) {
   unsigned ns = 32;
   int v;
   while ((v = lb_load_flag(d)) < want) {
-    if (++spins > (kLbSpinLimit >> 5)) {
+    if (++spins > lb_spin_limit(err)) {
       atomicExch(err, 1);
       return 0;
     }

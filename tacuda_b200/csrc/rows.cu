@@ -19,7 +19,7 @@ __host__ __device__ inline int line_entries(const Job& j) {
   switch (j.family) {
     case F_WILLR: need = j.ip[0]; break;
     case F_STOCH: need = j.ip[0] > j.ip[1] ? j.ip[0] : j.ip[1]; break;
-    case F_CCI: case F_MFI: need = j.ip[0] + 1; break;
+    case F_MFI: need = j.ip[0] + 1; break;
     default: return 0;
   }
   int cap = 1;
@@ -32,7 +32,7 @@ __host__ __device__ inline int line_bytes(const Job& j) {
   switch (j.family) {
     case F_WILLR: return 2 * 32 * cap * 4;
     case F_STOCH: return 4 * 32 * cap * 4;
-    case F_CCI: return 32 * cap * 8;
+    case F_CCI: return (j.ip[0] + 2 * C) * 32 * 8;
     case F_MFI: return 2 * 32 * cap * 8;
     default: return 0;
   }
@@ -53,8 +53,11 @@ __device__ void run_job(const Warp& w, const Job& j, unsigned char* line) {
     case F_STDDEV: w_moment_window(w, j, 1); break;
     case F_VAR: w_moment_window(w, j, 2); break;
     case F_WILLR: w_willr(w, j, reinterpret_cast<float*>(line), cap); break;
-    case F_STOCH: w_stoch(w, j, reinterpret_cast<float*>(line), cap); break;
-    case F_CCI: w_cci(w, j, reinterpret_cast<double*>(line), cap); break;
+    case F_STOCH:
+      if (j.ip[1] == 3) w_stoch<3>(w, j, reinterpret_cast<float*>(line), cap);
+      else w_stoch<0>(w, j, reinterpret_cast<float*>(line), cap);
+      break;
+    case F_CCI: w_cci(w, j, reinterpret_cast<double*>(line)); break;
     case F_MFI: w_mfi(w, j, reinterpret_cast<double*>(line), cap); break;
     case F_EMA: case F_RMA:
       if (f32) w_ema<float>(w, j); else w_ema<double>(w, j);
@@ -118,30 +121,46 @@ __device__ void produce(const Launch& L, const Layout& lay, unsigned char* smem,
                         int nchunks, int lane) {
   float* ring = reinterpret_cast<float*>(smem + lay.ring_off);
   const int NS = lay.NS, Hs = lay.Hs, RS = lay.RS;
+  const bool uni = !L.order && !L.offsets;
+  const long long s0T = (long long)blockIdx.x * 32 * L.T;
+  const int nvalid = (int)min(32ll, (long long)L.S - (long long)blockIdx.x * 32);
+  const unsigned long long limit = L.stall_test ? kStallWaitNs : kWaitNs;
   for (int c = 0; c < nchunks; ++c) {
     const int s = c % NS, use = c / NS;
-    if (use > 0 && !mbar_wait(&empty[s], (unsigned)((use - 1) & 1), abort_flag, err, lane)) break;
+    if (use > 0 && !mbar_wait(&empty[s], (unsigned)((use - 1) & 1), abort_flag, err, lane, limit)) break;
     const long long t = (long long)c * C + lane;
     const bool mir = s >= NS - Hs;
     const int off = (Hs + s) * C + lane, moff = (s - (NS - Hs)) * C + lane;
     for (int q = 0; q < lay.nplanes; ++q) {
-      const float* src = L.plane[lay.slot_plane[q]];
+      const float* base = L.plane[lay.slot_plane[q]];
       float* dst = ring + (size_t)q * 32 * RS;
+      if (uni) {
+        // rows of the group are consecutive rows of T bars
+        const bool in_row = t < L.T;
+        const float* src = base + s0T + t;
 #pragma unroll 4
-      for (int i = 0; i < 32; ++i) {
-        const long long b = tbase[i];
-        const bool ok = b >= 0 && t < tn[i];
-        const float* sp = ok ? src + b + t : src;
-        cp_async4(dst + i * RS + off, sp, ok);
-        if (mir) cp_async4(dst + i * RS + moff, sp, ok);
+        for (int i = 0; i < 32; ++i) {
+          const bool ok = in_row && i < nvalid;
+          const float* sp = ok ? src + (long long)i * L.T : base;
+          cp_async4(dst + i * RS + off, sp, ok);
+          if (mir) cp_async4(dst + i * RS + moff, sp, ok);
+        }
+      } else {
+#pragma unroll 4
+        for (int i = 0; i < 32; ++i) {
+          const long long b = tbase[i];
+          const bool ok = b >= 0 && t < tn[i];
+          const float* sp = ok ? base + b + t : base;
+          cp_async4(dst + i * RS + off, sp, ok);
+          if (mir) cp_async4(dst + i * RS + moff, sp, ok);
+        }
       }
     }
-    cp_async_arrive(&full[s]);
+    // test knob: chunk 0 is never announced, so the job warps' first wait runs out
+    if (!(L.stall_test && c == 0)) cp_async_arrive(&full[s]);
   }
   cp_async_wait_all();
 }
-
-__device__ int g_rows_err;  // sticky: a wait of the engine ran out on this device
 
 __global__ void __launch_bounds__(32 * (kMaxConsumers + 1), 1) rows_kernel(const __grid_constant__ Launch L, const __grid_constant__ Layout lay) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -151,7 +170,7 @@ __global__ void __launch_bounds__(32 * (kMaxConsumers + 1), 1) rows_kernel(const
   long long* tbase = reinterpret_cast<long long*>(smem + lay.tab_off);
   long long* tn = tbase + 32;
   int* misc = reinterpret_cast<int*>(tn + 32);  // [0] longest row of the group, [1] abort
-  int* err = L.err ? L.err : &g_rows_err;
+  int* err = L.sticky;
   if (warp == 0) {
     const long long idx = (long long)blockIdx.x * 32 + lane;
     long long b = -1, n = 0;
@@ -182,7 +201,7 @@ __global__ void __launch_bounds__(32 * (kMaxConsumers + 1), 1) rows_kernel(const
   const int maxn = misc[0];
   const int nchunks = (maxn + C - 1) / C;
   volatile int* abort_flag = misc + 1;
-  if (warp == lay.nconsumers) {
+  if (warp == lay.producer_warp) {
     produce(L, lay, smem, full, empty, tbase, tn, abort_flag, err, nchunks, lane);
     return;
   }
@@ -196,6 +215,7 @@ __global__ void __launch_bounds__(32 * (kMaxConsumers + 1), 1) rows_kernel(const
   w.tn = tn;
   w.abort_flag = abort_flag;
   w.err = err;
+  w.wait_ns = L.stall_test ? kStallWaitNs : kWaitNs;
   w.stage = reinterpret_cast<float*>(smem + lay.stage_off[warp]);
   w.lane = lane;
   w.nchunks = nchunks;
@@ -204,6 +224,10 @@ __global__ void __launch_bounds__(32 * (kMaxConsumers + 1), 1) rows_kernel(const
   w.NS = lay.NS;
   w.RS = lay.RS;
   w.n = tn[lane];
+  w.uni = !L.order && !L.offsets;
+  w.T = L.T;
+  w.s0T = (long long)blockIdx.x * 32 * L.T;
+  w.nvalid = (int)min(32ll, (long long)L.S - (long long)blockIdx.x * 32);
   run_job(w, L.jobs[lay.warp_job[warp]], smem + lay.line_off[warp]);
 }
 
@@ -235,6 +259,55 @@ struct DevState {
 std::mutex g_mutex;
 std::vector<DevState> g_dev;
 
+// Relative issue cost per bar of each family's job warp (instructions per
+// bar of its steady loop, rounded), and of the producer per staged plane.
+int family_cost(const Job& j) {
+  switch (j.family) {
+    case F_CCI: return 20 + 3 * j.ip[0];
+    case F_STOCH: return 45;
+    case F_ADX: case F_DX: return 40;
+    case F_MFI: return 35;
+    case F_BBANDS: return 30;
+    case F_WILLR: return 25;
+    case F_MACD: return 18;
+    case F_STDDEV: case F_VAR: return 22;
+    case F_RSI: return 16;
+    case F_ATR: case F_NATR: return 14;
+    case F_WMA: return 13;
+    case F_SMA: case F_SUM: return 11;
+    case F_OBV: return 8;
+    case F_EMA: case F_RMA: return 6;
+    default: return 20 + 2 * j.ip[0];
+  }
+}
+
+// Warp w of a CTA issues from sub-partition w % 4. The job warps and the
+// producer are placed longest-first on the least loaded sub-partition, so the
+// heaviest jobs do not share one.
+void assign_warps(const Launch& L, Layout& lay) {
+  const int n = L.njobs + 1;  // jobs + producer
+  int cost[kMaxConsumers + 1], order[kMaxConsumers + 1];
+  for (int i = 0; i < L.njobs; ++i) cost[i] = family_cost(L.jobs[i]);
+  cost[L.njobs] = 4 * lay.nplanes;
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order, order + n, [&](int a, int b) { return cost[a] > cost[b]; });
+  int load[4] = {0, 0, 0, 0}, used[4] = {0, 0, 0, 0};
+  for (int k = 0; k < n; ++k) {
+    int best = -1;
+    for (int q = 0; q < 4; ++q) {
+      // the warp ids of sub-partition q are q, q+4, ... below n
+      if (q + 4 * used[q] >= n) continue;
+      if (best < 0 || load[q] < load[best]) best = q;
+    }
+    const int w = best + 4 * used[best];
+    ++used[best];
+    load[best] += cost[order[k]];
+    const int item = order[k];
+    lay.warp_job[w] = item == L.njobs ? -1 : item;
+    if (item == L.njobs) lay.producer_warp = w;
+  }
+}
+
 }  // namespace
 
 bool supports(const Launch& L, long long max_len) {
@@ -245,6 +318,7 @@ bool supports(const Launch& L, long long max_len) {
     if (jb.prec != 0 || !family_supported(jb.family)) return false;
     if (rows_halo(jb) > kMaxHalo) return false;
     if (line_entries(jb) > kMaxLine) return false;
+    if (jb.family == F_CCI && jb.ip[0] > kMaxLine) return false;
   }
   return true;
 }
@@ -284,7 +358,7 @@ cudaError_t launch(Launch& L, long long max_len, cudaStream_t stream, LaunchStat
   }
   lay.nplanes = np;
   lay.Hs = std::max(1, (H + C - 1) / C);
-  lay.NS = lay.Hs + 2;
+  lay.NS = lay.Hs + 4;  // three chunks in flight ahead of the slowest job
   lay.RS = (lay.Hs + lay.NS) * C + 1;
   int off = 0;
   lay.ring_off = off;
@@ -295,14 +369,16 @@ cudaError_t launch(Launch& L, long long max_len, cudaStream_t stream, LaunchStat
   lay.tab_off = off;
   off += 64 * 8 + 16;
   lay.nconsumers = L.njobs;
-  for (int w = 0; w < L.njobs; ++w) {
-    lay.warp_job[w] = w;
+  assign_warps(L, lay);
+  for (int w = 0; w <= L.njobs; ++w) {
+    const int jb = lay.warp_job[w];
     off = (off + 15) & ~15;
     lay.stage_off[w] = off;
-    off += out_count(L.jobs[w].family) * 32 * (C + 1) * 4;
+    if (jb < 0) continue;
+    off += out_count(L.jobs[jb].family) * 32 * (C + 1) * 4;
     off = (off + 15) & ~15;
     lay.line_off[w] = off;
-    off += line_bytes(L.jobs[w]);
+    off += line_bytes(L.jobs[jb]);
   }
   lay.total = (off + 127) & ~127;
   if (lay.total > ds->smem_optin) return cudaErrorNotSupported;

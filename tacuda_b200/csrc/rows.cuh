@@ -43,6 +43,7 @@ constexpr int kMaxConsumers = 15;     // job warps per CTA (one more warp stages
 constexpr int kMaxLine = 64;          // per-lane history of the line-keeping families
 constexpr int kFp32MaxPeriod = 32;    // recurrences up to this period keep float32 state
 constexpr unsigned long long kWaitNs = 1000000000ull;  // one mbarrier wait gives up after 1 s
+constexpr unsigned long long kStallWaitNs = 1000000ull;  // 1 ms under the stall test knob
 constexpr unsigned kWaitPolls = 1u << 28;               // and after this many polls in any case
 
 struct Layout {
@@ -54,9 +55,10 @@ struct Layout {
   int bar_off;                        // uint64 full[NS], empty[NS]
   int tab_off;                        // long long base[32], n[32]; int maxn, abort
   int nconsumers;
-  int warp_job[kMaxConsumers];
-  int stage_off[kMaxConsumers];       // [nout][32][C+1] floats
-  int line_off[kMaxConsumers];        // per-warp history lines
+  int producer_warp;
+  int warp_job[kMaxConsumers + 1];    // job of each warp, -1 for the producer
+  int stage_off[kMaxConsumers + 1];   // [nout][32][C+1] floats
+  int line_off[kMaxConsumers + 1];    // per-warp history lines
   int total;
 };
 
@@ -98,7 +100,8 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // Bounded wait for the phase of `b` with parity `par`: false when the wait ran
 // out (the error word is set and the CTA's abort flag raised) or another warp
 // of the CTA aborted.
-__device__ bool mbar_wait(uint64_t* b, unsigned par, volatile int* abort_flag, int* err, int lane) {
+__device__ bool mbar_wait(uint64_t* b, unsigned par, volatile int* abort_flag, int* err, int lane,
+                          unsigned long long limit_ns) {
   unsigned long long t0 = 0;
   for (unsigned i = 0; i < kWaitPolls; ++i) {
     if (mbar_try_wait(b, par)) return true;
@@ -106,11 +109,11 @@ __device__ bool mbar_wait(uint64_t* b, unsigned par, volatile int* abort_flag, i
       if (*abort_flag) return false;
       const unsigned long long now = global_ns();
       if (t0 == 0) t0 = now;
-      else if (now - t0 > kWaitNs) break;
+      else if (now - t0 > limit_ns) break;
     }
   }
   if (lane == 0) {
-    atomicOr(err, 1);
+    if (err) atomicOr(err, 1);
     *abort_flag = 1;
   }
   return false;
@@ -136,6 +139,15 @@ struct Bad {
 
 // --------------------------------------------------------------- driver
 
+// a / b through the approximate reciprocal (max 1 ulp) and one rounding: the
+// ratios below need the float tolerance, not IEEE division's last bit.
+__device__ __forceinline__ float fdiv(float a, float b) {
+  float r;
+  asm("rcp.approx.f32 %0, %1;\n" : "=f"(r) : "f"(b));
+  return a * r;
+}
+__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
+
 struct Warp {
   unsigned char* smem;
   const Layout* lay;
@@ -147,16 +159,23 @@ struct Warp {
   int* err;
   float* stage;
   int lane, nchunks, maxn, Hs, NS, RS;
-  long long n;  // this lane's row length
+  unsigned long long wait_ns;  // limit of one wait
+  long long n;     // this lane's row length
+  bool uni;        // rows of the group are consecutive rows of a uniform batch
+  long long T;     // their length
+  long long s0T;   // element offset of the group's first row
+  int nvalid;      // rows of the group that exist
 
   __device__ __forceinline__ const float* X(int c, int plane) const {
     const float* ring = reinterpret_cast<const float*>(smem + lay->ring_off);
     return ring + ((size_t)lay->plane_slot[plane] * 32 + lane) * RS + (Hs + c % NS) * C;
   }
   __device__ __forceinline__ int lim(int c) const { return min(C, maxn - c * C); }
+  // bars of chunk c a steady (unrolled by 8) loop covers
+  __device__ __forceinline__ int lim8(int c) const { return (lim(c) + 7) & ~7; }
 
   __device__ __forceinline__ bool wait(int c) const {
-    return mbar_wait(&full[c % NS], (unsigned)((c / NS) & 1), abort_flag, err, lane);
+    return mbar_wait(&full[c % NS], (unsigned)((c / NS) & 1), abort_flag, err, lane, wait_ns);
   }
   // chunk c is done: chunk c - Hs is no longer read as a halo
   __device__ __forceinline__ void release(int c) const {
@@ -164,23 +183,54 @@ struct Warp {
     __syncwarp();
     if (r >= 0 && lane == 0) mbar_arrive(&empty[r % NS]);
   }
+  __device__ __forceinline__ float* stage_row(int k) const { return stage + (k * 32 + lane) * (C + 1); }
   __device__ __forceinline__ void put(int k, int r, float v) const { stage[(k * 32 + lane) * (C + 1) + r] = v; }
-  __device__ __forceinline__ void put_int(int k, int r, int v) const {
-    reinterpret_cast<int*>(stage)[(k * 32 + lane) * (C + 1) + r] = v;
-  }
   // coalesced row segments of output k for chunk c
   __device__ void flush(int k, float* out, int c) const {
     __syncwarp();
-    const long long t = (long long)c * C + lane;
-    const float* src = stage + k * 32 * (C + 1) + lane;
+    const int t0 = c * C;
+    const float* src = stage + k * 32 * (C + 1);
+    if (uni) {
+      if (((T | ((long long)(uintptr_t)out >> 2)) & 1) == 0) {
+        // even rows in 8-byte aligned planes: half a warp per row, two bars a lane
+        const int half = lane >> 4, col = (lane & 15) << 1;
+        if (t0 + col < T) {
+          float* p = out + s0T + half * T + t0 + col;
+          const float* sp = src + half * (C + 1) + col;
 #pragma unroll 4
-    for (int i = 0; i < 32; ++i) {
-      const long long b = tbase[i];
-      if (b >= 0 && t < tn[i]) out[b + t] = src[i * (C + 1)];
+          for (int i = half; i < nvalid; i += 2) {
+            float2 v;
+            v.x = sp[0];
+            v.y = sp[1];
+            *reinterpret_cast<float2*>(p) = v;
+            p += 2 * T;
+            sp += 2 * (C + 1);
+          }
+        }
+      } else if (t0 + lane < T) {
+        float* p = out + s0T + t0 + lane;
+        const float* sp = src + lane;
+#pragma unroll 4
+        for (int i = 0; i < nvalid; ++i) {
+          *p = *sp;
+          p += T;
+          sp += C + 1;
+        }
+      }
+    } else {
+      const long long t = t0 + lane;
+      src += lane;
+#pragma unroll 4
+      for (int i = 0; i < 32; ++i) {
+        const long long b = tbase[i];
+        if (b >= 0 && t < tn[i]) out[b + t] = src[i * (C + 1)];
+      }
     }
     __syncwarp();
   }
 };
+
+__device__ __forceinline__ bool all_lanes(bool v) { return __all_sync(kFull, v); }
 
 // ------------------------------------------------------------- windows
 
@@ -188,6 +238,9 @@ struct Warp {
 // float32 values are exact in FP64, so the running sum is the direct sum of
 // every window, with no drift along the row; NaN and +-inf are kept out of
 // the sums and counted, so each window sees them only while it holds them.
+// A chunk whose windows hold only finite values runs without that
+// bookkeeping (same arithmetic); if a non-finite value shows up, the chunk is
+// run again the general way from the saved sums.
 // talib08:14748-14812 TA_SMA, talib08:19171-19277 TA_WMA, BatchFused.cu:133-138 SUM.
 __device__ void w_sum_window(const Warp& w, const Job& j, int mode) {
   const int pl = j.in[0], p = j.ip[0];
@@ -199,118 +252,174 @@ __device__ void w_sum_window(const Warp& w, const Job& j, int mode) {
   for (int c = 0; c < w.nchunks; ++c) {
     if (!w.wait(c)) return;
     const float* X = w.X(c, pl);
-    const int t0 = c * C, lim = w.lim(c);
-    for (int r = 0; r < lim; ++r) {
-      const int t = t0 + r;
-      const float vin = X[r];
-      const bool out_bar = t >= p;
-      const float vout = out_bar ? X[r - p] : 0.0f;
-      const bool fi = finitef(vin), fo = finitef(vout);
-      if (!(fi && fo)) {
-        if (!fi) bad.add(vin, 1);
-        if (!fo) bad.add(vout, -1);
+    const float* Xo = X - p;
+    float* st = w.stage_row(0);
+    const int t0 = c * C;
+    bool general = !(t0 >= p && all_lanes(!bad.any()));
+    if (!general) {
+      const double s_in = s, ws_in = ws;
+      const int n8 = w.lim8(c);
+      for (int r8 = 0; r8 < n8; r8 += 8) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int r = r8 + u;
+          const double a = (double)X[r], b = (double)Xo[r];
+          if (mode == 2) ws = fma(dp, a, ws - s);
+          s = (s + a) - b;
+          st[r] = mode == 0 ? (float)(s * invp) : mode == 1 ? (float)s : (p == 1 ? X[r] : (float)(ws * invdiv));
+        }
       }
-      const double a = fi ? (double)vin : 0.0, b = fo ? (double)vout : 0.0;
-      if (mode == 2) ws = out_bar ? ws - s + dp * a : fma((double)(t + 1), a, ws);
-      s = (s + a) - b;
-      float o = qnan();
-      if (t >= p - 1) {
-        if (bad.any()) o = (mode == 2 && p == 1) ? vin : bad.value();
-        else if (mode == 0) o = (float)(s * invp);
-        else if (mode == 1) o = (float)s;
-        else o = p == 1 ? vin : (float)(ws * invdiv);
+      if (!all_lanes(isfinite(s) && isfinite(ws))) {
+        s = s_in;
+        ws = ws_in;
+        general = true;
       }
-      w.put(0, r, o);
+    }
+    if (general) {
+      const int lim = w.lim(c);
+      for (int r = 0; r < lim; ++r) {
+        const int t = t0 + r;
+        const float vin = X[r];
+        const bool out_bar = t >= p;
+        const float vout = out_bar ? Xo[r] : 0.0f;
+        const bool fi = finitef(vin), fo = finitef(vout);
+        if (!(fi && fo)) {
+          if (!fi) bad.add(vin, 1);
+          if (!fo) bad.add(vout, -1);
+        }
+        const double a = fi ? (double)vin : 0.0, b = fo ? (double)vout : 0.0;
+        if (mode == 2) ws = out_bar ? fma(dp, a, ws - s) : fma((double)(t + 1), a, ws);
+        s = (s + a) - b;
+        float o = qnan();
+        if (t >= p - 1) {
+          if (bad.any()) o = (mode == 2 && p == 1) ? vin : bad.value();
+          else if (mode == 0) o = (float)(s * invp);
+          else if (mode == 1) o = (float)s;
+          else o = p == 1 ? vin : (float)(ws * invdiv);
+        }
+        st[r] = o;
+      }
     }
     w.flush(0, (float*)j.out[0], c);
     w.release(c);
   }
 }
 
-// BBANDS / STDDEV / VAR (mode 0/1/2): moments of x - o about an origin o taken
-// at the first output bar of every chunk, where the window is summed directly
+// BBANDS / STDDEV / VAR (mode 0/1/2): moments of d = x - o about an origin o,
+// the bar at each chunk's first output, where the window is summed directly
 // (talib08:18047-18183 TA_VAR re-centres the same way); the variance follows
-// TA-Lib's E[d^2] - E[d]^2 in FP64 and is clamped at zero.
+// TA-Lib's E[d^2] - E[d]^2 in FP64 and is clamped at zero; the square root and
+// the bands in float32. A chunk whose windows are finite runs without NaN
+// bookkeeping, with the same arithmetic.
+__device__ __forceinline__ void moment_out(int mode, double o, double s1, double s2, double inv, float up, float dn,
+                                           float& o0, float& o1, float& o2) {
+  const double m1 = s1 * inv;
+  double var = fma(-m1, m1, s2 * inv);
+  var = var > 0.0 ? var : 0.0;
+  const float vf = (float)var;
+  if (mode == 2) {
+    o0 = vf;
+    return;
+  }
+  const float sd = sqrtf(vf);
+  if (mode == 1) {
+    o0 = sd * up;
+    return;
+  }
+  const float mid = (float)(o + m1);
+  if (up == dn) {
+    const float dv = sd * up;
+    o0 = mid + dv;
+    o2 = mid - dv;
+  } else {
+    o0 = fmaf(sd, up, mid);
+    o2 = mid - sd * dn;
+  }
+  o1 = mid;
+}
+
 __device__ void w_moment_window(const Warp& w, const Job& j, int mode) {
   const int pl = j.in[0], p = j.ip[0];
   const double inv = 1.0 / (double)p;
   const float up = (float)j.fp[0], dn = (float)j.fp[1];
-  const double upd = j.fp[0];
+  const int nout = mode == 0 ? 3 : 1;
   for (int c = 0; c < w.nchunks; ++c) {
     if (!w.wait(c)) return;
     const float* X = w.X(c, pl);
-    const int t0 = c * C, lim = w.lim(c);
-    double raw = 0.0, s2 = 0.0, o = 0.0;
-    int nn = 0;
-    bool seeded = false;
-    for (int r = 0; r < lim; ++r) {
-      const int t = t0 + r;
-      float o0 = qnan(), o1 = qnan(), o2 = qnan();
-      if (t >= p - 1) {
-        if (!seeded) {
-          seeded = true;
-          const float ov = X[r];
-          o = isnan(ov) ? 0.0 : (double)ov;
-          raw = s2 = 0.0;
-          nn = 0;
-          for (int i = 0; i < p; ++i) {
-            const float v = X[r - p + 1 + i];
-            if (isnan(v)) ++nn;
-            else {
-              raw += (double)v;
-              const double d = (double)v - o;
-              s2 = fma(d, d, s2);
-            }
-          }
-        } else {
-          const float vin = X[r], vout = X[r - p];
-          if (isnan(vout)) --nn;
-          else {
-            raw -= (double)vout;
-            const double d = (double)vout - o;
-            s2 = fma(-d, d, s2);
-          }
-          if (isnan(vin)) ++nn;
-          else {
-            raw += (double)vin;
-            const double d = (double)vin - o;
-            s2 = fma(d, d, s2);
-          }
+    const float* Xo = X - p;
+    float* st0 = w.stage_row(0);
+    float* st1 = w.stage_row(1);
+    float* st2 = w.stage_row(2);
+    const int t0 = c * C;
+    bool general = t0 < p - 1;
+    if (!general) {
+      // seed at bar t0 (r = 0)
+      const double o = (double)X[0];
+      double s1 = 0.0, s2 = 0.0;
+      for (int i = 0; i < p; ++i) {
+        const double d = (double)X[i - p + 1] - o;
+        s1 += d;
+        s2 = fma(d, d, s2);
+      }
+      float o0 = 0.0f, o1 = 0.0f, o2 = 0.0f;
+      moment_out(mode, o, s1, s2, inv, up, dn, o0, o1, o2);
+      st0[0] = o0;
+      if (mode == 0) { st1[0] = o1; st2[0] = o2; }
+      const int n8 = w.lim8(c);
+      for (int r8 = 0; r8 < n8; r8 += 8) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int r = r8 + u;
+          if (r == 0) continue;
+          const double di = (double)X[r] - o, dd = (double)Xo[r] - o;
+          s1 = (s1 + di) - dd;
+          s2 = fma(-dd, dd, fma(di, di, s2));
+          moment_out(mode, o, s1, s2, inv, up, dn, o0, o1, o2);
+          st0[r] = o0;
+          if (mode == 0) { st1[r] = o1; st2[r] = o2; }
         }
-        if (nn == 0) {
-          const double m1 = fma(-(double)p, o, raw) * inv;
-          double var = fma(-m1, m1, s2 * inv);
-          if (!(var > 0.0)) var = 0.0;
-          if (mode == 2) o0 = (float)var;
-          else if (mode == 1) {
-            const double sd = var != 0.0 ? sqrt(var) : 0.0;
-            o0 = (float)(upd != 1.0 ? sd * upd : sd);
+      }
+      if (!all_lanes(isfinite(s1) && isfinite(s2))) general = true;
+    }
+    if (general) {
+      const int lim = w.lim(c);
+      double s1 = 0.0, s2 = 0.0, o = 0.0;
+      int nn = 0;
+      bool seeded = false;
+      for (int r = 0; r < lim; ++r) {
+        const int t = t0 + r;
+        float o0 = qnan(), o1 = qnan(), o2 = qnan();
+        if (t >= p - 1) {
+          if (!seeded) {
+            seeded = true;
+            const float ov = X[r];
+            o = isnan(ov) ? 0.0 : (double)ov;
+            s1 = s2 = 0.0;
+            nn = 0;
+            for (int i = 0; i < p; ++i) {
+              const float v = X[r - p + 1 + i];
+              if (isnan(v)) ++nn;
+              else {
+                const double d = (double)v - o;
+                s1 += d;
+                s2 = fma(d, d, s2);
+              }
+            }
           } else {
-            const float sd = var != 0.0 ? sqrtf((float)var) : 0.0f;
-            const float mid = (float)(raw * inv);
-            if (up == dn) {
-              const float dv = sd * up;
-              o0 = mid + dv;
-              o2 = mid - dv;
-            } else {
-              o0 = fmaf(sd, up, mid);
-              o2 = mid - sd * dn;
-            }
-            o1 = mid;
+            const float vin = X[r], vout = Xo[r];
+            const double di = isnan(vin) ? 0.0 : (double)vin - o;
+            const double dd = isnan(vout) ? 0.0 : (double)vout - o;
+            nn += (isnan(vin) ? 1 : 0) - (isnan(vout) ? 1 : 0);
+            s1 = (s1 + di) - dd;
+            s2 = fma(-dd, dd, fma(di, di, s2));
           }
+          if (nn == 0) moment_out(mode, o, s1, s2, inv, up, dn, o0, o1, o2);
         }
-      }
-      w.put(0, r, o0);
-      if (mode == 0) {
-        w.put(1, r, o1);
-        w.put(2, r, o2);
+        st0[r] = o0;
+        if (mode == 0) { st1[r] = o1; st2[r] = o2; }
       }
     }
-    w.flush(0, (float*)j.out[0], c);
-    if (mode == 0) {
-      w.flush(1, (float*)j.out[1], c);
-      w.flush(2, (float*)j.out[2], c);
-    }
+    for (int k = 0; k < nout; ++k) w.flush(k, (float*)j.out[k], c);
     w.release(c);
   }
 }
@@ -323,27 +432,24 @@ __device__ void w_moment_window(const Warp& w, const Job& j, int mode) {
 // fmaxf / fminf scan does.
 template <bool kMax>
 struct VanHerk {
-  float* suf;  // this lane's line: suf[k * stride] for k in 0..p-1
-  int stride;
+  float* suf;  // this lane's line: suf[k * 32] for k in 0..p-1
   float pre;
   __device__ __forceinline__ static float op(float a, float b) { return kMax ? fmaxf(a, b) : fminf(a, b); }
-  // bar t at block position pos (t = k*p + pos); X points at bar t in the ring
-  __device__ __forceinline__ float step(const float* X, int r, int pos, int p, bool has_prev) {
-    const float x = X[r];
-    if (pos == 0) {
-      if (has_prev) {
-        float m = X[r - 1];
-        suf[(p - 1) * stride] = m;
-        for (int k = p - 2; k >= 0; --k) {
-          m = op(m, X[r - p + k]);
-          suf[k * stride] = m;
-        }
-      }
-      pre = x;
-    } else {
-      pre = op(pre, x);
+  // block start at bar t (t >= p): suffix extrema of bars t-p .. t-1
+  __device__ __forceinline__ void fill(const float* X, int r, int p) {
+    float m = X[r - 1];
+    suf[(p - 1) * 32] = m;
+    for (int k = p - 2; k >= 0; --k) {
+      m = op(m, X[r - p + k]);
+      suf[k * 32] = m;
     }
-    return pos == p - 1 ? pre : op(suf[(pos + 1) * stride], pre);
+  }
+  // bar t at block position pos (t = k*p + pos) with value x
+  __device__ __forceinline__ float step(float x, int pos, int p) {
+    pre = pos == 0 ? x : op(pre, x);
+    const int k = pos + 1 == p ? 0 : pos + 1;  // entry p does not exist
+    const float s = op(suf[k * 32], pre);
+    return pos == p - 1 ? pre : s;
   }
 };
 
@@ -352,30 +458,35 @@ struct VanHerk {
 // times -100 clamped to [-100, 0]; 0 for a zero range.
 __device__ void w_willr(const Warp& w, const Job& j, float* line, int cap) {
   const int ph = j.in[0], plo = j.in[1], pc = j.in[2], p = j.ip[0];
-  VanHerk<true> hh{line + w.lane, 32, 0.0f};
-  VanHerk<false> ll{line + 32 * cap + w.lane, 32, 0.0f};
+  VanHerk<true> hh{line + w.lane, 0.0f};
+  VanHerk<false> ll{line + 32 * cap + w.lane, 0.0f};
   int pos = 0;
   for (int c = 0; c < w.nchunks; ++c) {
     if (!w.wait(c)) return;
     const float* H = w.X(c, ph);
     const float* Lo = w.X(c, plo);
     const float* Cl = w.X(c, pc);
-    const int t0 = c * C, lim = w.lim(c);
-    for (int r = 0; r < lim; ++r) {
-      const int t = t0 + r;
-      const bool prev = t >= p;
-      float hi = hh.step(H, r, pos, p, prev);
-      float lo = ll.step(Lo, r, pos, p, prev);
-      if (++pos == p) pos = 0;
-      float o = qnan();
-      if (t >= p - 1) {
-        if (isnan(H[r])) hi = qnan();
-        if (isnan(Lo[r])) lo = qnan();
+    float* st = w.stage_row(0);
+    const int t0 = c * C, n8 = w.lim8(c);
+    for (int r8 = 0; r8 < n8; r8 += 8) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int r = r8 + u, t = t0 + r;
+        if (pos == 0 && t >= p) {
+          hh.fill(H, r, p);
+          ll.fill(Lo, r, p);
+        }
+        const float h = H[r], l = Lo[r];
+        float hi = hh.step(h, pos, p);
+        float lo = ll.step(l, pos, p);
+        pos = pos + 1 == p ? 0 : pos + 1;
+        hi = isnan(h) ? h : hi;
+        lo = isnan(l) ? l : lo;
         const float den = hi - lo;
-        const float v = den == 0.0f ? 0.0f : ((hi - Cl[r]) / den) * -100.0f;
-        o = isnan(v) ? qnan() : fminf(0.0f, fmaxf(-100.0f, v));
+        const float v = den == 0.0f ? 0.0f : fdiv(hi - Cl[r], den) * -100.0f;
+        const float o = isnan(v) ? qnan() : fminf(0.0f, fmaxf(-100.0f, v));
+        st[r] = t >= p - 1 ? o : qnan();
       }
-      w.put(0, r, o);
     }
     w.flush(0, (float*)j.out[0], c);
     w.release(c);
@@ -384,52 +495,81 @@ __device__ void w_willr(const Warp& w, const Job& j, float* line, int cap) {
 
 // STOCH (talib08:16115-16302, SMA slowing): fastK from the window extremes
 // anchored at the window's first bar, TA-Lib's zero-range test; slowK and
-// slowD are direct means of the last q fastK / slowK values, kept in per-lane
-// lines of cap (a power of two, >= p and q) entries.
+// slowD are direct means of the last q fastK / slowK values, summed oldest
+// first, from registers for q = Q > 0 or per-lane lines (Q = 0).
+template <int Q>
 __device__ void w_stoch(const Warp& w, const Job& j, float* line, int cap) {
-  const int ph = j.in[0], plo = j.in[1], pc = j.in[2], p = j.ip[0], q = j.ip[1];
-  const int lb = p - 1 + 2 * (q - 1);
+  const int ph = j.in[0], plo = j.in[1], pc = j.in[2], p = j.ip[0], q = Q > 0 ? Q : j.ip[1];
+  const int lb = p - 1 + 2 * (q - 1), kready = p - 1 + (q - 1);
   const int mask = cap - 1;
   const float invq = 1.0f / (float)q;
-  VanHerk<true> hh{line + w.lane, 32, 0.0f};
-  VanHerk<false> ll{line + 32 * cap + w.lane, 32, 0.0f};
-  float* fk = line + 2 * 32 * cap + w.lane;  // fk[(t & mask) * 32]
-  float* sk = line + 3 * 32 * cap + w.lane;
+  VanHerk<true> hh{line + w.lane, 0.0f};
+  VanHerk<false> ll{line + 32 * cap + w.lane, 0.0f};
+  float* fkl = line + 2 * 32 * cap + w.lane;  // [(t & mask) * 32]
+  float* skl = line + 3 * 32 * cap + w.lane;
+  float fh[4] = {0.0f, 0.0f, 0.0f, 0.0f}, sh[4] = {0.0f, 0.0f, 0.0f, 0.0f};  // [0] newest
   int pos = 0;
   for (int c = 0; c < w.nchunks; ++c) {
     if (!w.wait(c)) return;
     const float* H = w.X(c, ph);
     const float* Lo = w.X(c, plo);
     const float* Cl = w.X(c, pc);
-    const int t0 = c * C, lim = w.lim(c);
-    for (int r = 0; r < lim; ++r) {
-      const int t = t0 + r;
-      const bool prev = t >= p;
-      float hi = hh.step(H, r, pos, p, prev);
-      float lo = ll.step(Lo, r, pos, p, prev);
-      if (++pos == p) pos = 0;
-      float o0 = qnan(), o1 = qnan();
-      if (t >= p - 1) {
-        if (isnan(H[r - p + 1])) hi = qnan();
-        if (isnan(Lo[r - p + 1])) lo = qnan();
+    float* st0 = w.stage_row(0);
+    float* st1 = w.stage_row(1);
+    const int t0 = c * C, n8 = w.lim8(c);
+    for (int r8 = 0; r8 < n8; r8 += 8) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int r = r8 + u, t = t0 + r;
+        if (pos == 0 && t >= p) {
+          hh.fill(H, r, p);
+          ll.fill(Lo, r, p);
+        }
+        float hi = hh.step(H[r], pos, p);
+        float lo = ll.step(Lo[r], pos, p);
+        pos = pos + 1 == p ? 0 : pos + 1;
+        const float ha = H[r - p + 1], la = Lo[r - p + 1];
+        hi = isnan(ha) ? ha : hi;
+        lo = isnan(la) ? la : lo;
         const float range = hi - lo;
-        const float k = fabsf(range) <= 1e-14f * (fabsf(hi) + fabsf(lo)) ? 0.0f : ((Cl[r] - lo) / range) * 100.0f;
-        fk[(t & mask) * 32] = k;
-        if (t >= p - 1 + (q - 1)) {
-          float s = 0.0f;
-          for (int m = q - 1; m >= 0; --m) s += fk[((t - m) & mask) * 32];
+        const float k = fabsf(range) <= 1e-14f * (fabsf(hi) + fabsf(lo)) ? 0.0f : fdiv(Cl[r] - lo, range) * 100.0f;
+        float o0 = qnan(), o1 = qnan();
+        if (Q > 0) {
+#pragma unroll
+          for (int m = 3; m > 0; --m) fh[m] = fh[m - 1];
+          fh[0] = k;
+          float s = fh[Q - 1];
+#pragma unroll
+          for (int m = Q - 2; m >= 0; --m) s += fh[m];
           const float kv = s * invq;
-          sk[(t & mask) * 32] = kv;
+#pragma unroll
+          for (int m = 3; m > 0; --m) sh[m] = sh[m - 1];
+          sh[0] = kv;
+          float d = sh[Q - 1];
+#pragma unroll
+          for (int m = Q - 2; m >= 0; --m) d += sh[m];
           if (t >= lb) {
-            float d = 0.0f;
-            for (int m = q - 1; m >= 0; --m) d += sk[((t - m) & mask) * 32];
             o0 = kv;
             o1 = d * invq;
           }
+        } else if (t >= p - 1) {
+          fkl[(t & mask) * 32] = k;
+          if (t >= kready) {
+            float s = 0.0f;
+            for (int m = q - 1; m >= 0; --m) s += fkl[((t - m) & mask) * 32];
+            const float kv = s * invq;
+            skl[(t & mask) * 32] = kv;
+            if (t >= lb) {
+              float d = 0.0f;
+              for (int m = q - 1; m >= 0; --m) d += skl[((t - m) & mask) * 32];
+              o0 = kv;
+              o1 = d * invq;
+            }
+          }
         }
+        st0[r] = o0;
+        st1[r] = o1;
       }
-      w.put(0, r, o0);
-      w.put(1, r, o1);
     }
     w.flush(0, (float*)j.out[0], c);
     w.flush(1, (float*)j.out[1], c);
@@ -437,16 +577,23 @@ __device__ void w_stoch(const Warp& w, const Job& j, float* line, int cap) {
   }
 }
 
-// CCI (src/indicators/CCI.cu:11-40): typical price ((h+l)+c)/3 in FP64 into a
-// per-lane line, its running window sum, and the mean absolute deviation over
-// the window in FP64; output (tp - sma) / (0.015 md) when both are nonzero. A
-// window holding a non-finite typical price gives NaN, as the direct FP64 sum
-// of such a window does.
-__device__ void w_cci(const Warp& w, const Job& j, double* line, int cap) {
+// CCI (src/indicators/CCI.cu:11-40): typical price ((h+l)+c)/3 in FP64, its
+// window mean and the mean absolute deviation over the window in FP64;
+// (tp - sma) / (0.015 md) in float32 when both are nonzero. A window holding a
+// non-finite typical price gives NaN, as the direct FP64 sum of such a window
+// does.
+//
+// Per chunk, the typical prices of the chunk go into a per-lane line behind
+// the p of the chunk before (line[(p+r)*32], r = -p .. 31), the window means
+// into a second line, and the deviations are then summed for 8 bars at a
+// time, so every bar's sum is an independent chain. A chunk whose windows hold
+// only finite values skips the NaN bookkeeping; the arithmetic is the same
+// either way.
+__device__ void w_cci(const Warp& w, const Job& j, double* line) {
   const int ph = j.in[0], plo = j.in[1], pc = j.in[2], p = j.ip[0];
-  const int mask = cap - 1;
   const double invp = 1.0 / (double)p, third = 1.0 / 3.0;
-  double* tl = line + w.lane;  // tl[(t & mask) * 32]
+  double* tl = line + w.lane;                 // [(p + r) * 32]
+  double* ml = line + (p + C) * 32 + w.lane;  // window means [r * 32]
   double sum = 0.0;
   int last_bad = -(1 << 30);
   for (int c = 0; c < w.nchunks; ++c) {
@@ -454,34 +601,57 @@ __device__ void w_cci(const Warp& w, const Job& j, double* line, int cap) {
     const float* H = w.X(c, ph);
     const float* Lo = w.X(c, plo);
     const float* Cl = w.X(c, pc);
+    float* st = w.stage_row(0);
     const int t0 = c * C, lim = w.lim(c);
+    // the previous chunk's last p typical prices move to the front
+    if (c > 0)
+      for (int i = 0; i < p; ++i) tl[i * 32] = tl[(i + C) * 32];
+    double* cur = tl + p * 32;  // cur[r * 32]: bar t0 + r
+    double chk = 0.0;
+    for (int r = 0; r < lim; ++r) {
+      const double tp = (((double)H[r] + (double)Lo[r]) + (double)Cl[r]) * third;
+      cur[r * 32] = tp;
+      chk += tp * 0.0;
+    }
+    const bool steady = t0 >= p && all_lanes(last_bad <= t0 - p && chk == 0.0);
+    // window means; non-finite prices count as 0 and are tracked in last_bad
+    unsigned nanwin = 0;  // bit r: the window of bar t0 + r holds a non-finite price
     for (int r = 0; r < lim; ++r) {
       const int t = t0 + r;
-      const double tp = (((double)H[r] + (double)Lo[r]) + (double)Cl[r]) * third;
-      const bool fin = isfinite(tp);
-      if (!fin) last_bad = t;
-      const double tv = fin ? tp : 0.0;
-      tl[(t & mask) * 32] = tv;
-      const double gone = t >= p ? tl[((t - p) & mask) * 32] : 0.0;
-      sum = (sum + tv) - gone;
-      float o = qnan();
-      if (t >= p - 1) {
-        if (last_bad > t - p) o = qnan();
-        else {
-          const double sma = sum * invp;
-          double d0 = 0.0, d1 = 0.0;
-          int i = 0;
-          for (; i + 1 < p; i += 2) {
-            d0 += fabs(tl[((t - i) & mask) * 32] - sma);
-            d1 += fabs(tl[((t - i - 1) & mask) * 32] - sma);
-          }
-          if (i < p) d0 += fabs(tl[((t - i) & mask) * 32] - sma);
-          const float md = (float)((d0 + d1) * invp);
-          const float num = (float)(tv - sma);
-          o = (num != 0.0f && md != 0.0f) ? num / (0.015f * md) : 0.0f;
+      double tp = cur[r * 32];
+      if (!steady) {
+        if (!isfinite(tp)) {
+          last_bad = t;
+          tp = 0.0;
+          cur[r * 32] = 0.0;
         }
+        if (last_bad > t - p) nanwin |= 1u << r;
       }
-      w.put(0, r, o);
+      const double gone = t >= p ? cur[(r - p) * 32] : 0.0;
+      sum = (sum + tp) - gone;
+      ml[r * 32] = sum * invp;
+    }
+    const int n8 = (lim + 7) & ~7;
+    for (int r8 = 0; r8 < n8; r8 += 8) {
+      double sma[8], acc[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        sma[u] = ml[(r8 + u) * 32];
+        acc[u] = 0.0;
+      }
+      for (int i = 0; i < p; ++i) {
+        const double* wp = cur + (r8 - i) * 32;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) acc[u] += fabs(wp[u * 32] - sma[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int r = r8 + u, t = t0 + r;
+        const float md = (float)(acc[u] * invp);
+        const float num = (float)(cur[r * 32] - sma[u]);
+        const float o = (num != 0.0f && md != 0.0f) ? fdiv(num, 0.015f * md) : 0.0f;
+        st[r] = (t >= p - 1 && !((nanwin >> r) & 1u)) ? o : qnan();
+      }
     }
     w.flush(0, (float*)j.out[0], c);
     w.release(c);
@@ -490,8 +660,9 @@ __device__ void w_cci(const Warp& w, const Job& j, double* line, int cap) {
 
 // MFI (include/utils/StreamStates.h:749-792 precise::MfiState): flows of the
 // FP64 typical price times volume, signed by the typical price's change, in a
-// per-lane line; running positive / negative window sums, re-summed when one
-// turns negative; 100 * pos / (pos + neg), 0 below a total of 1.
+// per-lane line; running positive / negative window sums, re-summed directly
+// when one turns negative or a non-finite flow is in reach (the reference sums
+// every window); 100 * pos / (pos + neg), 0 below a total of 1.
 __device__ void w_mfi(const Warp& w, const Job& j, double* line, int cap) {
   const int ph = j.in[0], plo = j.in[1], pc = j.in[2], pv = j.in[3], p = j.ip[0];
   const int mask = cap - 1;
@@ -499,52 +670,47 @@ __device__ void w_mfi(const Warp& w, const Job& j, double* line, int cap) {
   double* pos_l = line + w.lane;  // [(t & mask) * 32]
   double* neg_l = line + 32 * cap + w.lane;
   double prev_tp = 0.0, ps = 0.0, ns = 0.0;
+  int last_bad = -(1 << 30);
   for (int c = 0; c < w.nchunks; ++c) {
     if (!w.wait(c)) return;
     const float* H = w.X(c, ph);
     const float* Lo = w.X(c, plo);
     const float* Cl = w.X(c, pc);
     const float* V = w.X(c, pv);
-    const int t0 = c * C, lim = w.lim(c);
-    for (int r = 0; r < lim; ++r) {
-      const int t = t0 + r;
-      const double tp = (((double)H[r] + (double)Lo[r]) + (double)Cl[r]) * third;
-      double a = 0.0, b = 0.0;
-      if (t >= 1 && isfinite(tp) && isfinite(prev_tp)) {
+    float* st = w.stage_row(0);
+    const int t0 = c * C, n8 = w.lim8(c);
+    for (int r8 = 0; r8 < n8; r8 += 8) {
+#pragma unroll 4
+      for (int u = 0; u < 8; ++u) {
+        const int r = r8 + u, t = t0 + r;
+        const double tp = (((double)H[r] + (double)Lo[r]) + (double)Cl[r]) * third;
         const double fl = tp * (double)V[r];
-        if (tp > prev_tp) a = fl;
-        else if (tp < prev_tp) b = fl;
-      }
-      prev_tp = tp;
-      const int slot = (t & mask) * 32;
-      pos_l[slot] = a;
-      neg_l[slot] = b;
-      float o = qnan();
-      if (t >= p) {
-        if (t == p) {
-          ps = ns = 0.0;
-          for (int i = p - 1; i >= 0; --i) {
-            ps += pos_l[((t - i) & mask) * 32];
-            ns += neg_l[((t - i) & mask) * 32];
+        const bool ok = t >= 1 && isfinite(tp) && isfinite(prev_tp);
+        const double a = ok && tp > prev_tp ? fl : 0.0, b = ok && tp < prev_tp ? fl : 0.0;
+        if (!isfinite(a + b)) last_bad = t;
+        prev_tp = tp;
+        const int slot = (t & mask) * 32, g = ((t - p) & mask) * 32;
+        const double ga = pos_l[g], gb = neg_l[g];
+        pos_l[slot] = a;
+        neg_l[slot] = b;
+        float o = qnan();
+        if (t >= p) {
+          if (t > p) {
+            ps = (ps - ga) + a;
+            ns = (ns - gb) + b;
           }
-        } else {
-          const int g = ((t - p) & mask) * 32;
-          ps -= pos_l[g];
-          ns -= neg_l[g];
-          ps += a;
-          ns += b;
-          if (ps < 0.0 || ns < 0.0) {
+          if (t == p || ps < 0.0 || ns < 0.0 || last_bad >= t - p) {
             ps = ns = 0.0;
             for (int i = p - 1; i >= 0; --i) {
               ps += pos_l[((t - i) & mask) * 32];
               ns += neg_l[((t - i) & mask) * 32];
             }
           }
+          const double tot = ps + ns;
+          o = tot < 1.0 ? 0.0f : 100.0f * fdiv((float)ps, (float)tot);
         }
-        const double tot = ps + ns;
-        o = tot < 1.0 ? 0.0f : (float)(100.0 * (ps / tot));
+        st[r] = o;
       }
-      w.put(0, r, o);
     }
     w.flush(0, (float*)j.out[0], c);
     w.release(c);
@@ -554,7 +720,8 @@ __device__ void w_mfi(const Warp& w, const Job& j, double* line, int cap) {
 // ------------------------------------------------------------ recurrences
 
 // EMA / RMA (talib08:5546-5627 TA_EMA, talib08:13614-13683 TA_RMA): SMA seed,
-// then fma(beta, y, k*x); leading NaNs skipped (BatchFused.cu:34-41).
+// then fma(beta, y, k*x); leading NaNs skipped (BatchFused.cu:34-41). Chunks
+// past every lane's seed run the bare recurrence.
 template <class R>
 __device__ void w_ema(const Warp& w, const Job& j) {
   const int pl = j.in[0], p = j.ip[0];
@@ -565,20 +732,34 @@ __device__ void w_ema(const Warp& w, const Job& j) {
   for (int c = 0; c < w.nchunks; ++c) {
     if (!w.wait(c)) return;
     const float* X = w.X(c, pl);
-    const int lim = w.lim(c);
-    for (int r = 0; r < lim; ++r) {
-      const float xf = X[r];
-      float o = qnan();
-      if (cnt >= 0 || !isnan(xf)) {
-        ++cnt;
-        const R x = (R)xf;
-        if (copy) y = x;
-        else if (cnt > p - 1) y = fma(beta, y, kk * x);
-        else if (cnt < p - 1) y += x;
-        else y = (y + x) / (R)p;
-        if (cnt >= p - 1) o = (float)y;
+    float* st = w.stage_row(0);
+    if (all_lanes(cnt >= p - 1)) {
+      const int n8 = w.lim8(c);
+      for (int r8 = 0; r8 < n8; r8 += 8) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const R x = (R)X[r8 + u];
+          y = copy ? x : fma(beta, y, kk * x);
+          st[r8 + u] = (float)y;
+        }
       }
-      w.put(0, r, o);
+      cnt += n8;
+    } else {
+      const int lim = w.lim(c);
+      for (int r = 0; r < lim; ++r) {
+        const float xf = X[r];
+        float o = qnan();
+        if (cnt >= 0 || !isnan(xf)) {
+          ++cnt;
+          const R x = (R)xf;
+          if (copy) y = x;
+          else if (cnt > p - 1) y = fma(beta, y, kk * x);
+          else if (cnt < p - 1) y += x;
+          else y = (y + x) / (R)p;
+          if (cnt >= p - 1) o = (float)y;
+        }
+        st[r] = o;
+      }
     }
     w.flush(0, (float*)j.out[0], c);
     w.release(c);
@@ -586,7 +767,13 @@ __device__ void w_ema(const Warp& w, const Job& j) {
 }
 
 // RSI (talib08:13996-14115): Wilder sums of gains and losses; a NaN change
-// poisons the rest of the row; leading NaNs skipped.
+// makes the rest of the row NaN; leading NaNs skipped.
+template <class R>
+__device__ __forceinline__ float rsi_out(R gain, R loss) {
+  const R tot = gain + loss;
+  return isnan(tot) ? qnan() : (tot > (R)0 ? (float)((R)100 * fdiv(gain, tot)) : 50.0f);
+}
+
 template <class R>
 __device__ void w_rsi(const Warp& w, const Job& j) {
   const int pl = j.in[0], p = j.ip[0];
@@ -596,17 +783,32 @@ __device__ void w_rsi(const Warp& w, const Job& j) {
   for (int c = 0; c < w.nchunks; ++c) {
     if (!w.wait(c)) return;
     const float* X = w.X(c, pl);
-    const int lim = w.lim(c);
-    for (int r = 0; r < lim; ++r) {
-      const float xf = X[r];
-      float o = qnan();
-      if (cnt >= 0 || !isnan(xf)) {
-        ++cnt;
-        if (cnt > 0) {
-          const R d = (R)xf - (R)X[r - 1];
-          if (isnan(d)) {
-            gain = loss = d;
-          } else {
+    float* st = w.stage_row(0);
+    if (all_lanes(cnt >= p)) {
+      R xp = (R)X[-1];
+      const int n8 = w.lim8(c);
+      for (int r8 = 0; r8 < n8; r8 += 8) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const R x = (R)X[r8 + u];
+          const R d = x - xp;
+          xp = x;
+          const R g = d > (R)0 ? d : (R)0, l = g - d;
+          gain = (gain * pm1 + g) * inv;
+          loss = (loss * pm1 + l) * inv;
+          st[r8 + u] = rsi_out(gain, loss);
+        }
+      }
+      cnt += n8;
+    } else {
+      const int lim = w.lim(c);
+      for (int r = 0; r < lim; ++r) {
+        const float xf = X[r];
+        float o = qnan();
+        if (cnt >= 0 || !isnan(xf)) {
+          ++cnt;
+          if (cnt > 0) {
+            const R d = (R)xf - (R)X[r - 1];
             const R g = d > (R)0 ? d : (R)0, l = g - d;
             if (cnt > p) {
               gain = (gain * pm1 + g) * inv;
@@ -619,13 +821,10 @@ __device__ void w_rsi(const Warp& w, const Job& j) {
               loss = (loss + l) * inv;
             }
           }
+          if (cnt >= p) o = rsi_out(gain, loss);
         }
-        if (cnt >= p) {
-          const R tot = gain + loss;
-          o = isnan(tot) ? qnan() : (tot > (R)0 ? (float)((R)100 * (gain / tot)) : 50.0f);
-        }
+        st[r] = o;
       }
-      w.put(0, r, o);
     }
     w.flush(0, (float*)j.out[0], c);
     w.release(c);
@@ -646,38 +845,60 @@ __device__ void w_macd(const Warp& w, const Job& j) {
   for (int c = 0; c < w.nchunks; ++c) {
     if (!w.wait(c)) return;
     const float* X = w.X(c, pl);
-    const int lim = w.lim(c);
-    for (int r = 0; r < lim; ++r) {
-      const float xf = X[r];
-      float o0 = qnan(), o1 = qnan(), o2 = qnan();
-      if (cnt >= 0 || !isnan(xf)) {
-        ++cnt;
-        const double x = (double)xf;
-        if (cnt > start) {
+    float* st0 = w.stage_row(0);
+    float* st1 = w.stage_row(1);
+    float* st2 = w.stage_row(2);
+    if (all_lanes(cnt >= ready)) {
+      const int n8 = w.lim8(c);
+      for (int r8 = 0; r8 < n8; r8 += 8) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int r = r8 + u;
+          const double x = (double)X[r];
           pf = fma(fb, pf, fk * x);
           ps = fma(sb, ps, sk * x);
-        } else if (cnt < start) {
-          ps += x;
-          if (cnt >= slow - fast) pf += x;
-        } else {
-          ps = (ps + x) / slow;
-          pf = (pf + x) / fast;
-        }
-        if (cnt >= start) {
           const double m = pf - ps;
-          if (cnt > ready) psig = sig == 1 ? m : fma(gb, psig, gk * m);
-          else if (cnt < ready) psig += m;
-          else psig = (psig + m) / sig;
-          if (cnt >= ready) {
-            o0 = (float)m;
-            o1 = (float)psig;
-            o2 = (float)(m - psig);
-          }
+          psig = sig == 1 ? m : fma(gb, psig, gk * m);
+          st0[r] = (float)m;
+          st1[r] = (float)psig;
+          st2[r] = (float)(m - psig);
         }
       }
-      w.put(0, r, o0);
-      w.put(1, r, o1);
-      w.put(2, r, o2);
+      cnt += n8;
+    } else {
+      const int lim = w.lim(c);
+      for (int r = 0; r < lim; ++r) {
+        const float xf = X[r];
+        float o0 = qnan(), o1 = qnan(), o2 = qnan();
+        if (cnt >= 0 || !isnan(xf)) {
+          ++cnt;
+          const double x = (double)xf;
+          if (cnt > start) {
+            pf = fma(fb, pf, fk * x);
+            ps = fma(sb, ps, sk * x);
+          } else if (cnt < start) {
+            ps += x;
+            if (cnt >= slow - fast) pf += x;
+          } else {
+            ps = (ps + x) / slow;
+            pf = (pf + x) / fast;
+          }
+          if (cnt >= start) {
+            const double m = pf - ps;
+            if (cnt > ready) psig = sig == 1 ? m : fma(gb, psig, gk * m);
+            else if (cnt < ready) psig += m;
+            else psig = (psig + m) / sig;
+            if (cnt >= ready) {
+              o0 = (float)m;
+              o1 = (float)psig;
+              o2 = (float)(m - psig);
+            }
+          }
+        }
+        st0[r] = o0;
+        st1[r] = o1;
+        st2[r] = o2;
+      }
     }
     w.flush(0, (float*)j.out[0], c);
     w.flush(1, (float*)j.out[1], c);
@@ -701,6 +922,12 @@ __device__ __forceinline__ R true_range_r(R hi, R lo, R yc) {
 // ATR / NATR / TRANGE (mode 0/1/2): Wilder smoothing of the true range from
 // bar 1, fma(wb, y, wa*tr) (talib08 TA_ATR; StreamStates.h:675-721).
 template <class R>
+__device__ __forceinline__ float atr_out(int mode, int p, R y, R cl) {
+  if (mode == 0 || p == 1) return (float)y;
+  return cl == (R)0 ? 0.0f : (float)(fdiv(y, cl) * (R)100);
+}
+
+template <class R>
 __device__ void w_atr(const Warp& w, const Job& j, int mode) {
   const int ph = j.in[0], plo = j.in[1], pc = j.in[2];
   const int p = mode == 2 ? 1 : j.ip[0];
@@ -711,27 +938,42 @@ __device__ void w_atr(const Warp& w, const Job& j, int mode) {
     const float* H = w.X(c, ph);
     const float* Lo = w.X(c, plo);
     const float* Cl = w.X(c, pc);
-    const int t0 = c * C, lim = w.lim(c);
-    for (int r = 0; r < lim; ++r) {
-      const int t = t0 + r;
-      float o = qnan();
-      if (t >= 1) {
-        const R tr = true_range_r<R>((R)H[r], (R)Lo[r], (R)Cl[r - 1]);
-        if (mode == 2) o = (float)tr;
-        else {
-          if (t > p) y = fma(wb, y, wa * tr);
-          else if (t < p) y += tr;
-          else y = (y + tr) / (R)p;
-          if (t >= p) {
-            if (mode == 0 || p == 1) o = (float)y;
-            else {
-              const R cl = (R)Cl[r];
-              o = cl == (R)0 ? 0.0f : (float)((y / cl) * (R)100);
-            }
+    float* st = w.stage_row(0);
+    const int t0 = c * C;
+    if (t0 > p || (mode == 2 && t0 >= 1)) {
+      R cp = (R)Cl[-1];
+      const int n8 = w.lim8(c);
+      for (int r8 = 0; r8 < n8; r8 += 8) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int r = r8 + u;
+          const R cl = (R)Cl[r];
+          const R tr = true_range_r<R>((R)H[r], (R)Lo[r], cp);
+          cp = cl;
+          if (mode == 2) st[r] = (float)tr;
+          else {
+            y = fma(wb, y, wa * tr);
+            st[r] = atr_out<R>(mode, p, y, cl);
           }
         }
       }
-      w.put(0, r, o);
+    } else {
+      const int lim = w.lim(c);
+      for (int r = 0; r < lim; ++r) {
+        const int t = t0 + r;
+        float o = qnan();
+        if (t >= 1) {
+          const R tr = true_range_r<R>((R)H[r], (R)Lo[r], (R)Cl[r - 1]);
+          if (mode == 2) o = (float)tr;
+          else {
+            if (t > p) y = fma(wb, y, wa * tr);
+            else if (t < p) y += tr;
+            else y = (y + tr) / (R)p;
+            if (t >= p) o = atr_out<R>(mode, p, y, (R)Cl[r]);
+          }
+        }
+        st[r] = o;
+      }
     }
     w.flush(0, (float*)j.out[0], c);
     w.release(c);
@@ -742,6 +984,30 @@ __device__ void w_atr(const Warp& w, const Job& j, int mode) {
 // Wilder sums of the true range and directional movements, DI+/DI-, DX, and
 // for ADX the Wilder mean of DX seeded at 2p-1.
 template <class R>
+struct DmBar {
+  R range, plus, minus;
+};
+
+template <class R>
+__device__ __forceinline__ DmBar<R> dm_bar(float h, float l, float hp, float lp, float cp) {
+  DmBar<R> b;
+  const float u = h - hp, dw = lp - l;
+  b.plus = (u > 0.0f && u > dw) ? (R)u : (R)0;
+  b.minus = (dw > 0.0f && dw > u) ? (R)dw : (R)0;
+  const R hh = (R)h, ll = (R)l, yc = (R)cp;
+  b.range = fmax(hh - ll, fmax(fabs(hh - yc), fabs(ll - yc)));
+  return b;
+}
+
+template <class R>
+__device__ __forceinline__ R dx_of(R tr, R pd, R md) {
+  const R dip = tr > (R)0 ? fdiv((R)100 * pd, tr) : (R)0;
+  const R dim = tr > (R)0 ? fdiv((R)100 * md, tr) : (R)0;
+  const R tot = dip + dim;
+  return tot > (R)0 ? fdiv((R)100 * fabs(dip - dim), tot) : (R)0;
+}
+
+template <class R>
 __device__ void w_adx(const Warp& w, const Job& j, bool adx) {
   const int ph = j.in[0], plo = j.in[1], pc = j.in[2], p = j.ip[0];
   const R a = (R)(((double)p - 1.0) / (double)p), invp = (R)(1.0 / (double)p);
@@ -751,45 +1017,66 @@ __device__ void w_adx(const Warp& w, const Job& j, bool adx) {
     const float* H = w.X(c, ph);
     const float* Lo = w.X(c, plo);
     const float* Cl = w.X(c, pc);
-    const int t0 = c * C, lim = w.lim(c);
-    for (int r = 0; r < lim; ++r) {
-      const int t = t0 + r;
-      const float h = H[r], l = Lo[r];
-      R range, plus = 0, minus = 0;
-      if (t == 0) {
-        range = (R)h - (R)l;
-      } else {
-        const float u = h - H[r - 1], dw = Lo[r - 1] - l;
-        plus = (u > 0.0f && u > dw) ? (R)u : (R)0;
-        minus = (dw > 0.0f && dw > u) ? (R)dw : (R)0;
-        const R hh = (R)h, ll = (R)l, yc = (R)Cl[r - 1];
-        range = fmax(hh - ll, fmax(fabs(hh - yc), fabs(ll - yc)));
-      }
-      float o = qnan();
-      if (t < p) {
-        tr += range;
-        pd += plus;
-        md += minus;
-      } else {
-        tr = a * tr + range;
-        pd = a * pd + plus;
-        md = a * md + minus;
-        const R dip = tr > (R)0 ? (R)100 * pd / tr : (R)0;
-        const R dim = tr > (R)0 ? (R)100 * md / tr : (R)0;
-        const R tot = dip + dim;
-        const R dx = tot > (R)0 ? (R)100 * fabs(dip - dim) / tot : (R)0;
-        if (!adx) o = (float)dx;
-        else if (t > 2 * p - 1) {
-          av = a * av + dx * invp;
-          o = (float)av;
-        } else if (t < 2 * p - 1) {
-          av += dx;
-        } else {
-          av = (av + dx) / (R)p;
-          o = (float)av;
+    float* st = w.stage_row(0);
+    const int t0 = c * C;
+    if (t0 > (adx ? 2 * p - 1 : p)) {
+      float hp = H[-1], lp = Lo[-1], cp = Cl[-1];
+      const int n8 = w.lim8(c);
+      for (int r8 = 0; r8 < n8; r8 += 8) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int r = r8 + u;
+          const float h = H[r], l = Lo[r];
+          const DmBar<R> b = dm_bar<R>(h, l, hp, lp, cp);
+          hp = h;
+          lp = l;
+          cp = Cl[r];
+          tr = a * tr + b.range;
+          pd = a * pd + b.plus;
+          md = a * md + b.minus;
+          const R dx = dx_of(tr, pd, md);
+          if (adx) {
+            av = a * av + dx * invp;
+            st[r] = (float)av;
+          } else {
+            st[r] = (float)dx;
+          }
         }
       }
-      w.put(0, r, o);
+    } else {
+      const int lim = w.lim(c);
+      for (int r = 0; r < lim; ++r) {
+        const int t = t0 + r;
+        DmBar<R> b;
+        if (t == 0) {
+          b.range = (R)H[r] - (R)Lo[r];
+          b.plus = b.minus = (R)0;
+        } else {
+          b = dm_bar<R>(H[r], Lo[r], H[r - 1], Lo[r - 1], Cl[r - 1]);
+        }
+        float o = qnan();
+        if (t < p) {
+          tr += b.range;
+          pd += b.plus;
+          md += b.minus;
+        } else {
+          tr = a * tr + b.range;
+          pd = a * pd + b.plus;
+          md = a * md + b.minus;
+          const R dx = dx_of(tr, pd, md);
+          if (!adx) o = (float)dx;
+          else if (t > 2 * p - 1) {
+            av = a * av + dx * invp;
+            o = (float)av;
+          } else if (t < 2 * p - 1) {
+            av += dx;
+          } else {
+            av = (av + dx) / (R)p;
+            o = (float)av;
+          }
+        }
+        st[r] = o;
+      }
     }
     w.flush(0, (float*)j.out[0], c);
     w.release(c);
@@ -808,43 +1095,60 @@ __device__ void w_volume(const Warp& w, const Job& j, int mode) {
     const float* I1 = w.X(c, j.in[1]);
     const float* I2 = mode ? w.X(c, j.in[2]) : I0;
     const float* I3 = mode ? w.X(c, j.in[3]) : I0;
-    const int t0 = c * C, lim = w.lim(c);
-    for (int r = 0; r < lim; ++r) {
-      const int t = t0 + r;
-      float o;
-      if (mode == 0) {
-        const double v = (double)I1[r];
-        if (t == 0) acc += v;
-        else {
-          const float pr = I0[r], pp = I0[r - 1];
+    float* st = w.stage_row(0);
+    const int t0 = c * C;
+    if (mode == 0 && t0 >= 1) {
+      float pp = I0[-1];
+      const int n8 = w.lim8(c);
+      for (int r8 = 0; r8 < n8; r8 += 8) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int r = r8 + u;
+          const double v = (double)I1[r];
+          const float pr = I0[r];
           acc += pr > pp ? v : (pr < pp ? -v : 0.0 * v);
-        }
-        o = (float)acc;
-      } else {
-        const double hi = I0[r], lo = I1[r], cl = I2[r], vo = I3[r];
-        double term = 0.0;
-        if (isfinite(hi) && isfinite(lo) && isfinite(cl) && isfinite(vo)) {
-          const double range = hi - lo;
-          if (range > 0.0) term = (((cl - lo) - (hi - cl)) / range) * vo;
-        }
-        acc += term;
-        if (mode == 1) o = (float)acc;
-        else {
-          if (t == 0) fastv = slowv = acc;
-          else {
-            fastv = kf * acc + (1.0 - kf) * fastv;
-            slowv = ks * acc + (1.0 - ks) * slowv;
-          }
-          o = t < warm ? qnan() : (float)(fastv - slowv);
+          pp = pr;
+          st[r] = (float)acc;
         }
       }
-      w.put(0, r, o);
+    } else {
+      const int lim = w.lim(c);
+      for (int r = 0; r < lim; ++r) {
+        const int t = t0 + r;
+        float o;
+        if (mode == 0) {
+          const double v = (double)I1[r];
+          if (t == 0) acc += v;
+          else {
+            const float pr = I0[r], pp = I0[r - 1];
+            acc += pr > pp ? v : (pr < pp ? -v : 0.0 * v);
+          }
+          o = (float)acc;
+        } else {
+          const double hi = I0[r], lo = I1[r], cl = I2[r], vo = I3[r];
+          double term = 0.0;
+          if (isfinite(hi) && isfinite(lo) && isfinite(cl) && isfinite(vo)) {
+            const double range = hi - lo;
+            if (range > 0.0) term = (((cl - lo) - (hi - cl)) / range) * vo;
+          }
+          acc += term;
+          if (mode == 1) o = (float)acc;
+          else {
+            if (t == 0) fastv = slowv = acc;
+            else {
+              fastv = kf * acc + (1.0 - kf) * fastv;
+              slowv = ks * acc + (1.0 - ks) * slowv;
+            }
+            o = t < warm ? qnan() : (float)(fastv - slowv);
+          }
+        }
+        st[r] = o;
+      }
     }
     w.flush(0, (float*)j.out[0], c);
     w.release(c);
   }
 }
-
 
 // ------------------------------------------------------ further families
 // The families below follow the same TA-Lib / reference conventions as the

@@ -42,6 +42,11 @@ cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, long long total_ba
                          LaunchStats* stats);
 int max_lookback_halo(const Launch& L);
 
+// The per-device error word (bit 0: a bounded wait of an engine ran out) and
+// its read-and-clear; the read synchronises with the legacy default stream.
+int* sticky_word();
+cudaError_t take_sticky_error(int* value);
+
 namespace rows {
 // Row-parallel engine (rows.cu): whether it takes this job set and batch, and
 // its launch. Returns cudaErrorNotSupported for job sets it does not take.
