@@ -1340,14 +1340,15 @@ __device__ __forceinline__ void stoch_round(const Ctx<K>& c, const Job& j) {
   c.flush(1, (float*)j.out[1]);
 }
 
-// CCI(p): src/indicators/CCI.cu:11-40: typical price ((h+l)+c)/3 in FP64, its
-// window mean and mean absolute deviation; (tp - sma)/(0.015*md), 0 unless both
-// the numerator and md are nonzero.
+// CCI(p): src/indicators/CCI.cu:11-40, in its arithmetic: typical price
+// ((h+l)+c)/3.0 in FP64, sma = direct window sum / p, md = deviation sum / p
+// (both summed from the newest bar back), (tp - sma)/(0.015*md) in FP64, 0
+// unless both the numerator and md are nonzero.
 template <int K>
 __device__ __forceinline__ void cci_round(const Ctx<K>& c, const Job& j) {
   const int p = j.ip[0];
   const int g0 = c.gb0();
-  const double inv_p = 1.0 / (double)p;
+  const double dp = (double)p;
   for (int k = 0; k < K; ++k) {
     const int t = g0 + k;
     if (!c.valid(t)) break;
@@ -1355,10 +1356,10 @@ __device__ __forceinline__ void cci_round(const Ctx<K>& c, const Job& j) {
     if (t >= p - 1) {
       double sum = 0.0;
       for (int i = 0; i < p; ++i) sum += c.typ(t - i);
-      const double sma = sum * inv_p;
+      const double sma = sum / dp;
       double dev = 0.0;
       for (int i = 0; i < p; ++i) dev += fabs(c.typ(t - i) - sma);
-      const double md = dev * inv_p;
+      const double md = dev / dp;
       const double num = c.typ(t) - sma;
       o = (num != 0.0 && md != 0.0) ? (float)(num / (0.015 * md)) : 0.0f;
     }

@@ -32,7 +32,7 @@ __host__ __device__ inline int line_bytes(const Job& j) {
   switch (j.family) {
     case F_WILLR: return 2 * 32 * cap * 4;
     case F_STOCH: return 4 * 32 * cap * 4;
-    case F_CCI: return (j.ip[0] + 2 * C) * 32 * 8;
+    case F_CCI: return (j.ip[0] + C) * 32 * 8;
     case F_MFI: return 2 * 32 * cap * 8;
     default: return 0;
   }
@@ -263,7 +263,7 @@ std::vector<DevState> g_dev;
 // bar of its steady loop, rounded), and of the producer per staged plane.
 int family_cost(const Job& j) {
   switch (j.family) {
-    case F_CCI: return 20 + 3 * j.ip[0];
+    case F_CCI: return 30 + 5 * j.ip[0];
     case F_STOCH: return 45;
     case F_ADX: case F_DX: return 40;
     case F_MFI: return 35;

@@ -20,6 +20,11 @@
 // Outputs go through a per-warp [nout][32][C+1] transpose buffer and leave as
 // coalesced row segments.
 //
+// The warps of a CTA run up to 15 different families at once, so the hot code
+// of all of them competes for the SM's instruction cache; the per-bar loops
+// are therefore not unrolled (unrolled by 8 they measured 1.7x slower on the
+// 13-indicator pass, with most issue slots lost to instruction fetch).
+//
 // Arithmetic: float32 for the bulk (ranges, ratios, Wilder and EMA states of
 // short periods, window extrema); FP64 where the result needs it: the window
 // sums of float32 inputs (exact in FP64, so a running sum equals the direct
@@ -260,7 +265,7 @@ __device__ void w_sum_window(const Warp& w, const Job& j, int mode) {
       const double s_in = s, ws_in = ws;
       const int n8 = w.lim8(c);
       for (int r8 = 0; r8 < n8; r8 += 8) {
-#pragma unroll
+#pragma unroll 1
         for (int u = 0; u < 8; ++u) {
           const int r = r8 + u;
           const double a = (double)X[r], b = (double)Xo[r];
@@ -367,7 +372,7 @@ __device__ void w_moment_window(const Warp& w, const Job& j, int mode) {
       if (mode == 0) { st1[0] = o1; st2[0] = o2; }
       const int n8 = w.lim8(c);
       for (int r8 = 0; r8 < n8; r8 += 8) {
-#pragma unroll
+#pragma unroll 1
         for (int u = 0; u < 8; ++u) {
           const int r = r8 + u;
           if (r == 0) continue;
@@ -577,25 +582,22 @@ __device__ void w_stoch(const Warp& w, const Job& j, float* line, int cap) {
   }
 }
 
-// CCI (src/indicators/CCI.cu:11-40): typical price ((h+l)+c)/3 in FP64, its
-// window mean and the mean absolute deviation over the window in FP64;
-// (tp - sma) / (0.015 md) in float32 when both are nonzero. A window holding a
-// non-finite typical price gives NaN, as the direct FP64 sum of such a window
-// does.
+// CCI (src/indicators/CCI.cu:11-40), in the reference's arithmetic: typical
+// price (((double)h + l) + c) / 3.0, the window sum taken directly from the
+// newest bar back, sma = sum / p, the mean absolute deviation summed in the
+// same order, md = dev / p, and (tp - sma) / (0.015 md) in FP64 when both are
+// nonzero, rounded once to float. Direct sums keep a constant window's
+// deviation exactly zero (a running sum would leave rounding noise that the
+// quotient turns into +-66.67), and a non-finite price makes every window
+// holding it NaN without extra bookkeeping.
 //
 // Per chunk, the typical prices of the chunk go into a per-lane line behind
-// the p of the chunk before (line[(p+r)*32], r = -p .. 31), the window means
-// into a second line, and the deviations are then summed for 8 bars at a
-// time, so every bar's sum is an independent chain. A chunk whose windows hold
-// only finite values skips the NaN bookkeeping; the arithmetic is the same
-// either way.
+// the p of the chunk before (line[(p+r)*32], r = -p .. 31); both sums run for
+// 8 bars at a time, so every bar's sum is an independent chain.
 __device__ void w_cci(const Warp& w, const Job& j, double* line) {
   const int ph = j.in[0], plo = j.in[1], pc = j.in[2], p = j.ip[0];
-  const double invp = 1.0 / (double)p, third = 1.0 / 3.0;
-  double* tl = line + w.lane;                 // [(p + r) * 32]
-  double* ml = line + (p + C) * 32 + w.lane;  // window means [r * 32]
-  double sum = 0.0;
-  int last_bad = -(1 << 30);
+  const double dp = (double)p;
+  double* tl = line + w.lane;  // [(p + r) * 32]
   for (int c = 0; c < w.nchunks; ++c) {
     if (!w.wait(c)) return;
     const float* H = w.X(c, ph);
@@ -607,38 +609,19 @@ __device__ void w_cci(const Warp& w, const Job& j, double* line) {
     if (c > 0)
       for (int i = 0; i < p; ++i) tl[i * 32] = tl[(i + C) * 32];
     double* cur = tl + p * 32;  // cur[r * 32]: bar t0 + r
-    double chk = 0.0;
-    for (int r = 0; r < lim; ++r) {
-      const double tp = (((double)H[r] + (double)Lo[r]) + (double)Cl[r]) * third;
-      cur[r * 32] = tp;
-      chk += tp * 0.0;
-    }
-    const bool steady = t0 >= p && all_lanes(last_bad <= t0 - p && chk == 0.0);
-    // window means; non-finite prices count as 0 and are tracked in last_bad
-    unsigned nanwin = 0;  // bit r: the window of bar t0 + r holds a non-finite price
-    for (int r = 0; r < lim; ++r) {
-      const int t = t0 + r;
-      double tp = cur[r * 32];
-      if (!steady) {
-        if (!isfinite(tp)) {
-          last_bad = t;
-          tp = 0.0;
-          cur[r * 32] = 0.0;
-        }
-        if (last_bad > t - p) nanwin |= 1u << r;
-      }
-      const double gone = t >= p ? cur[(r - p) * 32] : 0.0;
-      sum = (sum + tp) - gone;
-      ml[r * 32] = sum * invp;
-    }
+    for (int r = 0; r < lim; ++r) cur[r * 32] = (((double)H[r] + (double)Lo[r]) + (double)Cl[r]) / 3.0;
     const int n8 = (lim + 7) & ~7;
     for (int r8 = 0; r8 < n8; r8 += 8) {
       double sma[8], acc[8];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        sma[u] = ml[(r8 + u) * 32];
-        acc[u] = 0.0;
+      for (int u = 0; u < 8; ++u) sma[u] = acc[u] = 0.0;
+      for (int i = 0; i < p; ++i) {
+        const double* wp = cur + (r8 - i) * 32;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) sma[u] += wp[u * 32];
       }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) sma[u] = sma[u] / dp;
       for (int i = 0; i < p; ++i) {
         const double* wp = cur + (r8 - i) * 32;
 #pragma unroll
@@ -647,10 +630,10 @@ __device__ void w_cci(const Warp& w, const Job& j, double* line) {
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
         const int r = r8 + u, t = t0 + r;
-        const float md = (float)(acc[u] * invp);
-        const float num = (float)(cur[r * 32] - sma[u]);
-        const float o = (num != 0.0f && md != 0.0f) ? fdiv(num, 0.015f * md) : 0.0f;
-        st[r] = (t >= p - 1 && !((nanwin >> r) & 1u)) ? o : qnan();
+        const double md = acc[u] / dp;
+        const double num = cur[r * 32] - sma[u];
+        const float o = (num != 0.0 && md != 0.0) ? (float)(num / (0.015 * md)) : 0.0f;
+        st[r] = t >= p - 1 ? o : qnan();
       }
     }
     w.flush(0, (float*)j.out[0], c);
@@ -736,7 +719,7 @@ __device__ void w_ema(const Warp& w, const Job& j) {
     if (all_lanes(cnt >= p - 1)) {
       const int n8 = w.lim8(c);
       for (int r8 = 0; r8 < n8; r8 += 8) {
-#pragma unroll
+#pragma unroll 1
         for (int u = 0; u < 8; ++u) {
           const R x = (R)X[r8 + u];
           y = copy ? x : fma(beta, y, kk * x);
@@ -788,7 +771,7 @@ __device__ void w_rsi(const Warp& w, const Job& j) {
       R xp = (R)X[-1];
       const int n8 = w.lim8(c);
       for (int r8 = 0; r8 < n8; r8 += 8) {
-#pragma unroll
+#pragma unroll 1
         for (int u = 0; u < 8; ++u) {
           const R x = (R)X[r8 + u];
           const R d = x - xp;
@@ -851,7 +834,7 @@ __device__ void w_macd(const Warp& w, const Job& j) {
     if (all_lanes(cnt >= ready)) {
       const int n8 = w.lim8(c);
       for (int r8 = 0; r8 < n8; r8 += 8) {
-#pragma unroll
+#pragma unroll 1
         for (int u = 0; u < 8; ++u) {
           const int r = r8 + u;
           const double x = (double)X[r];
@@ -944,7 +927,7 @@ __device__ void w_atr(const Warp& w, const Job& j, int mode) {
       R cp = (R)Cl[-1];
       const int n8 = w.lim8(c);
       for (int r8 = 0; r8 < n8; r8 += 8) {
-#pragma unroll
+#pragma unroll 1
         for (int u = 0; u < 8; ++u) {
           const int r = r8 + u;
           const R cl = (R)Cl[r];
@@ -1023,7 +1006,7 @@ __device__ void w_adx(const Warp& w, const Job& j, bool adx) {
       float hp = H[-1], lp = Lo[-1], cp = Cl[-1];
       const int n8 = w.lim8(c);
       for (int r8 = 0; r8 < n8; r8 += 8) {
-#pragma unroll
+#pragma unroll 1
         for (int u = 0; u < 8; ++u) {
           const int r = r8 + u;
           const float h = H[r], l = Lo[r];
@@ -1101,7 +1084,7 @@ __device__ void w_volume(const Warp& w, const Job& j, int mode) {
       float pp = I0[-1];
       const int n8 = w.lim8(c);
       for (int r8 = 0; r8 < n8; r8 += 8) {
-#pragma unroll
+#pragma unroll 1
         for (int u = 0; u < 8; ++u) {
           const int r = r8 + u;
           const double v = (double)I1[r];
