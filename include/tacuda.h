@@ -411,11 +411,17 @@ CTAPI_EXPORT ctStatus_t ct_b200_plan_destroy(ctB200Plan* plan);
  * fastest (also stored in the autotuner cache). Synchronises `stream`. */
 CTAPI_EXPORT ctStatus_t ct_b200_plan_autotune(ctB200Plan* plan, const ctB200Series* series,
                                               const ctB200Job* jobs, int numJobs, cudaStream_t stream);
-/* Launch shape chosen by a plan: engine (0 warp per series, 1 thread per
- * series, 2 warp per tile with look-back), bars per lane, warps per block,
- * block cap (0 = as many as fit). Null outputs are skipped. */
+/* Launch shape chosen by a plan: engine (0 warp-scan: a warp per series,
+ * 1 row-parallel: a CTA per 32 series, 2 look-back: a warp per tile), bars per
+ * lane, warps per block, block cap (0 = as many as fit). Null outputs are
+ * skipped. */
 CTAPI_EXPORT ctStatus_t ct_b200_plan_describe(const ctB200Plan* plan, int* engine, int* barsPerLane,
                                               int* warpsPerBlock, int* blocks);
+/* Candidates the last ct_b200_plan_autotune timed: up to maxOut entries of
+ * engine, bars per lane, warps per block and milliseconds per launch (null
+ * arrays are skipped). Returns how many it timed (0 before any autotune). */
+CTAPI_EXPORT int ct_b200_plan_candidates(const ctB200Plan* plan, int maxOut, int* engine, int* barsPerLane,
+                                         int* warpsPerBlock, float* ms);
 
 /* All selected candle patterns of a uniform batch in one pass, int32 signals
  * (pattern k of mask at d_out + k * seriesLen * numSeries). */

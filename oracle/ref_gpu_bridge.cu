@@ -18,7 +18,15 @@
 //     src/api/api_batch.cu:76-117);
 //   * src/api/BatchFused.cu FusedCall::launch: the fused per-row kernels of
 //     ct_{sma,ema,rsi,atr,macd,bbands,stochastic,wma,natr,stddev,sum,min,max,
-//     obv,mfi,ad,adosc}_batch_d (src/api/BatchFused.cu:178-213).
+//     obv,mfi,ad,adosc}_batch_d (src/api/BatchFused.cu:178-213);
+//   * the per-series ("plain", TACUDA_BATCH_FUSED=0) path of the batch entry
+//     points (src/api/api_batch.cu:478-533): for every series, the indicator
+//     object that the single-series ct_*_d entry constructs, calculate() on one
+//     stream (src/api/api_device.cu: ct_sma_d :539, ct_ema_d, ct_wma_d, ct_rsi_d,
+//     ct_atr_d :818, ct_adx_d, ct_bbands_d :1131, ct_stochastic_d :1053,
+//     ct_cci_d, ct_obv_d, ct_mfi_d, ct_willr_d). MACD's ct_macd_d runs MACDEXT,
+//     which needs the moving-average and TA-Lib 0.8.3 runner sources; it is not
+//     bridged.
 #include <cuda_runtime.h>
 
 #include <exception>
@@ -26,10 +34,19 @@
 #include "BatchFused.h"
 #include "BatchShort.h"
 #include <indicators/ADX.h>
+#include <indicators/ATR.h>
+#include <indicators/BBANDS.h>
 #include <indicators/CCI.h>
 #include <indicators/Correl.h>
 #include <indicators/DX.h>
+#include <indicators/EMA.h>
+#include <indicators/MFI.h>
+#include <indicators/OBV.h>
+#include <indicators/RSI.h>
+#include <indicators/SMA.h>
+#include <indicators/Stochastic.h>
 #include <indicators/WILLR.h>
+#include <indicators/WMA.h>
 
 namespace {
 
@@ -129,6 +146,37 @@ int refgpu_fused(int family, const float* in0, const float* in1, const float* in
   const td::FusedCall call = td::fused_call(static_cast<td::FusedFamily>(family), p, q, r, 1, up, dn);
   const ctStatus_t st = call.launch(in, out, T, S, s);
   return st == CT_STATUS_SUCCESS ? 0 : 10 + (int)st;
+}
+
+// Per-series path, family codes: 1 SMA, 2 EMA, 3 WMA, 4 RSI, 5 ATR, 6 ADX,
+// 7 BBANDS, 8 STOCH (slowK, slowD), 9 CCI, 10 OBV (close, volume), 11 MFI,
+// 12 WILLR. Inputs h, l, c, v as the family reads them; outputs o0..o2.
+int refgpu_plain(int family, const float* h, const float* l, const float* c, const float* v, float* o0, float* o1,
+                 float* o2, int T, int S, int p, int q, float up, float dn, void* stream) {
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  return guarded([&] {
+    for (int r = 0; r < S; ++r) {
+      const size_t off = (size_t)r * T;
+      const float *hr = h ? h + off : nullptr, *lr = l ? l + off : nullptr, *cr = c ? c + off : nullptr;
+      const float* vr = v ? v + off : nullptr;
+      float *a = o0 + off, *b = o1 ? o1 + off : nullptr, *d = o2 ? o2 + off : nullptr;
+      switch (family) {
+        case 1: tacuda::SMA(p).calculate(cr, a, T, s); break;
+        case 2: tacuda::EMA(p).calculate(cr, a, T, s); break;
+        case 3: tacuda::WMA(p).calculate(cr, a, T, s); break;
+        case 4: tacuda::RSI(p).calculate(cr, a, T, s); break;
+        case 5: tacuda::ATR(p, 0.0f).calculate(hr, lr, cr, a, T, s); break;
+        case 6: tacuda::ADX(p).calculate(hr, lr, cr, a, T, s); break;
+        case 7: tacuda::BBANDS(p, up, dn).calculate(cr, a, b, d, T, s); break;
+        case 8: tacuda::Stochastic(p, q).calculate(hr, lr, cr, a, b, T, s); break;
+        case 9: tacuda::CCI(p).calculate(hr, lr, cr, a, T, s); break;
+        case 10: tacuda::OBV().calculate(cr, vr, a, T, s); break;
+        case 11: tacuda::MFI(p).calculate(hr, lr, cr, vr, a, T, s); break;
+        case 12: tacuda::WILLR(p).calculate(hr, lr, cr, a, T, s); break;
+        default: throw std::exception();
+      }
+    }
+  });
 }
 
 }  // extern "C"

@@ -82,6 +82,8 @@ def _load() -> ct.CDLL:
     lib.ct_b200_plan_autotune.argtypes = [_P, ct.POINTER(ctB200Series), ct.POINTER(ctB200Job), _I, _P]
     lib.ct_b200_plan_describe.argtypes = [_P, ct.POINTER(_I), ct.POINTER(_I), ct.POINTER(_I), ct.POINTER(_I)]
     lib.ct_b200_plan_destroy.argtypes = [_P]
+    lib.ct_b200_plan_candidates.argtypes = [_P, _I, _P, _P, _P, _P]
+    lib.ct_b200_plan_candidates.restype = _I
     lib.ct_b200_cdl_batch_d.argtypes = [_P, _P, _P, _P, _P, _I, _I, ct.c_uint64, _P]
     lib.ct_b200_alpha_checkpoint_doubles.argtypes = [_I]
     lib.ct_b200_alpha_checkpoint_doubles.restype = ct.c_longlong
@@ -303,6 +305,20 @@ class Plan:
         call_status(get_lib().ct_b200_plan_describe(self.handle, ct.byref(m), ct.byref(k), ct.byref(w),
                                                     ct.byref(b)), "ct_b200_plan_describe")
         return {"mode": m.value, "bars_per_lane": k.value, "warps_per_block": w.value, "max_blocks": b.value}
+
+    ENGINES = {0: "warp-scan", 1: "row-parallel", 2: "look-back"}
+
+    def candidates(self) -> list[dict]:
+        """Launch shapes the last autotune() timed, with milliseconds per launch."""
+        lib = get_lib()
+        n = lib.ct_b200_plan_candidates(self.handle, 0, None, None, None, None)
+        if n <= 0:
+            return []
+        m, k, w = (np.zeros(n, np.int32) for _ in range(3))
+        ms = np.zeros(n, np.float32)
+        lib.ct_b200_plan_candidates(self.handle, n, m.ctypes.data, k.ctypes.data, w.ctypes.data, ms.ctypes.data)
+        return [{"engine": self.ENGINES.get(int(m[i]), str(int(m[i]))), "bars_per_lane": int(k[i]),
+                 "warps_per_block": int(w[i]), "ms": float(ms[i])} for i in range(n)]
 
     def close(self) -> None:
         if self.handle:

@@ -322,6 +322,11 @@ struct ctB200Plan {
   tb::SchedulePlan sched;
   tb::LaunchStats stats;
   int device = 0;
+  struct Tried {
+    tb::SchedulePlan plan;
+    float ms;
+  };
+  std::vector<Tried> tried;  // candidates of the last autotune and their times per launch
 };
 
 extern "C" {
@@ -1007,6 +1012,9 @@ ctStatus_t ct_b200_fused_batch(const ctB200Series* hs, const ctB200Job* hjobs, i
   }
   const char* copy_err = nullptr;
   const int rows = (L.S + nchunks - 1) / nchunks;
+  // every chunk runs the plan of the whole batch, so its rows get the bits the
+  // device entry gives them (an engine's rows never depend on the other rows)
+  const tb::SchedulePlan whole = tb::plan_for(L, (long long)L.S * L.T, L.T);
   for (int c = 0; c < nchunks && st == CT_STATUS_SUCCESS && !copy_err; ++c) {
     const int r0 = c * rows, r1 = std::min(L.S, r0 + rows);
     if (r0 >= r1) break;
@@ -1027,7 +1035,7 @@ ctStatus_t ct_b200_fused_batch(const ctB200Series* hs, const ctB200Job* hjobs, i
       const int nout = jb.family == tb::F_CDL ? 1 : output_count(jb.family);
       for (int o = 0; o < nout; ++o) jb.out[o] = static_cast<char*>(jb.out[o]) + off * 4;
     }
-    st = launch(Lc, (long long)cnt, L.T, nullptr, cs, who);
+    st = launch(Lc, (long long)cnt, L.T, &whole, cs, who);
     if (st != CT_STATUS_SUCCESS) break;
     for (const Back& b : back)
       if (cudaMemcpyAsync(b.host + off, b.dev + off, cnt * 4, cudaMemcpyDeviceToHost, cs) != cudaSuccess)
@@ -1488,47 +1496,45 @@ ctStatus_t ct_b200_plan_autotune(ctB200Plan* plan, const ctB200Series* series, c
   clear_error();
   const char* who = "ct_b200_plan_autotune";
   if (!plan) return fail(CT_STATUS_INVALID_ARGUMENT, std::string(who) + ": null plan");
-  const int ks[3] = {4, 8, 16};
-  const int ws[3] = {4, 8, 16};
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   float best = 1e30f;
   tb::SchedulePlan bestPlan = plan->sched;
-  // candidates: warp-per-series and look-back engines over round widths and
-  // block sizes, the series-parallel engine over group counts
+  // candidates: the row-parallel engine; the warp-scan engine over round
+  // widths and block sizes; the look-back engine where its tiles fit the rows
   std::vector<tb::SchedulePlan> cands;
-  for (int mode : {0, 2})
-      for (int ki : ks) {
-        if (ki == 4 && plan->maxlen > 4096) continue;
-        if (mode == 2 && plan->maxlen < 4ll * 32 * ki) continue;
-        for (int wi : ws) {
-          tb::SchedulePlan cand;
-          cand.mode = mode;
-          cand.k = ki;
-          cand.warps_per_block = wi;
-          cands.push_back(cand);
-        }
-      }
-  for (int g : {1, 2, 4, 8}) {
-    if (g * plan->njobs > tb::kMaxJobs) continue;
+  {
     tb::SchedulePlan cand;
     cand.mode = 1;
-    cand.groups = g;
     cands.push_back(cand);
   }
-  (void)ws;
+  for (int mode : {0, 2})
+    for (int ki : {4, 8, 16}) {
+      if (ki == 4 && plan->maxlen > 4096) continue;
+      if (mode == 2 && plan->maxlen < 4ll * 32 * ki) continue;
+      for (int wi : {4, 8, 16}) {
+        tb::SchedulePlan cand;
+        cand.mode = mode;
+        cand.k = ki;
+        cand.warps_per_block = wi;
+        cands.push_back(cand);
+      }
+    }
+  plan->tried.clear();
   for (const tb::SchedulePlan& cand : cands) {
-    {
-      ctStatus_t st = plan_launch(plan, series, jobs, numJobs, cand, stream, who, nullptr);  // warm-up
-      if (st != CT_STATUS_SUCCESS) continue;
-      cudaEventRecord(e0, stream);
-      for (int r = 0; r < 3; ++r) plan_launch(plan, series, jobs, numJobs, cand, stream, who, nullptr);
-      cudaEventRecord(e1, stream);
-      if (cudaEventSynchronize(e1) != cudaSuccess) continue;
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      if (ms < best) { best = ms; bestPlan = cand; }
+    ctStatus_t st = plan_launch(plan, series, jobs, numJobs, cand, stream, who, nullptr);  // warm-up
+    if (st != CT_STATUS_SUCCESS) continue;
+    cudaEventRecord(e0, stream);
+    for (int r = 0; r < 3; ++r) plan_launch(plan, series, jobs, numJobs, cand, stream, who, nullptr);
+    cudaEventRecord(e1, stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess) continue;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    plan->tried.push_back({cand, ms / 3.0f});
+    if (ms < best) {
+      best = ms;
+      bestPlan = cand;
     }
   }
   cudaEventDestroy(e0);
@@ -1553,6 +1559,21 @@ ctStatus_t ct_b200_plan_describe(const ctB200Plan* plan, int* engine, int* barsP
   if (warpsPerBlock) *warpsPerBlock = plan->sched.warps_per_block;
   if (blocks) *blocks = plan->sched.max_blocks;
   return CT_STATUS_SUCCESS;
+}
+
+int ct_b200_plan_candidates(const ctB200Plan* plan, int maxOut, int* engine, int* barsPerLane, int* warpsPerBlock,
+                            float* ms) {
+  clear_error();
+  if (!plan) return 0;
+  const int n = (int)plan->tried.size();
+  for (int i = 0; i < n && i < maxOut; ++i) {
+    const ctB200Plan::Tried& t = plan->tried[(size_t)i];
+    if (engine) engine[i] = t.plan.mode;
+    if (barsPerLane) barsPerLane[i] = t.plan.k;
+    if (warpsPerBlock) warpsPerBlock[i] = t.plan.warps_per_block;
+    if (ms) ms[i] = t.ms;
+  }
+  return n;
 }
 
 ctStatus_t ct_b200_plan_destroy(ctB200Plan* plan) {

@@ -1,5 +1,6 @@
 // Row-parallel engine: kernel and launcher (see rows.cuh for the design).
 #include "rows.cuh"
+#include "rows_bars.cuh"
 
 #include <algorithm>
 #include <climits>
@@ -13,7 +14,24 @@
 namespace tb {
 namespace rows {
 
-// Per-warp history line (entries per lane, a power of two; 0: none).
+// Jobs run bar-parallel (rows_bars.cuh), as a mask of families. CCI sums its
+// windows directly in either form, so it always goes bar-parallel, where a
+// team of warps shares it. WILLR and STOCH give the same bits in both forms
+// (window extremes are exact); bar-parallel costs more instructions but
+// splits over a team, which pays only when few jobs share the CTA. The other
+// window families keep their running row-sequential form.
+static_assert(F_COUNT <= 64, "bar-parallel family mask holds 64 families");
+inline unsigned long long bar_parallel_mask(const Launch& L) {
+  unsigned long long m = 1ull << F_CCI;
+  if (L.njobs <= 4) m |= (1ull << F_WILLR) | (1ull << F_STOCH);
+  return m;
+}
+__host__ __device__ inline bool bar_parallel(unsigned long long mask, int family) {
+  return family >= 0 && family < 64 && ((mask >> family) & 1ull) != 0;
+}
+
+// Per-lane history line of a row-sequential job (entries per lane, a power of
+// two; 0: none).
 __host__ __device__ inline int line_entries(const Job& j) {
   int need = 0;
   switch (j.family) {
@@ -27,12 +45,19 @@ __host__ __device__ inline int line_entries(const Job& j) {
   return cap;
 }
 
-__host__ __device__ inline int line_bytes(const Job& j) {
+// Bytes of a job warp's own lines.
+__host__ __device__ inline int line_bytes(const Job& j, unsigned long long bp) {
+  if (bar_parallel(bp, j.family)) {
+    switch (j.family) {
+      case F_STOCH: return 2 * kBarLine * 4;
+      case F_CCI: return kBarLine * 8;
+      default: return 0;
+    }
+  }
   const int cap = line_entries(j);
   switch (j.family) {
     case F_WILLR: return 2 * 32 * cap * 4;
     case F_STOCH: return 4 * 32 * cap * 4;
-    case F_CCI: return (j.ip[0] + C) * 32 * 8;
     case F_MFI: return 2 * 32 * cap * 8;
     default: return 0;
   }
@@ -43,7 +68,6 @@ __host__ __device__ inline int out_count(int family) {
 }
 
 __device__ void run_job(const Warp& w, const Job& j, unsigned char* line) {
-  const int cap = line_entries(j);
   const bool f32 = j.ip[0] <= kFp32MaxPeriod;
   switch (j.family) {
     case F_SMA: w_sum_window(w, j, 0); break;
@@ -52,13 +76,17 @@ __device__ void run_job(const Warp& w, const Job& j, unsigned char* line) {
     case F_BBANDS: w_moment_window(w, j, 0); break;
     case F_STDDEV: w_moment_window(w, j, 1); break;
     case F_VAR: w_moment_window(w, j, 2); break;
-    case F_WILLR: w_willr(w, j, reinterpret_cast<float*>(line), cap); break;
-    case F_STOCH:
-      if (j.ip[1] == 3) w_stoch<3>(w, j, reinterpret_cast<float*>(line), cap);
-      else w_stoch<0>(w, j, reinterpret_cast<float*>(line), cap);
+    case F_WILLR:
+      if (bar_parallel(w.lay->bp_mask, F_WILLR)) b_willr(w, j);
+      else w_willr(w, j, reinterpret_cast<float*>(line), line_entries(j));
       break;
-    case F_CCI: w_cci(w, j, reinterpret_cast<double*>(line)); break;
-    case F_MFI: w_mfi(w, j, reinterpret_cast<double*>(line), cap); break;
+    case F_STOCH:
+      if (bar_parallel(w.lay->bp_mask, F_STOCH)) b_stoch(w, j, reinterpret_cast<float*>(line));
+      else if (j.ip[1] == 3) w_stoch<3>(w, j, reinterpret_cast<float*>(line), line_entries(j));
+      else w_stoch<0>(w, j, reinterpret_cast<float*>(line), line_entries(j));
+      break;
+    case F_CCI: b_cci(w, j, reinterpret_cast<double*>(line)); break;
+    case F_MFI: w_mfi(w, j, reinterpret_cast<double*>(line), line_entries(j)); break;
     case F_EMA: case F_RMA:
       if (f32) w_ema<float>(w, j); else w_ema<double>(w, j);
       break;
@@ -228,6 +256,8 @@ __global__ void __launch_bounds__(32 * (kMaxConsumers + 1), 1) rows_kernel(const
   w.T = L.T;
   w.s0T = (long long)blockIdx.x * 32 * L.T;
   w.nvalid = (int)min(32ll, (long long)L.S - (long long)blockIdx.x * 32);
+  w.tk = lay.warp_team[warp] & 255;
+  w.tm = lay.warp_team[warp] >> 8;
   run_job(w, L.jobs[lay.warp_job[warp]], smem + lay.line_off[warp]);
 }
 
@@ -259,39 +289,76 @@ struct DevState {
 std::mutex g_mutex;
 std::vector<DevState> g_dev;
 
-// Relative issue cost per bar of each family's job warp (instructions per
-// bar of its steady loop, rounded), and of the producer per staged plane.
-int family_cost(const Job& j) {
+// Relative time of a job's warp over a chunk when it runs alone, from single
+// job launches at 4000 x 234 (microseconds above the launch's fixed cost),
+// for the warp placement and the team sizes. A bar-parallel job's figure is
+// for one warp; a team of m divides it by m.
+int family_cost(const Job& j, unsigned long long bp) {
+  const int p = j.ip[0];
   switch (j.family) {
-    case F_CCI: return 30 + 5 * j.ip[0];
-    case F_STOCH: return 45;
-    case F_ADX: case F_DX: return 40;
-    case F_MFI: return 35;
-    case F_BBANDS: return 30;
-    case F_WILLR: return 25;
-    case F_MACD: return 18;
-    case F_STDDEV: case F_VAR: return 22;
-    case F_RSI: return 16;
-    case F_ATR: case F_NATR: return 14;
-    case F_WMA: return 13;
-    case F_SMA: case F_SUM: return 11;
-    case F_OBV: return 8;
-    case F_EMA: case F_RMA: return 6;
-    default: return 20 + 2 * j.ip[0];
+    case F_CCI: return 14 * p;
+    case F_MFI: return 44;
+    case F_STOCH: return bar_parallel(bp, F_STOCH) ? 7 * p : 37;
+    case F_BBANDS: return 35;
+    case F_WILLR: return bar_parallel(bp, F_WILLR) ? 6 * p : 33;
+    case F_ADX: case F_DX: return 27;
+    case F_STDDEV: case F_VAR: return 25;
+    case F_MACD: return 21;
+    case F_RSI: return 18;
+    case F_ATR: case F_NATR: return 11;
+    case F_OBV: case F_AD: return 10;
+    case F_WMA: return 9;
+    case F_SMA: case F_SUM: return 9;
+    case F_EMA: case F_RMA: return 4;
+    default: return 10 + p;
   }
 }
 
-// Warp w of a CTA issues from sub-partition w % 4. The job warps and the
-// producer are placed longest-first on the least loaded sub-partition, so the
-// heaviest jobs do not share one.
+// Job warps: one per job, and spare warps up to kMaxConsumers go to the
+// bar-parallel jobs as team members (rows split between them), each time to
+// the job whose warps carry the most work, while that is more than the
+// heaviest row-sequential job's. Warp w of a CTA issues from sub-partition
+// w % 4: the job warps and the producer are placed longest-first on the least
+// loaded sub-partition, so the heaviest warps do not share one.
 void assign_warps(const Launch& L, Layout& lay) {
-  const int n = L.njobs + 1;  // jobs + producer
-  int cost[kMaxConsumers + 1], order[kMaxConsumers + 1];
-  for (int i = 0; i < L.njobs; ++i) cost[i] = family_cost(L.jobs[i]);
-  cost[L.njobs] = 4 * lay.nplanes;
-  for (int i = 0; i < n; ++i) order[i] = i;
+  int team[kMaxConsumers];
+  int nw = L.njobs, seq_max = 0;
+  for (int j = 0; j < L.njobs; ++j) {
+    team[j] = 1;
+    if (!bar_parallel(lay.bp_mask, L.jobs[j].family)) seq_max = std::max(seq_max, family_cost(L.jobs[j], lay.bp_mask));
+  }
+  while (nw < kMaxConsumers) {
+    int best = -1;
+    double bc = (double)seq_max;
+    for (int j = 0; j < L.njobs; ++j) {
+      if (!bar_parallel(lay.bp_mask, L.jobs[j].family)) continue;
+      const double c = (double)family_cost(L.jobs[j], lay.bp_mask) / team[j];
+      if (c > bc) {
+        bc = c;
+        best = j;
+      }
+    }
+    if (best < 0) break;
+    ++team[best];
+    ++nw;
+  }
+  const int n = nw + 1;  // job warps + producer
+  int item_job[kMaxConsumers + 1], item_k[kMaxConsumers + 1], order[kMaxConsumers + 1];
+  double cost[kMaxConsumers + 1];
+  int i = 0;
+  for (int j = 0; j < L.njobs; ++j)
+    for (int k = 0; k < team[j]; ++k, ++i) {
+      item_job[i] = j;
+      item_k[i] = k;
+      cost[i] = (double)family_cost(L.jobs[j], lay.bp_mask) / team[j];
+    }
+  item_job[i] = -1;
+  item_k[i] = 0;
+  cost[i] = 4.0 * lay.nplanes;
+  for (int k = 0; k < n; ++k) order[k] = k;
   std::stable_sort(order, order + n, [&](int a, int b) { return cost[a] > cost[b]; });
-  int load[4] = {0, 0, 0, 0}, used[4] = {0, 0, 0, 0};
+  double load[4] = {0, 0, 0, 0};
+  int used[4] = {0, 0, 0, 0};
   for (int k = 0; k < n; ++k) {
     int best = -1;
     for (int q = 0; q < 4; ++q) {
@@ -301,11 +368,13 @@ void assign_warps(const Launch& L, Layout& lay) {
     }
     const int w = best + 4 * used[best];
     ++used[best];
-    load[best] += cost[order[k]];
-    const int item = order[k];
-    lay.warp_job[w] = item == L.njobs ? -1 : item;
-    if (item == L.njobs) lay.producer_warp = w;
+    const int it = order[k];
+    load[best] += cost[it];
+    lay.warp_job[w] = item_job[it];
+    lay.warp_team[w] = item_job[it] < 0 ? (1 << 8) : (item_k[it] | team[item_job[it]] << 8);
+    if (item_job[it] < 0) lay.producer_warp = w;
   }
+  lay.nconsumers = nw;
 }
 
 }  // namespace
@@ -317,8 +386,7 @@ bool supports(const Launch& L, long long max_len) {
     const Job& jb = L.jobs[j];
     if (jb.prec != 0 || !family_supported(jb.family)) return false;
     if (rows_halo(jb) > kMaxHalo) return false;
-    if (line_entries(jb) > kMaxLine) return false;
-    if (jb.family == F_CCI && jb.ip[0] > kMaxLine) return false;
+    if (jb.family != F_CCI && line_entries(jb) > kMaxLine) return false;
   }
   return true;
 }
@@ -368,27 +436,27 @@ cudaError_t launch(Launch& L, long long max_len, cudaStream_t stream, LaunchStat
   off += 2 * lay.NS * 8;
   lay.tab_off = off;
   off += 64 * 8 + 16;
-  lay.nconsumers = L.njobs;
+  lay.bp_mask = bar_parallel_mask(L);
   assign_warps(L, lay);
-  for (int w = 0; w <= L.njobs; ++w) {
+  for (int w = 0; w <= lay.nconsumers; ++w) {
     const int jb = lay.warp_job[w];
     off = (off + 15) & ~15;
     lay.stage_off[w] = off;
     if (jb < 0) continue;
-    off += out_count(L.jobs[jb].family) * 32 * (C + 1) * 4;
+    if (!bar_parallel(lay.bp_mask, L.jobs[jb].family)) off += out_count(L.jobs[jb].family) * 32 * (C + 1) * 4;
     off = (off + 15) & ~15;
     lay.line_off[w] = off;
-    off += line_bytes(L.jobs[jb]);
+    off += line_bytes(L.jobs[jb], lay.bp_mask);
   }
   lay.total = (off + 127) & ~127;
   if (lay.total > ds->smem_optin) return cudaErrorNotSupported;
   const long long groups = ((long long)L.S + 31) / 32;
   if (groups > INT_MAX) return cudaErrorInvalidValue;
-  const int threads = 32 * (L.njobs + 1);
+  const int threads = 32 * (lay.nconsumers + 1);
   rows_kernel<<<(unsigned)groups, threads, lay.total, stream>>>(L, lay);
   if (stats) {
     stats->blocks = (int)groups;
-    stats->warps_per_block = L.njobs + 1;
+    stats->warps_per_block = lay.nconsumers + 1;
     stats->smem_per_block = lay.total;
     stats->k = 0;
     stats->blocks_per_sm = 1;

@@ -44,8 +44,8 @@ namespace rows {
 
 constexpr int C = 32;                 // bars per chunk
 constexpr int kMaxHalo = 64;          // bars of history a job may read before a chunk
-constexpr int kMaxConsumers = 15;     // job warps per CTA (one more warp stages the inputs)
 constexpr int kMaxLine = 64;          // per-lane history of the line-keeping families
+constexpr int kMaxConsumers = 19;     // job warps per CTA (one more warp stages the inputs)
 constexpr int kFp32MaxPeriod = 32;    // recurrences up to this period keep float32 state
 constexpr unsigned long long kWaitNs = 1000000000ull;  // one mbarrier wait gives up after 1 s
 constexpr unsigned long long kStallWaitNs = 1000000ull;  // 1 ms under the stall test knob
@@ -62,6 +62,8 @@ struct Layout {
   int nconsumers;
   int producer_warp;
   int warp_job[kMaxConsumers + 1];    // job of each warp, -1 for the producer
+  int warp_team[kMaxConsumers + 1];   // member k and team size m of a bar-parallel job: k | m << 8
+  unsigned long long bp_mask;         // families that run bar-parallel (1 << family)
   int stage_off[kMaxConsumers + 1];   // [nout][32][C+1] floats
   int line_off[kMaxConsumers + 1];    // per-warp history lines
   int total;
@@ -153,6 +155,20 @@ __device__ __forceinline__ float fdiv(float a, float b) {
 }
 __device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
 
+// x / d correctly rounded, from y = RN(1/d), without a divide: the product
+// x*y is within 1.5 ulp of the quotient, a first FMA correction brings it
+// within one ulp, and then one more correction rounds it correctly
+// (Markstein's theorem: P. Markstein, "Computation of elementary functions on
+// the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990). Holds
+// for normal operands; zeros and non-finite quotients pass through x*y, which
+// is already right for them.
+__device__ __forceinline__ double div_by(double x, double d, double y) {
+  const double q0 = x * y;
+  const double q1 = fma(fma(-q0, d, x), y, q0);
+  const double q2 = fma(fma(-q1, d, x), y, q1);
+  return (q0 == 0.0 || !(fabs(q0) < __longlong_as_double(0x7ff0000000000000ll))) ? q0 : q2;
+}
+
 struct Warp {
   unsigned char* smem;
   const Layout* lay;
@@ -170,10 +186,22 @@ struct Warp {
   long long T;     // their length
   long long s0T;   // element offset of the group's first row
   int nvalid;      // rows of the group that exist
+  int tk, tm;      // bar-parallel jobs: this warp takes rows tk, tk + tm, ... of the group
 
-  __device__ __forceinline__ const float* X(int c, int plane) const {
+  __device__ __forceinline__ const float* X(int c, int plane) const { return Xrow(c, plane, lane); }
+  // row r's line of chunk c: [i] is bar c*C + i, i >= -Hs*C
+  __device__ __forceinline__ const float* Xrow(int c, int plane, int r) const {
     const float* ring = reinterpret_cast<const float*>(smem + lay->ring_off);
-    return ring + ((size_t)lay->plane_slot[plane] * 32 + lane) * RS + (Hs + c % NS) * C;
+    return ring + ((size_t)lay->plane_slot[plane] * 32 + r) * RS + (Hs + c % NS) * C;
+  }
+  // output offset and length of row r of the group (length 0 for a missing row)
+  __device__ __forceinline__ long long row_len(int r, long long& base) const {
+    if (uni) {
+      base = s0T + (long long)r * T;
+      return r < nvalid ? T : 0;
+    }
+    base = tbase[r];
+    return base >= 0 ? tn[r] : 0;
   }
   __device__ __forceinline__ int lim(int c) const { return min(C, maxn - c * C); }
   // bars of chunk c a steady (unrolled by 8) loop covers
@@ -578,65 +606,6 @@ __device__ void w_stoch(const Warp& w, const Job& j, float* line, int cap) {
     }
     w.flush(0, (float*)j.out[0], c);
     w.flush(1, (float*)j.out[1], c);
-    w.release(c);
-  }
-}
-
-// CCI (src/indicators/CCI.cu:11-40), in the reference's arithmetic: typical
-// price (((double)h + l) + c) / 3.0, the window sum taken directly from the
-// newest bar back, sma = sum / p, the mean absolute deviation summed in the
-// same order, md = dev / p, and (tp - sma) / (0.015 md) in FP64 when both are
-// nonzero, rounded once to float. Direct sums keep a constant window's
-// deviation exactly zero (a running sum would leave rounding noise that the
-// quotient turns into +-66.67), and a non-finite price makes every window
-// holding it NaN without extra bookkeeping.
-//
-// Per chunk, the typical prices of the chunk go into a per-lane line behind
-// the p of the chunk before (line[(p+r)*32], r = -p .. 31); both sums run for
-// 8 bars at a time, so every bar's sum is an independent chain.
-__device__ void w_cci(const Warp& w, const Job& j, double* line) {
-  const int ph = j.in[0], plo = j.in[1], pc = j.in[2], p = j.ip[0];
-  const double dp = (double)p;
-  double* tl = line + w.lane;  // [(p + r) * 32]
-  for (int c = 0; c < w.nchunks; ++c) {
-    if (!w.wait(c)) return;
-    const float* H = w.X(c, ph);
-    const float* Lo = w.X(c, plo);
-    const float* Cl = w.X(c, pc);
-    float* st = w.stage_row(0);
-    const int t0 = c * C, lim = w.lim(c);
-    // the previous chunk's last p typical prices move to the front
-    if (c > 0)
-      for (int i = 0; i < p; ++i) tl[i * 32] = tl[(i + C) * 32];
-    double* cur = tl + p * 32;  // cur[r * 32]: bar t0 + r
-    for (int r = 0; r < lim; ++r) cur[r * 32] = (((double)H[r] + (double)Lo[r]) + (double)Cl[r]) / 3.0;
-    const int n8 = (lim + 7) & ~7;
-    for (int r8 = 0; r8 < n8; r8 += 8) {
-      double sma[8], acc[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) sma[u] = acc[u] = 0.0;
-      for (int i = 0; i < p; ++i) {
-        const double* wp = cur + (r8 - i) * 32;
-#pragma unroll
-        for (int u = 0; u < 8; ++u) sma[u] += wp[u * 32];
-      }
-#pragma unroll
-      for (int u = 0; u < 8; ++u) sma[u] = sma[u] / dp;
-      for (int i = 0; i < p; ++i) {
-        const double* wp = cur + (r8 - i) * 32;
-#pragma unroll
-        for (int u = 0; u < 8; ++u) acc[u] += fabs(wp[u * 32] - sma[u]);
-      }
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int r = r8 + u, t = t0 + r;
-        const double md = acc[u] / dp;
-        const double num = cur[r * 32] - sma[u];
-        const float o = (num != 0.0 && md != 0.0) ? (float)(num / (0.015 * md)) : 0.0f;
-        st[r] = t >= p - 1 ? o : qnan();
-      }
-    }
-    w.flush(0, (float*)j.out[0], c);
     w.release(c);
   }
 }

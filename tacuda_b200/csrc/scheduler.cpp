@@ -75,8 +75,9 @@ SchedulePlan plan_for(const Launch& L, long long total_bars, long long max_len) 
   SchedulePlan p;
   // Engine by batch shape, as the reference's dispatcher picks its fused path
   // when seriesLen <= 4 * numSeries (src/api/BatchFused.cu:158-176):
-  //  * row-parallel: a thread per row and job; every row walks its bars in
-  //    TA-Lib's order, with no scans;
+  //  * row-parallel: a CTA per 32 rows, a warp per job (lanes are the rows,
+  //    each walking its bars in TA-Lib's order with no scans) or a team of
+  //    warps per direct-window job (lanes are the bars of one row);
   //  * look-back: few long rows, rounds of one row on different warps chained
   //    by decoupled look-back;
   //  * warp-scan otherwise: a warp per row, a round's bars split over lanes.

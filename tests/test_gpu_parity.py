@@ -44,8 +44,9 @@ def run_case(name, params, shape, seed=6):
 
 @pytest.fixture(params=["sp", "ws", "lb"])
 def mode(request):
-    """Every engine: series-parallel (thread per series), warp per series, and
-    warp per tile chained by decoupled look-back."""
+    """Every engine: row-parallel (a CTA per 32 rows, "sp"), warp-scan (a warp
+    per series, "ws"), and look-back (a warp per tile chained by decoupled
+    look-back, "lb")."""
     os.environ["TACUDA_B200_MODE"] = request.param
     yield request.param
     del os.environ["TACUDA_B200_MODE"]
@@ -128,7 +129,7 @@ def test_stream_zero_and_user_stream_agree():
         np.testing.assert_array_equal(x.view(np.uint32), y.view(np.uint32))
 
 
-@pytest.mark.parametrize("name", ["ema", "rsi", "macd", "atr", "adx", "bbands", "stoch", "cci", "mfi", "obv"])
+@pytest.mark.parametrize("name", ["ema", "rsi", "macd", "atr", "adx", "bbands", "stoch", "cci", "mfi", "obv", "willr"])
 def test_row_independence(name, mode):
     """With the engine pinned, as the reference pins its fused path with
     TACUDA_BATCH_FUSED=1, rows, their order, batch size and future bars cannot
