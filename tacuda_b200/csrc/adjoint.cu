@@ -1,8 +1,8 @@
 // Differentiable EMA / MACD / RSI with a per-series smoothing coefficient
 // alpha, and their hand-written adjoint.
 //
-// Forward (one thread per series, TA-Lib's structure with alpha in place of
-// the recurrence coefficient; periods fix the lookback and the seeds):
+// Forward (TA-Lib's structure with alpha in place of the recurrence
+// coefficient; periods fix the lookback and the seeds):
 //   EMA(p):  mean of x[0..p-1] at bar p-1, then y = fma(1-a, y, a*x)
 //            (talib08 TA_EMA; a = 2/(p+1) gives TA_EMA's coefficients).
 //   MACD(fast, slow, signal): slow EMA with TA-Lib's 2/(slow+1); fast EMA

@@ -14,7 +14,7 @@
 #pragma once
 
 #include "engine.h"
-#include "sp_candles.cuh"
+#include "cdl_rules.cuh"
 
 namespace tb {
 namespace cdl {
@@ -22,7 +22,7 @@ namespace cdl {
 constexpr int kTileBars = 256;             // bars per tile = threads per block
 constexpr int kHalo = 16;                  // staged bars before the tile
 constexpr int kSpan = kTileBars + kHalo;
-constexpr int kAnchors = kTileBars + sp::kCdlBack;
+constexpr int kAnchors = kTileBars + rules::kCdlBack;
 
 struct TileSmem {
   float o[kSpan], h[kSpan], l[kSpan], c[kSpan];
@@ -53,10 +53,10 @@ struct TileBars {
   // TA-Lib candle average of setting st anchored at bar t-d:
   // factor * (sum / count) / divisor, the mean precomputed per anchor.
   __device__ __forceinline__ double AVG(int st, int d) const {
-    const int slot = sp::set_slot(st);
-    const double factor = (double)sp::set_factor(st);
+    const int slot = rules::set_slot(st);
+    const double factor = (double)rules::set_factor(st);
     if (slot < 0) return factor * RB(d);
-    const double m = s->mean[slot][i - kHalo - d + sp::kCdlBack];
+    const double m = s->mean[slot][i - kHalo - d + rules::kCdlBack];
     return slot == 2 ? factor * m / 2.0 : factor * m;
   }
 };
@@ -98,18 +98,18 @@ __global__ void __launch_bounds__(kTileBars) tile_kernel(const __grid_constant__
         const float o = ok ? A.plane[0][g] : 0.0f, h = ok ? A.plane[1][g] : 0.0f;
         const float l = ok ? A.plane[2][g] : 0.0f, c = ok ? A.plane[3][g] : 0.0f;
         sm.o[i] = o; sm.h[i] = h; sm.l[i] = l; sm.c[i] = c;
-        sm.rng[0][i] = sp::cdl_range(sp::CR_BODY, o, h, l, c);
-        sm.rng[1][i] = sp::cdl_range(sp::CR_HL, o, h, l, c);
-        sm.rng[2][i] = sp::cdl_range(sp::CR_SHADOW, o, h, l, c);
+        sm.rng[0][i] = rules::cdl_range(rules::CR_BODY, o, h, l, c);
+        sm.rng[1][i] = rules::cdl_range(rules::CR_HL, o, h, l, c);
+        sm.rng[2][i] = rules::cdl_range(rules::CR_SHADOW, o, h, l, c);
         sm.us[i] = (double)h - fmax((double)o, (double)c);
         sm.ls[i] = fmin((double)o, (double)c) - (double)l;
       }
       __syncthreads();
       for (int j = tid; j < 4 * kAnchors; j += kTileBars) {
         const int slot = j / kAnchors, a = j - slot * kAnchors;
-        const long long ta = t0 - sp::kCdlBack + a;  // anchor bar in the row
-        const int per = sp::kSlotPeriod[slot];
-        const int ia = kHalo - sp::kCdlBack + a;     // staged index of the anchor
+        const long long ta = t0 - rules::kCdlBack + a;  // anchor bar in the row
+        const int per = rules::kSlotPeriod[slot];
+        const int ia = kHalo - rules::kCdlBack + a;     // staged index of the anchor
         const double* r = sm.rng[slot_range(slot)];
         double m;
         const long long start = ta - per < 0 ? 0 : ta - per;
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(kTileBars) tile_kernel(const __grid_constant__
           while (mask) {
             const int k = __ffsll((long long)mask) - 1;
             mask &= mask - 1;
-            const int v = t >= sp::kCdlLookbackDev[k] ? sp::cdl_eval(k, b) : 0;
+            const int v = t >= rules::kCdlLookbackDev[k] ? rules::cdl_eval(k, b) : 0;
             const long long at = (long long)k * j.cdl_stride + base + t;
             if (j.cdl_int32) reinterpret_cast<int*>(j.out[0])[at] = v;
             else reinterpret_cast<float*>(j.out[0])[at] = (float)v;

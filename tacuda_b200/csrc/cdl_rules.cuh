@@ -1,34 +1,28 @@
-// Candlestick engine (series-parallel): the 61 TA-Lib CDL patterns (plus the
-// reference's legacy bullish/bearish engulfing split) for every bar.
-//
-// TA-Lib's candle settings average one of three ranges (real body |c-o|,
-// high-low, upper+lower shadows) over the 10 or 5 bars before an anchor bar
-// (include/utils/CandleUtils.h:37-63, 1466-1495). Per chunk, the first candle
-// warp of a group writes the four distinct trailing sums (body/10, high-low/10,
-// shadows/10, high-low/5) for the anchors r-4 .. C-1 of its 32 rows into a
-// shared table, sliding them in FP64: the ranges of float32 bars are exact in
-// FP64 and so are their sums, so the table equals the reference's per-call
-// re-summing bit for bit. Every candle warp of the group then evaluates its own
-// subset of patterns bar by bar from the staged bars and the table and writes
-// each pattern through a transpose buffer as coalesced rows (int32 or float).
+// TA-Lib's 61 candlestick pattern rules (plus the reference's legacy bullish /
+// bearish engulfing split) as templates over a bar view B, which provides the
+// bars before the current one (O/H/L/C(d), d bars back), their real body and
+// shadows in FP64, and AVG(setting, d): TA-Lib's candle average of a setting
+// anchored d bars back (include/utils/CandleUtils.h:37-63, 1466-1495).
+// The candle tile kernel (candles.cuh) supplies the view.
 #pragma once
 
-#include "sp_families.cuh"
+#include "common.cuh"
+#include "engine.h"
 
 namespace tb {
-namespace sp {
+namespace rules {
 
 enum CdlRange { CR_BODY = 0, CR_HL = 1, CR_SHADOW = 2 };
 enum CdlSet {
   BODY_LONG = 0, BODY_VERY_LONG, BODY_SHORT, BODY_DOJI, SHADOW_LONG, SHADOW_VERY_LONG, SHADOW_SHORT,
   SHADOW_VERY_SHORT, NEAR, FAR, EQUAL
 };
-// table slot of each setting (-1: uses the bar itself), factor, divisor, period
-__device__ __constant__ const int kSetSlot[11] = {0, 0, 0, 1, -1, -1, 2, 1, 3, 3, 3};
-__device__ __constant__ const float kSetFactor[11] = {1.0f, 3.0f, 1.0f, 0.1f, 1.0f, 2.0f, 1.0f, 0.1f, 0.2f, 0.6f, 0.05f};
+// averaging period of each range slot (body/10, high-low/10, shadows/10,
+// high-low/5)
 __device__ __constant__ const int kSlotPeriod[4] = {10, 10, 10, 5};
-// The same tables as constant expressions: the pattern functions pass literal
-// settings, so these fold at compile time.
+// range slot (-1: the bar itself) and factor of each setting, as constant
+// expressions: the pattern functions pass literal settings, so these fold at
+// compile time.
 __host__ __device__ constexpr int set_slot(int s) {
   return s <= 2 ? 0 : s == 3 ? 1 : s <= 5 ? -1 : s == 6 ? 2 : s == 7 ? 1 : 3;
 }
@@ -39,59 +33,12 @@ __host__ __device__ constexpr float set_factor(int s) {
 
 constexpr int kCdlBack = 5;  // anchors r-5 .. r (HIKKAKEMOD reads NEAR at r-5)
 
-// Shared table of trailing sums: [slot 0..3][row 0..31][anchor r + kCdlBack]
-// (anchor a holds the sum of the slot's range over bars a-period .. a-1)
-struct CdlTable {
-  double* p;
-  int W;  // C + kCdlBack
-  __device__ __forceinline__ double& at(int slot, int row, int r) const {
-    return p[((size_t)slot * 32 + row) * W + r + kCdlBack];
-  }
-};
-
 __device__ __forceinline__ double cdl_range(int type, float o, float h, float l, float c) {
   const double od = o, hd = h, ld = l, cd = c;
   if (type == CR_BODY) return fabs(cd - od);
   if (type == CR_HL) return hd - ld;
   return (hd - fmax(od, cd)) + (fmin(od, cd) - ld);
 }
-
-// View of one row at bar r for the pattern decisions.
-struct Bars {
-  const CdlTable* tb;
-  int lane, r;
-  long long t;
-  const float *Op, *Hp, *Lp, *Cp;
-  __device__ __forceinline__ float O(int d) const { return Op[r - d]; }
-  __device__ __forceinline__ float H(int d) const { return Hp[r - d]; }
-  __device__ __forceinline__ float L(int d) const { return Lp[r - d]; }
-  __device__ __forceinline__ float C(int d) const { return Cp[r - d]; }
-  __device__ __forceinline__ double RB(int d) const { return fabs((double)C(d) - (double)O(d)); }
-  __device__ __forceinline__ double US(int d) const { return (double)H(d) - fmax((double)O(d), (double)C(d)); }
-  __device__ __forceinline__ double LS(int d) const { return fmin((double)O(d), (double)C(d)) - (double)L(d); }
-  __device__ __forceinline__ int COL(int d) const { return C(d) >= O(d) ? 1 : -1; }
-  __device__ __forceinline__ float TOP(int d) const { return fmaxf(O(d), C(d)); }
-  __device__ __forceinline__ float BOT(int d) const { return fminf(O(d), C(d)); }
-  __device__ __forceinline__ bool BGAP_UP(int a, int b) const { return fminf(O(a), C(a)) > fmaxf(O(b), C(b)); }
-  __device__ __forceinline__ bool BGAP_DN(int a, int b) const { return fmaxf(O(a), C(a)) < fminf(O(b), C(b)); }
-  __device__ __forceinline__ bool RGAP_UP(int a, int b) const { return L(a) > H(b); }
-  __device__ __forceinline__ bool RGAP_DN(int a, int b) const { return H(a) < L(b); }
-  // TA-Lib candle average of setting s anchored at bar r-d
-  __device__ __forceinline__ double AVG(int s, int d) const {
-    const int slot = set_slot(s);
-    const double factor = (double)set_factor(s);
-    const double div = slot == 2 ? 2.0 : 1.0;
-    const long long a = t - d;
-    if (slot < 0) return factor * RB(d) / div;
-    const int per = kSlotPeriod[slot];
-    const long long cnt = a < per ? a : per;
-    if (cnt <= 0) {
-      const int type = slot == 0 ? CR_BODY : (slot == 2 ? CR_SHADOW : CR_HL);
-      return factor * cdl_range(type, O(d), H(d), L(d), C(d)) / div;
-    }
-    return factor * (tb->at(slot, lane, r - d) / (double)cnt) / div;
-  }
-};
 
 #define CDL_FN(name) template <class B> __device__ __forceinline__ int name(const B& b)
 
@@ -538,58 +485,5 @@ __device__ __constant__ const unsigned char kCdlLookbackDev[63] = {
     10, 5, 10, 11, 12, 11, 11, 11, 14, 10, 10, 10, 6, 14, 12, 12, 11, 11, 10, 14, 11, 11, 10, 10, 12, 7, 10, 7, 11, 12,
     12, 12, 2};
 
-// Candle job: pattern subset `cdl_mask` of one group. `writer` fills the
-// group's trailing-sum table; `bar_id`/`nthreads` name the barrier shared by
-// the group's candle warps.
-__device__ void sp_cdl_job(Driver& drv, const Job& j, const Stage& st, int lane, const CdlTable& tbl, bool writer,
-                           int bar_id, int nthreads) {
-  const int po = j.in[0], ph = j.in[1], pl = j.in[2], pc = j.in[3];
-  for (int c = 0; c < drv.nchunks; ++c) {
-    drv.begin(c);
-    const Row rw = drv.row(c);
-    const float* Op = drv.pptr(c, po);
-    const float* Hp = drv.pptr(c, ph);
-    const float* Lp = drv.pptr(c, pl);
-    const float* Cp = drv.pptr(c, pc);
-    const int lim = (int)min((long long)C, rw.n - rw.t0);
-    if (writer) {
-      for (int slot = 0; slot < 4; ++slot) {
-        const int per = kSlotPeriod[slot];
-        const int type = slot == 0 ? CR_BODY : (slot == 2 ? CR_SHADOW : CR_HL);
-        auto rg = [&](int r) { return cdl_range(type, Op[r], Hp[r], Lp[r], Cp[r]); };
-        const int a0 = -kCdlBack;
-        double s = 0.0;
-        for (int i = 1; i <= per; ++i) s += rg(a0 - i);
-        for (int a = a0; a < lim; ++a) {
-          tbl.at(slot, lane, a) = s;
-          s += rg(a) - rg(a - per);
-        }
-      }
-    }
-    asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthreads) : "memory");
-    Bars b;
-    b.tb = &tbl;
-    b.lane = lane;
-    b.Op = Op; b.Hp = Hp; b.Lp = Lp; b.Cp = Cp;
-    int* ibuf = reinterpret_cast<int*>(st.buf);
-    uint64_t mask = j.cdl_mask;
-    while (mask) {
-      const int k = __ffsll((long long)mask) - 1;
-      mask &= mask - 1;
-      const int lb = kCdlLookbackDev[k];
-      for (int r = 0; r < lim; ++r) {
-        b.r = r;
-        b.t = rw.t0 + r;
-        const int v = b.t >= lb ? cdl_eval(k, b) : 0;
-        if (j.cdl_int32) ibuf[lane * (C + 1) + r] = v;
-        else st.buf[lane * (C + 1) + r] = (float)v;
-      }
-      if (j.cdl_int32) st.flush_int(0, (int*)j.out[0] + (long long)k * j.cdl_stride, drv.my_base, drv.my_n, rw.t0, lane);
-      else st.flush(0, (float*)j.out[0] + (long long)k * j.cdl_stride, drv.my_base, drv.my_n, rw.t0, lane);
-    }
-    drv.end(c);
-  }
-}
-
-}  // namespace sp
+}  // namespace rules
 }  // namespace tb

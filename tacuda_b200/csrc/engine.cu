@@ -22,7 +22,6 @@
 #include "jobs.h"
 #ifndef TB_PREC_TU
 #include "candles.cuh"
-#include "sp_candles.cuh"
 #endif
 
 #include <algorithm>
