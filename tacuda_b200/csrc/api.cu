@@ -916,7 +916,7 @@ ctStatus_t ct_b200_alpha_backward_d(const float* d_close, const float* d_alpha, 
 // Auxiliary streams of the host-memory entry point (per device, created once):
 // row chunks rotate over them so one chunk's copy-in, another's kernel and a
 // third's copy-out overlap.
-static constexpr int kPipeStreams = 3;
+static constexpr int kPipeStreams = 8;
 static std::mutex g_pipe_mutex;
 static std::vector<std::vector<cudaStream_t>> g_pipe_streams;
 

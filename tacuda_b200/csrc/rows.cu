@@ -303,7 +303,29 @@ bool family_supported(int f) {
 
 // bars of history a job reads before a chunk: one more than its lookback halo
 // (the bar leaving a running window, the previous close)
-int rows_halo(const Job& j) { return job_halo(j) + 1; }
+int rows_halo(const Job& j) {
+  int h = job_halo(j);
+  // WILLR / STOCH rebuild their van Herk blocks at every chunk from up to
+  // 2p - 1 bars before it
+  if (j.family == F_WILLR || j.family == F_STOCH) h = std::max(h, 2 * j.ip[0] - 1);
+  return h + 1;
+}
+
+// Jobs split over a team of warps by chunks: row-sequential windows whose
+// chunks share no state. Like the bar-parallel WILLR / STOCH, this pays only
+// when few jobs share the CTA (a single BBANDS: 53 -> 24 us, MFI: 63 -> 45 us
+// at 4000 x 234); with many jobs the SM's issue rate, not one warp's chain,
+// bounds the CTA, and the extra warps slowed the 13-indicator pass (181 ->
+// 188 us).
+inline bool chunk_team(const Launch& L, int family) {
+  if (L.njobs > 4) return false;
+  switch (family) {
+    case F_WILLR: case F_STOCH: case F_MFI: case F_BBANDS: case F_STDDEV: case F_VAR:
+      return true;
+    default:
+      return false;
+  }
+}
 
 struct DevState {
   int sms = 0, smem_optin = 0;
@@ -312,49 +334,54 @@ struct DevState {
 std::mutex g_mutex;
 std::vector<DevState> g_dev;
 
-// Relative time of a job's warp over a chunk when it runs alone, from single
-// job launches at 4000 x 234 (microseconds above the launch's fixed cost),
-// for the warp placement and the team sizes. A bar-parallel job's figure is
-// for one warp; a team of m divides it by m.
+// Relative time a job's warp needs for the rows of a CTA, from a per-warp
+// timing trace of the 13-indicator pass at 4000 x 234 (microseconds a warp
+// was busy, i.e. not waiting on the ring, with the other jobs beside it), for
+// the warp placement and the team sizes. A team of m warps divides a job's
+// figure by m.
 int family_cost(const Job& j, unsigned long long bp) {
   const int p = j.ip[0];
   switch (j.family) {
-    case F_CCI: return 14 * p;
-    case F_MFI: return 44;
-    case F_STOCH: return bar_parallel(bp, F_STOCH) ? 7 * p : 37;
-    case F_BBANDS: return 35;
-    case F_WILLR: return bar_parallel(bp, F_WILLR) ? 6 * p : 33;
-    case F_ADX: case F_DX: return 27;
-    case F_STDDEV: case F_VAR: return 25;
-    case F_MACD: return 21;
-    case F_RSI: return 18;
-    case F_ATR: case F_NATR: return 11;
-    case F_OBV: case F_AD: return 10;
-    case F_WMA: return 9;
-    case F_SMA: case F_SUM: return 9;
-    case F_EMA: case F_RMA: return 4;
-    default: return 10 + p;
+    case F_CCI: return 36 * p;
+    case F_MFI: return 150;
+    case F_STOCH: return bar_parallel(bp, F_STOCH) ? 30 * p : 147;
+    case F_WILLR: return bar_parallel(bp, F_WILLR) ? 25 * p : 143;
+    case F_ADX: case F_DX: return 95;
+    case F_BBANDS: return 94;
+    case F_MACD: return 87;
+    case F_STDDEV: case F_VAR: return 70;
+    case F_RSI: return 63;
+    case F_WMA: return 60;
+    case F_OBV: case F_AD: return 57;
+    case F_SMA: case F_SUM: return 53;
+    case F_ATR: case F_NATR: return 49;
+    case F_EMA: case F_RMA: return 44;
+    default: return 40 + 4 * p;
   }
 }
 
-// Job warps: one per job, and spare warps up to kMaxConsumers go to the
-// bar-parallel jobs as team members (rows split between them), each time to
-// the job whose warps carry the most work, while that is more than the
-// heaviest row-sequential job's. Warp w of a CTA issues from sub-partition
+// Job warps: one per job, and spare warps up to kMaxConsumers go to the jobs
+// that can be split as team members (a bar-parallel job splits its rows, a
+// chunk-team job its chunks), each time to the job whose warps carry the most
+// work, while that is more than the heaviest job that cannot be split. Warp w of a CTA issues from sub-partition
 // w % 4: the job warps and the producer are placed longest-first on the least
 // loaded sub-partition, so the heaviest warps do not share one.
-void assign_warps(const Launch& L, Layout& lay) {
+void assign_warps(const Launch& L, Layout& lay, int budget) {
   int team[kMaxConsumers];
   int nw = L.njobs, seq_max = 0;
   for (int j = 0; j < L.njobs; ++j) {
     team[j] = 1;
-    if (!bar_parallel(lay.bp_mask, L.jobs[j].family)) seq_max = std::max(seq_max, family_cost(L.jobs[j], lay.bp_mask));
+    const int f = L.jobs[j].family;
+    if (!bar_parallel(lay.bp_mask, f) && !chunk_team(L, f)) seq_max = std::max(seq_max, family_cost(L.jobs[j], lay.bp_mask));
   }
-  while (nw < kMaxConsumers) {
+  while (nw < budget) {
     int best = -1;
     double bc = (double)seq_max;
     for (int j = 0; j < L.njobs; ++j) {
-      if (!bar_parallel(lay.bp_mask, L.jobs[j].family)) continue;
+      const int f = L.jobs[j].family;
+      if (!bar_parallel(lay.bp_mask, f) && !chunk_team(L, f)) continue;
+      // a chunk team works on at most the ring's NS - Hs chunks at once
+      if (!bar_parallel(lay.bp_mask, f) && team[j] >= lay.NS - lay.Hs) continue;
       const double c = (double)family_cost(L.jobs[j], lay.bp_mask) / team[j];
       if (c > bc) {
         bc = c;
@@ -377,7 +404,7 @@ void assign_warps(const Launch& L, Layout& lay) {
     }
   item_job[i] = -1;
   item_k[i] = 0;
-  cost[i] = 4.0 * lay.nplanes;
+  cost[i] = 18.0 * lay.nplanes;
   for (int k = 0; k < n; ++k) order[k] = k;
   std::stable_sort(order, order + n, [&](int a, int b) { return cost[a] > cost[b]; });
   double load[4] = {0, 0, 0, 0};
@@ -462,19 +489,26 @@ cudaError_t launch(Launch& L, long long max_len, cudaStream_t stream, LaunchStat
   lay.tab_off = off;
   off += 64 * 8 + 16;
   lay.bp_mask = bar_parallel_mask(L);
-  assign_warps(L, lay);
-  for (int w = 0; w <= lay.nconsumers; ++w) {
-    const int jb = lay.warp_job[w];
-    off = (off + 15) & ~15;
-    lay.stage_off[w] = off;
-    if (jb < 0) continue;
-    if (!bar_parallel(lay.bp_mask, L.jobs[jb].family)) off += out_count(L.jobs[jb].family) * 32 * (C + 1) * 4;
-    off = (off + 15) & ~15;
-    lay.line_off[w] = off;
-    off += line_bytes(L.jobs[jb], lay.bp_mask);
+  // team members cost shared memory (a transpose stage and lines each): give
+  // up spare warps until the layout fits
+  const int fixed = off;
+  for (int budget = kMaxConsumers;; --budget) {
+    assign_warps(L, lay, budget);
+    off = fixed;
+    for (int w = 0; w <= lay.nconsumers; ++w) {
+      const int jb = lay.warp_job[w];
+      off = (off + 15) & ~15;
+      lay.stage_off[w] = off;
+      if (jb < 0) continue;
+      if (!bar_parallel(lay.bp_mask, L.jobs[jb].family)) off += out_count(L.jobs[jb].family) * 32 * (C + 1) * 4;
+      off = (off + 15) & ~15;
+      lay.line_off[w] = off;
+      off += line_bytes(L.jobs[jb], lay.bp_mask);
+    }
+    lay.total = (off + 127) & ~127;
+    if (lay.total <= ds->smem_optin) break;
+    if (budget <= L.njobs) return cudaErrorNotSupported;
   }
-  lay.total = (off + 127) & ~127;
-  if (lay.total > ds->smem_optin) return cudaErrorNotSupported;
   const long long groups = ((long long)L.S + 31) / 32;
   if (groups > INT_MAX) return cudaErrorInvalidValue;
   const int threads = 32 * (lay.nconsumers + 1);

@@ -204,6 +204,8 @@ struct Warp {
     return base >= 0 ? tn[r] : 0;
   }
   __device__ __forceinline__ int lim(int c) const { return min(C, maxn - c * C); }
+  // chunk c is this warp's share of a job split over a team by chunks
+  __device__ __forceinline__ bool own(int c) const { return tm <= 1 || c % tm == tk; }
   // bars of chunk c a steady (unrolled by 8) loop covers
   __device__ __forceinline__ int lim8(int c) const { return (lim(c) + 7) & ~7; }
 
@@ -343,7 +345,8 @@ __device__ void w_sum_window(const Warp& w, const Job& j, int mode) {
 // (talib08:18047-18183 TA_VAR re-centres the same way); the variance follows
 // TA-Lib's E[d^2] - E[d]^2 in FP64 and is clamped at zero; the square root and
 // the bands in float32. A chunk whose windows are finite runs without NaN
-// bookkeeping, with the same arithmetic.
+// bookkeeping, with the same arithmetic. Chunks share no state, so a team of
+// warps can share the job by chunks.
 __device__ __forceinline__ void moment_out(int mode, double o, double s1, double s2, double inv, float up, float dn,
                                            float& o0, float& o1, float& o2) {
   const double m1 = s1 * inv;
@@ -378,6 +381,10 @@ __device__ void w_moment_window(const Warp& w, const Job& j, int mode) {
   const int nout = mode == 0 ? 3 : 1;
   for (int c = 0; c < w.nchunks; ++c) {
     if (!w.wait(c)) return;
+    if (!w.own(c)) {
+      w.release(c);
+      continue;
+    }
     const float* X = w.X(c, pl);
     const float* Xo = X - p;
     float* st0 = w.stage_row(0);
@@ -477,6 +484,20 @@ struct VanHerk {
       suf[k * 32] = m;
     }
   }
+  // the state entering chunk-relative bar 0 (row bar t0), rebuilt from the
+  // halo: the extremum of the current block's bars before t0 and the
+  // suffixes of the block before it; returns t0's block position. Reads
+  // back to bar t0 - pos - p (at most 2p - 1 bars).
+  __device__ __forceinline__ int reseed(const float* X, long long t0, int p) {
+    const int pos = (int)(t0 % p);
+    if (pos > 0) {
+      float m = X[-pos];
+      for (int k = -pos + 1; k < 0; ++k) m = op(m, X[k]);
+      pre = m;
+      if (t0 - pos >= p) fill(X, -pos, p);
+    }
+    return pos;
+  }
   // bar t at block position pos (t = k*p + pos) with value x
   __device__ __forceinline__ float step(float x, int pos, int p) {
     pre = pos == 0 ? x : op(pre, x);
@@ -488,19 +509,26 @@ struct VanHerk {
 
 // WILLR (src/indicators/WILLR.cu:11-30): extremes anchored at the current bar
 // (a NaN high or low there gives NaN, earlier NaNs are skipped), float32 ratio
-// times -100 clamped to [-100, 0]; 0 for a zero range.
+// times -100 clamped to [-100, 0]; 0 for a zero range. Every chunk rebuilds its
+// van Herk state from the halo (extremes are exact, so the bits do not
+// change), and a team of warps can share the job by chunks.
 __device__ void w_willr(const Warp& w, const Job& j, float* line, int cap) {
   const int ph = j.in[0], plo = j.in[1], pc = j.in[2], p = j.ip[0];
   VanHerk<true> hh{line + w.lane, 0.0f};
   VanHerk<false> ll{line + 32 * cap + w.lane, 0.0f};
-  int pos = 0;
   for (int c = 0; c < w.nchunks; ++c) {
     if (!w.wait(c)) return;
+    if (!w.own(c)) {
+      w.release(c);
+      continue;
+    }
     const float* H = w.X(c, ph);
     const float* Lo = w.X(c, plo);
     const float* Cl = w.X(c, pc);
     float* st = w.stage_row(0);
     const int t0 = c * C, n8 = w.lim8(c);
+    int pos = hh.reseed(H, t0, p);
+    ll.reseed(Lo, t0, p);
     for (int r8 = 0; r8 < n8; r8 += 8) {
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
@@ -526,10 +554,25 @@ __device__ void w_willr(const Warp& w, const Job& j, float* line, int cap) {
   }
 }
 
+// fastK of chunk-relative bar r from its window directly (extremes anchored
+// at the window's first bar, as the running form gives them)
+__device__ __forceinline__ float stoch_fastk(const float* H, const float* Lo, const float* Cl, int r, int p) {
+  float hi = H[r - p + 1], lo = Lo[r - p + 1];
+  for (int i = r - p + 2; i <= r; ++i) {
+    const float a = H[i], b = Lo[i];
+    hi = a > hi ? a : hi;
+    lo = b < lo ? b : lo;
+  }
+  const float range = hi - lo;
+  return fabsf(range) <= 1e-14f * (fabsf(hi) + fabsf(lo)) ? 0.0f : fdiv(Cl[r] - lo, range) * 100.0f;
+}
+
 // STOCH (talib08:16115-16302, SMA slowing): fastK from the window extremes
 // anchored at the window's first bar, TA-Lib's zero-range test; slowK and
 // slowD are direct means of the last q fastK / slowK values, summed oldest
-// first, from registers for q = Q > 0 or per-lane lines (Q = 0).
+// first, from registers for q = Q > 0 or per-lane lines (Q = 0). Every chunk
+// rebuilds its state from the halo, so a team of warps can share the job by
+// chunks.
 template <int Q>
 __device__ void w_stoch(const Warp& w, const Job& j, float* line, int cap) {
   const int ph = j.in[0], plo = j.in[1], pc = j.in[2], p = j.ip[0], q = Q > 0 ? Q : j.ip[1];
@@ -541,15 +584,45 @@ __device__ void w_stoch(const Warp& w, const Job& j, float* line, int cap) {
   float* fkl = line + 2 * 32 * cap + w.lane;  // [(t & mask) * 32]
   float* skl = line + 3 * 32 * cap + w.lane;
   float fh[4] = {0.0f, 0.0f, 0.0f, 0.0f}, sh[4] = {0.0f, 0.0f, 0.0f, 0.0f};  // [0] newest
-  int pos = 0;
   for (int c = 0; c < w.nchunks; ++c) {
     if (!w.wait(c)) return;
+    if (!w.own(c)) {
+      w.release(c);
+      continue;
+    }
     const float* H = w.X(c, ph);
     const float* Lo = w.X(c, plo);
     const float* Cl = w.X(c, pc);
     float* st0 = w.stage_row(0);
     float* st1 = w.stage_row(1);
     const int t0 = c * C, n8 = w.lim8(c);
+    // state entering bar t0 from the halo: the van Herk blocks, and fastK /
+    // slowK of the 2(q-1) / q-1 bars before t0 (window extremes are exact, so
+    // the bits do not depend on where a chunk starts)
+    int pos = hh.reseed(H, t0, p);
+    ll.reseed(Lo, t0, p);
+    if (Q > 0) {
+      float fk[2 * (Q > 0 ? Q : 1)];
+#pragma unroll
+      for (int i = 0; i < 2 * (Q - 1); ++i) fk[i] = stoch_fastk(H, Lo, Cl, i - 2 * (Q - 1), p);  // oldest first
+#pragma unroll
+      for (int m = 0; m < Q - 1; ++m) {
+        fh[m] = fk[2 * (Q - 1) - 1 - m];
+        // slowK of bar t0-1-m: fastK of bars t0-m-q .. t0-1-m, oldest first
+        const int e = 2 * (Q - 1) - 1 - m;
+        float sk = fk[e - (Q - 1)];
+#pragma unroll
+        for (int i = e - (Q - 1) + 1; i <= e; ++i) sk += fk[i];
+        sh[m] = sk * invq;
+      }
+    } else {
+      for (int r = -2 * (q - 1); r < 0; ++r) fkl[((t0 + r) & mask) * 32] = stoch_fastk(H, Lo, Cl, r, p);
+      for (int r = -(q - 1); r < 0; ++r) {
+        float sk = fkl[((t0 + r - q + 1) & mask) * 32];
+        for (int m = q - 2; m >= 0; --m) sk += fkl[((t0 + r - m) & mask) * 32];
+        skl[((t0 + r) & mask) * 32] = sk * invq;
+      }
+    }
     for (int r8 = 0; r8 < n8; r8 += 8) {
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
@@ -611,31 +684,60 @@ __device__ void w_stoch(const Warp& w, const Job& j, float* line, int cap) {
 }
 
 // MFI (include/utils/StreamStates.h:749-792 precise::MfiState): flows of the
-// FP64 typical price times volume, signed by the typical price's change, in a
-// per-lane line; running positive / negative window sums, re-summed directly
-// when one turns negative or a non-finite flow is in reach (the reference sums
-// every window); 100 * pos / (pos + neg), 0 below a total of 1.
+// FP64 typical price ((h+l)+c)/3.0 (correctly rounded, div_by) times volume,
+// signed by the typical price's change, in a per-lane line; running positive /
+// negative window sums, re-summed directly when one turns negative or a
+// non-finite flow is in reach (the reference sums every window); 100 * pos /
+// (pos + neg), 0 below a total of 1. Every chunk starts from sums rebuilt from
+// the halo, so a chunk depends on no state of the chunk before and a team of
+// warps can share the job by chunks.
 __device__ void w_mfi(const Warp& w, const Job& j, double* line, int cap) {
   const int ph = j.in[0], plo = j.in[1], pc = j.in[2], pv = j.in[3], p = j.ip[0];
   const int mask = cap - 1;
   const double third = 1.0 / 3.0;
   double* pos_l = line + w.lane;  // [(t & mask) * 32]
   double* neg_l = line + 32 * cap + w.lane;
-  double prev_tp = 0.0, ps = 0.0, ns = 0.0;
-  int last_bad = -(1 << 30);
   for (int c = 0; c < w.nchunks; ++c) {
     if (!w.wait(c)) return;
+    if (!w.own(c)) {
+      w.release(c);
+      continue;
+    }
     const float* H = w.X(c, ph);
     const float* Lo = w.X(c, plo);
     const float* Cl = w.X(c, pc);
     const float* V = w.X(c, pv);
     float* st = w.stage_row(0);
     const int t0 = c * C, n8 = w.lim8(c);
+    // the state entering bar t0, rebuilt from the ring's halo: the flows of
+    // bars t0-p .. t0-1 (from bar 0 in the first p bars), their sums taken
+    // oldest first, and the previous typical price
+    double ps = 0.0, ns = 0.0, prev_tp = 0.0;
+    int last_bad = -(1 << 30);
+    if (t0 > 0) {
+      const int r0 = max(-p, -t0);
+      double prev = t0 + r0 >= 1 ? div_by(((double)H[r0 - 1] + (double)Lo[r0 - 1]) + (double)Cl[r0 - 1], 3.0, third)
+                                 : 0.0;
+      for (int r = r0; r < 0; ++r) {
+        const int t = t0 + r;
+        const double tp = div_by(((double)H[r] + (double)Lo[r]) + (double)Cl[r], 3.0, third);
+        const double fl = tp * (double)V[r];
+        const bool ok = t >= 1 && isfinite(tp) && isfinite(prev);
+        const double a = ok && tp > prev ? fl : 0.0, b = ok && tp < prev ? fl : 0.0;
+        if (!isfinite(a + b)) last_bad = t;
+        prev = tp;
+        pos_l[(t & mask) * 32] = a;
+        neg_l[(t & mask) * 32] = b;
+        ps += a;
+        ns += b;
+      }
+      prev_tp = prev;
+    }
     for (int r8 = 0; r8 < n8; r8 += 8) {
 #pragma unroll 4
       for (int u = 0; u < 8; ++u) {
         const int r = r8 + u, t = t0 + r;
-        const double tp = (((double)H[r] + (double)Lo[r]) + (double)Cl[r]) * third;
+        const double tp = div_by(((double)H[r] + (double)Lo[r]) + (double)Cl[r], 3.0, third);
         const double fl = tp * (double)V[r];
         const bool ok = t >= 1 && isfinite(tp) && isfinite(prev_tp);
         const double a = ok && tp > prev_tp ? fl : 0.0, b = ok && tp < prev_tp ? fl : 0.0;
