@@ -422,6 +422,13 @@ CTAPI_EXPORT ctStatus_t ct_b200_plan_describe(const ctB200Plan* plan, int* engin
  * arrays are skipped). Returns how many it timed (0 before any autotune). */
 CTAPI_EXPORT int ct_b200_plan_candidates(const ctB200Plan* plan, int maxOut, int* engine, int* barsPerLane,
                                          int* warpsPerBlock, float* ms);
+/* Row-parallel engine layout of a plan: the partitions its job set is split
+ * into (one grid row each) and the 32-row groups each CTA runs; 0 = the
+ * library's default for the job set. Null outputs are skipped. */
+CTAPI_EXPORT ctStatus_t ct_b200_plan_describe_rows(const ctB200Plan* plan, int* parts, int* groups);
+/* The same for each candidate of the last autotune, in the order of
+ * ct_b200_plan_candidates (0 for candidates of the other engines). */
+CTAPI_EXPORT int ct_b200_plan_candidates_rows(const ctB200Plan* plan, int maxOut, int* parts, int* groups);
 
 /* All selected candle patterns of a uniform batch in one pass, int32 signals
  * (pattern k of mask at d_out + k * seriesLen * numSeries). */

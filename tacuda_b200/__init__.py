@@ -84,6 +84,9 @@ def _load() -> ct.CDLL:
     lib.ct_b200_plan_destroy.argtypes = [_P]
     lib.ct_b200_plan_candidates.argtypes = [_P, _I, _P, _P, _P, _P]
     lib.ct_b200_plan_candidates.restype = _I
+    lib.ct_b200_plan_describe_rows.argtypes = [_P, ct.POINTER(_I), ct.POINTER(_I)]
+    lib.ct_b200_plan_candidates_rows.argtypes = [_P, _I, _P, _P]
+    lib.ct_b200_plan_candidates_rows.restype = _I
     lib.ct_b200_cdl_batch_d.argtypes = [_P, _P, _P, _P, _P, _I, _I, ct.c_uint64, _P]
     lib.ct_b200_alpha_checkpoint_doubles.argtypes = [_I]
     lib.ct_b200_alpha_checkpoint_doubles.restype = ct.c_longlong
@@ -304,7 +307,13 @@ class Plan:
         m, k, w, b = _I(), _I(), _I(), _I()
         call_status(get_lib().ct_b200_plan_describe(self.handle, ct.byref(m), ct.byref(k), ct.byref(w),
                                                     ct.byref(b)), "ct_b200_plan_describe")
-        return {"mode": m.value, "bars_per_lane": k.value, "warps_per_block": w.value, "max_blocks": b.value}
+        d = {"mode": m.value, "bars_per_lane": k.value, "warps_per_block": w.value, "max_blocks": b.value}
+        if m.value == 1:
+            p, g = _I(), _I()
+            call_status(get_lib().ct_b200_plan_describe_rows(self.handle, ct.byref(p), ct.byref(g)),
+                        "ct_b200_plan_describe_rows")
+            d.update(parts=p.value, groups=g.value)  # 0: the library's default for the job set
+        return d
 
     ENGINES = {0: "warp-scan", 1: "row-parallel", 2: "look-back"}
 
@@ -317,8 +326,18 @@ class Plan:
         m, k, w = (np.zeros(n, np.int32) for _ in range(3))
         ms = np.zeros(n, np.float32)
         lib.ct_b200_plan_candidates(self.handle, n, m.ctypes.data, k.ctypes.data, w.ctypes.data, ms.ctypes.data)
-        return [{"engine": self.ENGINES.get(int(m[i]), str(int(m[i]))), "bars_per_lane": int(k[i]),
-                 "warps_per_block": int(w[i]), "ms": float(ms[i])} for i in range(n)]
+        p, g = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        lib.ct_b200_plan_candidates_rows(self.handle, n, p.ctypes.data, g.ctypes.data)
+        out = []
+        for i in range(n):
+            c = {"engine": self.ENGINES.get(int(m[i]), str(int(m[i])))}
+            if int(m[i]) == 1:
+                c.update(parts=int(p[i]), groups=int(g[i]))
+            else:
+                c.update(bars_per_lane=int(k[i]), warps_per_block=int(w[i]))
+            c["ms"] = float(ms[i])
+            out.append(c)
+        return out
 
     def close(self) -> None:
         if self.handle:

@@ -39,6 +39,15 @@ def _run(cmd):
     subprocess.run(cmd, check=True)
 
 
+def _compile(cmd, obj: Path):
+    """Compile, then date the object at the compile's start: a source edited
+    while nvcc ran stays newer than the object and is rebuilt next time."""
+    import time
+    t0 = time.time()
+    _run(cmd)
+    os.utime(obj, (t0, t0))
+
+
 def _includes(src: Path, seen: set) -> set:
     """Project headers a source includes, directly or through other headers."""
     import re
@@ -70,10 +79,10 @@ def build_library(verbose: bool = False) -> Path:
                    f"-I{ROOT / 'include'}", f"-I{CSRC}", *defines, "-c", str(src), "-o", str(obj)]
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
-            jobs.append(cmd)
+            jobs.append((cmd, obj))
     # translation units compile in parallel (the two engine halves dominate)
     with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
-        for f in [ex.submit(_run, cmd) for cmd in jobs]:
+        for f in [ex.submit(_compile, cmd, obj) for cmd, obj in jobs]:
             f.result()
     _run([nvcc(), *ARCH, "-shared", "-o", str(OUT), *objs])
     return OUT

@@ -1504,9 +1504,13 @@ ctStatus_t ct_b200_plan_autotune(ctB200Plan* plan, const ctB200Series* series, c
   // candidates: the row-parallel engine; the warp-scan engine over round
   // widths and block sizes; the look-back engine where its tiles fit the rows
   std::vector<tb::SchedulePlan> cands;
-  {
+  // row-parallel engine: the job set whole (one row group per CTA) or split
+  // into partitions with two row groups per CTA
+  for (const int pg : {0x11, 0x42, 0x52, 0x62}) {
     tb::SchedulePlan cand;
     cand.mode = 1;
+    cand.parts = pg >> 4;
+    cand.groups = pg & 15;
     cands.push_back(cand);
   }
   for (int mode : {0, 2})
@@ -1559,6 +1563,26 @@ ctStatus_t ct_b200_plan_describe(const ctB200Plan* plan, int* engine, int* barsP
   if (warpsPerBlock) *warpsPerBlock = plan->sched.warps_per_block;
   if (blocks) *blocks = plan->sched.max_blocks;
   return CT_STATUS_SUCCESS;
+}
+
+ctStatus_t ct_b200_plan_describe_rows(const ctB200Plan* plan, int* parts, int* groups) {
+  clear_error();
+  if (!plan) return fail(CT_STATUS_INVALID_ARGUMENT, "ct_b200_plan_describe_rows: null plan");
+  if (parts) *parts = plan->sched.parts;
+  if (groups) *groups = plan->sched.groups;
+  return CT_STATUS_SUCCESS;
+}
+
+int ct_b200_plan_candidates_rows(const ctB200Plan* plan, int maxOut, int* parts, int* groups) {
+  clear_error();
+  if (!plan) return 0;
+  const int n = (int)plan->tried.size();
+  for (int i = 0; i < n && i < maxOut; ++i) {
+    const ctB200Plan::Tried& t = plan->tried[(size_t)i];
+    if (parts) parts[i] = t.plan.parts;
+    if (groups) groups[i] = t.plan.groups;
+  }
+  return n;
 }
 
 int ct_b200_plan_candidates(const ctB200Plan* plan, int maxOut, int* engine, int* barsPerLane, int* warpsPerBlock,

@@ -751,7 +751,7 @@ cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, long long total_ba
   // row-parallel engine; job sets it does not take (or whose layout does not
   // fit its shared memory) run on the warp-scan engine
   if (plan.mode == 1 && rows::supports(L, L.max_len)) {
-    const cudaError_t e = rows::launch(L, L.max_len, stream, stats);
+    const cudaError_t e = rows::launch(L, L.max_len, stream, stats, plan.parts, plan.groups);
     if (e != cudaErrorNotSupported) return e;
   }
   if (L.njobs > 0 && L.jobs[0].prec != 0) return launch_prec(L, plan, total_bars, stream, stats);

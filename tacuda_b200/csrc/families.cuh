@@ -1177,10 +1177,34 @@ __device__ __forceinline__ void talib_bar_round(const Ctx<K>& c, const Job& j, C
 // QSTICK(p) through the reference's TA-Lib runner (talib08 TA_QSTICK,
 // src/compat/Talib08.cu:72-97): from the first bar f where open and close are
 // both present, the mean of close - open over the last p bars, from bar
-// f + p - 1. TA_QSTICK keeps a running FP64 sum, so the first NaN difference g
-// at or after f turns every later output NaN; the windows here are summed
-// directly (exact for float32 inputs) and stop at g. Scratch carry: v[0] =
-// g + 1 (0 while none is known).
+// f + p - 1. TA_QSTICK keeps a running FP64 sum: the first NaN difference g
+// at or after f turns every later output NaN, and so does the first infinite
+// difference gi once it leaves the window (inf - inf), i.e. from bar gi + p.
+// The windows here are summed directly (exact for float32 inputs) and stop at
+// min(g, gi + p). Scratch carries: v[0] = g + 1, v[1] = gi + 1 (0 while none
+// is known).
+template <int K>
+__device__ __forceinline__ int qstick_first(const Ctx<K>& c, const Job& j, int f, int g0, bool inf, int slot,
+                                            double& carry) {
+  const int po = j.in[0], pc = j.in[1];
+  if (!c.lb && carry > 0.0) return (int)carry - 1;
+  int first = 0x7fffffff;
+  if (f >= 0) {
+    for (int k = 0; k < K; ++k) {
+      const int t = g0 + k;
+      if (!c.valid(t) || t < f) continue;
+      const double d = (double)c.x(pc, t) - (double)c.x(po, t);
+      if (inf ? isinf(d) : isnan(d)) { first = t; break; }
+    }
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) first = min(first, __shfl_xor_sync(kFull, first, d));
+  const int local = first == 0x7fffffff ? -1 : first;
+  const int v = c.lb ? lb_first_index(c.lbd + j.lb_slot + slot, c.lbs, c.tile, local, c.err, c.lane) : local;
+  carry = v >= 0 ? (double)v + 1.0 : 0.0;
+  return v;
+}
+
 template <int K>
 __device__ __forceinline__ void qstick_round(const Ctx<K>& c, const Job& j, Carry& cy) {
   const int po = j.in[0], pc = j.in[1], p = j.ip[0];
@@ -1199,27 +1223,14 @@ __device__ __forceinline__ void qstick_round(const Ctx<K>& c, const Job& j, Carr
     const int local = first == 0x7fffffff ? -1 : first;
     f = c.lb ? lb_first_index(c.lbd + j.lb_slot, c.lbs, c.tile, local, c.err, c.lane) : local;
   }
-  int g;
-  if (!c.lb && cy.v[0] > 0.0) {
-    g = (int)cy.v[0] - 1;
-  } else {
-    int first = 0x7fffffff;
-    if (f >= 0) {
-      for (int k = 0; k < K; ++k) {
-        const int t = g0 + k;
-        if (c.valid(t) && t >= f && isnan((double)c.x(pc, t) - (double)c.x(po, t))) { first = t; break; }
-      }
-    }
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) first = min(first, __shfl_xor_sync(kFull, first, d));
-    const int local = first == 0x7fffffff ? -1 : first;
-    g = c.lb ? lb_first_index(c.lbd + j.lb_slot + 1, c.lbs, c.tile, local, c.err, c.lane) : local;
-  }
+  const int g = qstick_first(c, j, f, g0, false, 1, cy.v[0]);
+  const int gi = qstick_first(c, j, f, g0, true, 2, cy.v[1]);
+  const int stop = g < 0 ? (gi < 0 ? 0x7fffffff : gi + p) : (gi < 0 ? g : min(g, gi + p));
   for (int k = 0; k < K; ++k) {
     const int t = g0 + k;
     if (!c.valid(t)) break;
     float o = qnan();
-    if (f >= 0 && t >= f + p - 1 && (g < 0 || t < g)) {
+    if (f >= 0 && t >= f + p - 1 && t < stop) {
       double s = 0.0;
       for (int i = t - p + 1; i <= t; ++i) s += (double)c.x(pc, i) - (double)c.x(po, i);
       o = (float)(s / (double)p);
@@ -1227,7 +1238,6 @@ __device__ __forceinline__ void qstick_round(const Ctx<K>& c, const Job& j, Carr
     c.put(0, k, o);
   }
   cy.f = f;
-  cy.v[0] = g >= 0 ? (double)g + 1.0 : 0.0;
   c.flush(0, (float*)j.out[0]);
 }
 

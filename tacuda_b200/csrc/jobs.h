@@ -11,7 +11,8 @@ namespace tb {
 // recurrence stage, in the order the round functions address them.
 inline int lb_slots(const Job& j) {
   switch (j.family) {
-    case F_EMA: case F_RMA: case F_QSTICK: return 2;
+    case F_EMA: case F_RMA: return 2;
+    case F_QSTICK: return 3;
     case F_DEMA: return 3;
     case F_TEMA: return 4;
     case F_T3: return 7;

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -21,9 +22,9 @@ namespace rows {
 // splits over a team, which pays only when few jobs share the CTA. The other
 // window families keep their running row-sequential form.
 static_assert(F_COUNT <= 64, "bar-parallel family mask holds 64 families");
-inline unsigned long long bar_parallel_mask(const Launch& L) {
+inline unsigned long long bar_parallel_mask(int njobs) {
   unsigned long long m = 1ull << F_CCI;
-  if (L.njobs <= 4) m |= (1ull << F_WILLR) | (1ull << F_STOCH);
+  if (njobs <= 4) m |= (1ull << F_WILLR) | (1ull << F_STOCH);
   return m;
 }
 __host__ __device__ inline bool bar_parallel(unsigned long long mask, int family) {
@@ -168,12 +169,12 @@ __device__ void run_job(const Warp& w, const Job& j, unsigned char* line) {
 // warps have released the chunk that last used its slot.
 __device__ void produce(const Launch& L, const Layout& lay, unsigned char* smem, uint64_t* full, uint64_t* empty,
                         const long long* tbase, const long long* tn, volatile int* abort_flag, int* err,
-                        int nchunks, int lane) {
+                        int nchunks, int lane, long long group) {
   float* ring = reinterpret_cast<float*>(smem + lay.ring_off);
   const int NS = lay.NS, Hs = lay.Hs, RS = lay.RS;
   const bool uni = !L.order && !L.offsets;
-  const long long s0T = (long long)blockIdx.x * 32 * L.T;
-  const int nvalid = (int)min(32ll, (long long)L.S - (long long)blockIdx.x * 32);
+  const long long s0T = group * 32 * L.T;
+  const int nvalid = (int)min(32ll, (long long)L.S - group * 32);
   const unsigned long long limit = L.stall_test ? kStallWaitNs : kWaitNs;
   for (int c = 0; c < nchunks; ++c) {
     const int s = c % NS, use = c / NS;
@@ -212,18 +213,27 @@ __device__ void produce(const Launch& L, const Layout& lay, unsigned char* smem,
   cp_async_wait_all();
 }
 
+// CTA (x, y): partition y of the job set over row groups x*G .. x*G+G-1; each
+// group has its own warps, ring, mbarriers and tables (a block of lay.total
+// bytes of shared memory), so the groups of a CTA run independently.
 template <bool kAll>
-__global__ void __launch_bounds__(32 * (kMaxConsumers + 1), 1) rows_kernel(const __grid_constant__ Launch L, const __grid_constant__ Layout lay) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+__global__ void __launch_bounds__(32 * kMaxWarps, 1) rows_kernel(const __grid_constant__ Launch L, const __grid_constant__ Split sp) {
+  extern __shared__ __align__(16) unsigned char smem_all[];
+  const Layout& lay = sp.lay[blockIdx.y];
+  const int wpg = lay.nconsumers + 1;
+  const int gw = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sub = gw / wpg, warp = gw - sub * wpg;
+  const long long group = (long long)blockIdx.x * sp.G + sub;
+  const bool live = sub < sp.G && group * 32 < (long long)L.S;
+  unsigned char* smem = smem_all + (size_t)(live ? sub : 0) * lay.total;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + lay.bar_off);
   uint64_t* empty = full + lay.NS;
   long long* tbase = reinterpret_cast<long long*>(smem + lay.tab_off);
   long long* tn = tbase + 32;
   int* misc = reinterpret_cast<int*>(tn + 32);  // [0] longest row of the group, [1] abort
   int* err = L.sticky;
-  if (warp == 0) {
-    const long long idx = (long long)blockIdx.x * 32 + lane;
+  if (live && warp == 0) {
+    const long long idx = group * 32 + lane;
     long long b = -1, n = 0;
     if (idx < L.S) {
       const int s = L.order ? L.order[idx] : (int)idx;
@@ -249,11 +259,12 @@ __global__ void __launch_bounds__(32 * (kMaxConsumers + 1), 1) rows_kernel(const
     }
   }
   __syncthreads();
+  if (!live) return;
   const int maxn = misc[0];
   const int nchunks = (maxn + C - 1) / C;
   volatile int* abort_flag = misc + 1;
   if (warp == lay.producer_warp) {
-    produce(L, lay, smem, full, empty, tbase, tn, abort_flag, err, nchunks, lane);
+    produce(L, lay, smem, full, empty, tbase, tn, abort_flag, err, nchunks, lane, group);
     return;
   }
   if (warp > lay.nconsumers) return;
@@ -277,8 +288,8 @@ __global__ void __launch_bounds__(32 * (kMaxConsumers + 1), 1) rows_kernel(const
   w.n = tn[lane];
   w.uni = !L.order && !L.offsets;
   w.T = L.T;
-  w.s0T = (long long)blockIdx.x * 32 * L.T;
-  w.nvalid = (int)min(32ll, (long long)L.S - (long long)blockIdx.x * 32);
+  w.s0T = group * 32 * L.T;
+  w.nvalid = (int)min(32ll, (long long)L.S - group * 32);
   w.tk = lay.warp_team[warp] & 255;
   w.tm = lay.warp_team[warp] >> 8;
   run_job<kAll>(w, L.jobs[lay.warp_job[warp]], smem + lay.line_off[warp]);
@@ -317,8 +328,8 @@ int rows_halo(const Job& j) {
 // at 4000 x 234); with many jobs the SM's issue rate, not one warp's chain,
 // bounds the CTA, and the extra warps slowed the 13-indicator pass (181 ->
 // 188 us).
-inline bool chunk_team(const Launch& L, int family) {
-  if (L.njobs > 4) return false;
+inline bool chunk_team(int njobs, int family) {
+  if (njobs > 4) return false;
   switch (family) {
     case F_WILLR: case F_STOCH: case F_MFI: case F_BBANDS: case F_STDDEV: case F_VAR:
       return true;
@@ -366,23 +377,25 @@ int family_cost(const Job& j, unsigned long long bp) {
 // work, while that is more than the heaviest job that cannot be split. Warp w of a CTA issues from sub-partition
 // w % 4: the job warps and the producer are placed longest-first on the least
 // loaded sub-partition, so the heaviest warps do not share one.
-void assign_warps(const Launch& L, Layout& lay, int budget) {
+void assign_warps(const Launch& L, const int* jl, int nj, Layout& lay, int budget) {
   int team[kMaxConsumers];
-  int nw = L.njobs, seq_max = 0;
-  for (int j = 0; j < L.njobs; ++j) {
+  int nw = nj, seq_max = 0;
+  for (int j = 0; j < nj; ++j) {
     team[j] = 1;
-    const int f = L.jobs[j].family;
-    if (!bar_parallel(lay.bp_mask, f) && !chunk_team(L, f)) seq_max = std::max(seq_max, family_cost(L.jobs[j], lay.bp_mask));
+    const Job& jb = L.jobs[jl[j]];
+    if (!bar_parallel(lay.bp_mask, jb.family) && !chunk_team(nj, jb.family))
+      seq_max = std::max(seq_max, family_cost(jb, lay.bp_mask));
   }
   while (nw < budget) {
     int best = -1;
     double bc = (double)seq_max;
-    for (int j = 0; j < L.njobs; ++j) {
-      const int f = L.jobs[j].family;
-      if (!bar_parallel(lay.bp_mask, f) && !chunk_team(L, f)) continue;
+    for (int j = 0; j < nj; ++j) {
+      const Job& jb = L.jobs[jl[j]];
+      const int f = jb.family;
+      if (!bar_parallel(lay.bp_mask, f) && !chunk_team(nj, f)) continue;
       // a chunk team works on at most the ring's NS - Hs chunks at once
       if (!bar_parallel(lay.bp_mask, f) && team[j] >= lay.NS - lay.Hs) continue;
-      const double c = (double)family_cost(L.jobs[j], lay.bp_mask) / team[j];
+      const double c = (double)family_cost(jb, lay.bp_mask) / team[j];
       if (c > bc) {
         bc = c;
         best = j;
@@ -396,11 +409,11 @@ void assign_warps(const Launch& L, Layout& lay, int budget) {
   int item_job[kMaxConsumers + 1], item_k[kMaxConsumers + 1], order[kMaxConsumers + 1];
   double cost[kMaxConsumers + 1];
   int i = 0;
-  for (int j = 0; j < L.njobs; ++j)
+  for (int j = 0; j < nj; ++j)
     for (int k = 0; k < team[j]; ++k, ++i) {
       item_job[i] = j;
       item_k[i] = k;
-      cost[i] = (double)family_cost(L.jobs[j], lay.bp_mask) / team[j];
+      cost[i] = (double)family_cost(L.jobs[jl[j]], lay.bp_mask) / team[j];
     }
   item_job[i] = -1;
   item_k[i] = 0;
@@ -420,11 +433,159 @@ void assign_warps(const Launch& L, Layout& lay, int budget) {
     ++used[best];
     const int it = order[k];
     load[best] += cost[it];
-    lay.warp_job[w] = item_job[it];
-    lay.warp_team[w] = item_job[it] < 0 ? (1 << 8) : (item_k[it] | team[item_job[it]] << 8);
-    if (item_job[it] < 0) lay.producer_warp = w;
+    const int jb = item_job[it];
+    lay.warp_job[w] = jb < 0 ? -1 : jl[jb];
+    lay.warp_team[w] = jb < 0 ? (1 << 8) : (item_k[it] | team[jb] << 8);
+    if (jb < 0) lay.producer_warp = w;
   }
   lay.nconsumers = nw;
+}
+
+// The shared-memory layout and warps of one row group running jobs jl[0..nj)
+// with at most `budget` job warps, within `limit` bytes: team warps are given
+// up until it fits. False when even one warp per job does not fit.
+bool build_layout(const Launch& L, const int* jl, int nj, int budget, int limit, int depth, Layout& lay) {
+  std::memset(&lay, 0, sizeof(lay));
+  unsigned mask = 0;
+  int H = 1;
+  for (int j = 0; j < nj; ++j) {
+    mask |= job_planes(L.jobs[jl[j]]);
+    H = std::max(H, rows_halo(L.jobs[jl[j]]));
+  }
+  int np = 0;
+  for (int p = 0; p < P_COUNT; ++p) {
+    lay.plane_slot[p] = (mask & (1u << p)) ? np : -1;
+    if (mask & (1u << p)) lay.slot_plane[np++] = p;
+  }
+  lay.nplanes = np;
+  lay.Hs = std::max(1, (H + C - 1) / C);
+  lay.NS = lay.Hs + depth;  // depth - 1 chunks in flight ahead of the slowest job
+  lay.RS = (lay.Hs + lay.NS) * C + 1;
+  int off = 0;
+  lay.ring_off = off;
+  off += np * 32 * lay.RS * 4;
+  off = (off + 15) & ~15;
+  lay.bar_off = off;
+  off += 2 * lay.NS * 8;
+  lay.tab_off = off;
+  off += 64 * 8 + 16;
+  lay.bp_mask = bar_parallel_mask(nj);
+  // team members cost shared memory (a transpose stage and lines each): give
+  // up spare warps until the layout fits
+  const int fixed = off;
+  for (int b = std::min(budget, kMaxConsumers);; --b) {
+    if (b < nj) return false;
+    assign_warps(L, jl, nj, lay, b);
+    off = fixed;
+    for (int w = 0; w <= lay.nconsumers; ++w) {
+      const int jb = lay.warp_job[w];
+      off = (off + 15) & ~15;
+      lay.stage_off[w] = off;
+      if (jb < 0) continue;
+      if (!bar_parallel(lay.bp_mask, L.jobs[jb].family)) off += out_count(L.jobs[jb].family) * 32 * (C + 1) * 4;
+      off = (off + 15) & ~15;
+      lay.line_off[w] = off;
+      off += line_bytes(L.jobs[jb], lay.bp_mask);
+    }
+    lay.total = (off + 127) & ~127;
+    if (lay.total <= limit) return true;
+  }
+}
+
+// Jobs into P partitions by the measured per-warp cost, heaviest first: onto
+// the least loaded partition that already reads the job's input planes while
+// it stays within 1.2x the mean load, else onto the least loaded partition (a
+// partition's ring holds only the planes its jobs read).
+void partition_jobs(const Launch& L, int P, int* part) {
+  const unsigned long long bp = bar_parallel_mask(L.njobs);
+  int order[kMaxJobs];
+  double load[kMaxParts] = {}, total = 0.0;
+  unsigned planes[kMaxParts] = {};
+  for (int j = 0; j < L.njobs; ++j) {
+    order[j] = j;
+    total += family_cost(L.jobs[j], bp);
+  }
+  std::stable_sort(order, order + L.njobs,
+                   [&](int a, int b) { return family_cost(L.jobs[a], bp) > family_cost(L.jobs[b], bp); });
+  const double cap = 1.2 * total / P;
+  for (int k = 0; k < L.njobs; ++k) {
+    const int j = order[k];
+    const unsigned m = job_planes(L.jobs[j]);
+    const double c = family_cost(L.jobs[j], bp);
+    int best = -1;
+    for (int q = 0; q < P; ++q)
+      if (planes[q] != 0 && (planes[q] & m) == m && load[q] + c <= cap && (best < 0 || load[q] < load[best])) best = q;
+    if (best < 0) {
+      best = 0;
+      for (int q = 1; q < P; ++q)
+        if (load[q] < load[best]) best = q;
+    }
+    part[j] = best;
+    load[best] += c;
+    planes[best] |= m;
+  }
+}
+
+// partition_jobs, then the partitions left empty dropped; returns their number
+int partition_nonempty(const Launch& L, int P, int* part) {
+  partition_jobs(L, P, part);
+  int id[kMaxParts], n = 0;
+  for (int q = 0; q < P; ++q) {
+    id[q] = -1;
+    for (int j = 0; j < L.njobs; ++j)
+      if (part[j] == q) {
+        id[q] = n++;
+        break;
+      }
+  }
+  for (int j = 0; j < L.njobs; ++j) part[j] = id[part[j]];
+  return n;
+}
+
+// The partitions, groups per CTA and per-partition layouts of a launch
+// (host only). TACUDA_B200_ROWS_PARTS / TACUDA_B200_ROWS_GROUPS /
+// TACUDA_B200_ROWS_DEPTH pin P, G and the ring depth (read on every call);
+// none of them changes a bit of any output. False when no layout fits.
+bool plan_split(const Launch& L, int parts, int groups, int smem_optin, Split& sp) {
+  if (const char* v = std::getenv("TACUDA_B200_ROWS_PARTS")) parts = std::atoi(v);
+  if (const char* v = std::getenv("TACUDA_B200_ROWS_GROUPS")) groups = std::atoi(v);
+  // Defaults: a job set of five or more jobs is split into five partitions,
+  // each CTA running two row groups (13-indicator pass, 4000 x 234: 210 ->
+  // 152 us; the same jobs over 10,000 ragged rows: 12.6 -> 8.2 ms). A CTA then
+  // holds the code of a few families instead of all of them, and each SM works
+  // on 64 rows of a partition instead of 32 rows of everything.
+  if (parts <= 0) parts = L.njobs >= 5 ? 5 : 1;
+  if (groups <= 0) groups = parts > 1 ? 2 : 1;
+  int P = std::max(1, std::min({parts > 0 ? parts : 1, L.njobs, kMaxParts}));
+  int G = std::max(1, std::min(groups > 0 ? groups : 1, kMaxWarps / 2));
+  const long long ngroups = ((long long)L.S + 31) / 32;
+  if (G > ngroups) G = (int)ngroups;
+  int part[kMaxJobs];
+  P = partition_nonempty(L, P, part);
+  std::memset(&sp, 0, sizeof(sp));
+  sp.P = P;
+  // ring depth (chunks past the halo): 4, or less when that lets G groups fit
+  int dmax = 4, dmin = 2;
+  if (const char* v = std::getenv("TACUDA_B200_ROWS_DEPTH")) dmax = dmin = std::max(2, std::min(4, std::atoi(v)));
+  // the largest G <= the request whose partitions all fit: job warps within
+  // the CTA's warp budget and G groups within the shared memory
+  for (;; --G) {
+    if (G < 1) return false;
+    const int budget = kMaxWarps / G - 1;
+    bool ok = false;
+    for (int depth = dmax; depth >= (G > 1 ? dmin : dmax) && !ok; --depth) {
+      ok = true;
+      for (int q = 0; q < P && ok; ++q) {
+        int jl[kMaxJobs], nj = 0;
+        for (int j = 0; j < L.njobs; ++j)
+          if (part[j] == q) jl[nj++] = j;
+        ok = nj > 0 && build_layout(L, jl, nj, budget, smem_optin / G, depth, sp.lay[q]);
+      }
+    }
+    if (ok) break;
+  }
+  sp.G = G;
+  return true;
 }
 
 }  // namespace
@@ -441,7 +602,7 @@ bool supports(const Launch& L, long long max_len) {
   return true;
 }
 
-cudaError_t launch(Launch& L, long long max_len, cudaStream_t stream, LaunchStats* stats) {
+cudaError_t launch(Launch& L, long long max_len, cudaStream_t stream, LaunchStats* stats, int parts, int groups) {
   if (!supports(L, max_len)) return cudaErrorNotSupported;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -463,63 +624,25 @@ cudaError_t launch(Launch& L, long long max_len, cudaStream_t stream, LaunchStat
       ds->attr = true;
     }
   }
-  Layout lay;
-  std::memset(&lay, 0, sizeof(lay));
-  unsigned mask = 0;
-  int H = 1;
-  for (int j = 0; j < L.njobs; ++j) {
-    mask |= job_planes(L.jobs[j]);
-    H = std::max(H, rows_halo(L.jobs[j]));
+  Split sp;
+  if (!plan_split(L, parts, groups, ds->smem_optin, sp)) return cudaErrorNotSupported;
+  const int P = sp.P, G = sp.G;
+  const long long ngroups = ((long long)L.S + 31) / 32;
+  int wmax = 0, smem = 0;
+  for (int q = 0; q < P; ++q) {
+    wmax = std::max(wmax, sp.lay[q].nconsumers + 1);
+    smem = std::max(smem, G * sp.lay[q].total);
   }
-  int np = 0;
-  for (int p = 0; p < P_COUNT; ++p) {
-    lay.plane_slot[p] = (mask & (1u << p)) ? np : -1;
-    if (mask & (1u << p)) lay.slot_plane[np++] = p;
-  }
-  lay.nplanes = np;
-  lay.Hs = std::max(1, (H + C - 1) / C);
-  lay.NS = lay.Hs + 4;  // three chunks in flight ahead of the slowest job
-  lay.RS = (lay.Hs + lay.NS) * C + 1;
-  int off = 0;
-  lay.ring_off = off;
-  off += np * 32 * lay.RS * 4;
-  off = (off + 15) & ~15;
-  lay.bar_off = off;
-  off += 2 * lay.NS * 8;
-  lay.tab_off = off;
-  off += 64 * 8 + 16;
-  lay.bp_mask = bar_parallel_mask(L);
-  // team members cost shared memory (a transpose stage and lines each): give
-  // up spare warps until the layout fits
-  const int fixed = off;
-  for (int budget = kMaxConsumers;; --budget) {
-    assign_warps(L, lay, budget);
-    off = fixed;
-    for (int w = 0; w <= lay.nconsumers; ++w) {
-      const int jb = lay.warp_job[w];
-      off = (off + 15) & ~15;
-      lay.stage_off[w] = off;
-      if (jb < 0) continue;
-      if (!bar_parallel(lay.bp_mask, L.jobs[jb].family)) off += out_count(L.jobs[jb].family) * 32 * (C + 1) * 4;
-      off = (off + 15) & ~15;
-      lay.line_off[w] = off;
-      off += line_bytes(L.jobs[jb], lay.bp_mask);
-    }
-    lay.total = (off + 127) & ~127;
-    if (lay.total <= ds->smem_optin) break;
-    if (budget <= L.njobs) return cudaErrorNotSupported;
-  }
-  const long long groups = ((long long)L.S + 31) / 32;
-  if (groups > INT_MAX) return cudaErrorInvalidValue;
-  const int threads = 32 * (lay.nconsumers + 1);
+  const dim3 grid((unsigned)((ngroups + G - 1) / G), (unsigned)P);
+  const int threads = 32 * G * wmax;
   bool all = false;
   for (int j = 0; j < L.njobs; ++j) all |= !core_family(L.jobs[j].family);
-  if (all) rows_kernel<true><<<(unsigned)groups, threads, lay.total, stream>>>(L, lay);
-  else rows_kernel<false><<<(unsigned)groups, threads, lay.total, stream>>>(L, lay);
+  if (all) rows_kernel<true><<<grid, threads, smem, stream>>>(L, sp);
+  else rows_kernel<false><<<grid, threads, smem, stream>>>(L, sp);
   if (stats) {
-    stats->blocks = (int)groups;
-    stats->warps_per_block = lay.nconsumers + 1;
-    stats->smem_per_block = lay.total;
+    stats->blocks = (int)(grid.x * grid.y);
+    stats->warps_per_block = G * wmax;
+    stats->smem_per_block = smem;
     stats->k = 0;
     stats->blocks_per_sm = 1;
   }

@@ -45,7 +45,9 @@ namespace rows {
 constexpr int C = 32;                 // bars per chunk
 constexpr int kMaxHalo = 64;          // bars of history a job may read before a chunk
 constexpr int kMaxLine = 64;          // per-lane history of the line-keeping families
-constexpr int kMaxConsumers = 19;     // job warps per CTA (one more warp stages the inputs)
+constexpr int kMaxConsumers = 19;     // job warps per row group (one more warp stages the inputs)
+constexpr int kMaxWarps = kMaxConsumers + 1;  // warps per CTA over all its row groups
+constexpr int kMaxParts = 8;          // partitions of a job set (one per grid row)
 constexpr int kFp32MaxPeriod = 32;    // recurrences up to this period keep float32 state
 constexpr unsigned long long kWaitNs = 1000000000ull;  // one mbarrier wait gives up after 1 s
 constexpr unsigned long long kStallWaitNs = 1000000ull;  // 1 ms under the stall test knob
@@ -67,6 +69,13 @@ struct Layout {
   int stage_off[kMaxConsumers + 1];   // [nout][32][C+1] floats
   int line_off[kMaxConsumers + 1];    // per-warp history lines
   int total;
+};
+
+// A launch: the job set split into P partitions (grid row y runs partition y
+// with layout lay[y]), each CTA running G row groups of 32 rows.
+struct Split {
+  int P, G;
+  Layout lay[kMaxParts];
 };
 
 // ------------------------------------------------------------ primitives
@@ -1551,10 +1560,13 @@ __device__ void w_talib_bar(const Warp& w, const Job& j, int mode) {
 }
 
 // QSTICK (qstick_round in families.cuh): TA_QSTICK's mean of close - open from
-// the runner's start bar; after a NaN difference every later output is NaN.
+// the runner's start bar; after a NaN difference every later output is NaN,
+// and so is every output from p bars after an infinite difference (the
+// running sum's inf - inf when it leaves the window).
 __device__ void w_qstick(const Warp& w, const Job& j) {
   const int po = j.in[0], pc = j.in[1], p = j.ip[0];
-  int f = -1, g = -1;
+  int f = -1;
+  long long stop = 1ll << 62;
   for (int c = 0; c < w.nchunks; ++c) {
     if (!w.wait(c)) return;
     const float* O = w.X(c, po);
@@ -1563,9 +1575,13 @@ __device__ void w_qstick(const Warp& w, const Job& j) {
     for (int r = 0; r < lim; ++r) {
       const int t = t0 + r;
       if (f < 0 && !isnan(O[r]) && !isnan(C2[r])) f = t;
-      if (f >= 0 && g < 0 && isnan((double)C2[r] - (double)O[r])) g = t;
+      if (f >= 0) {
+        const double d = (double)C2[r] - (double)O[r];
+        if (isnan(d)) stop = min(stop, (long long)t);
+        else if (isinf(d)) stop = min(stop, (long long)t + p);
+      }
       float o = qnan();
-      if (f >= 0 && t >= f + p - 1 && g < 0) {
+      if (f >= 0 && t >= f + p - 1 && t < stop) {
         double s = 0.0;
         for (int i = r - p + 1; i <= r; ++i) s += (double)C2[i] - (double)O[i];
         o = (float)(s / (double)p);

@@ -41,8 +41,8 @@ void load_cache_locked() {
   ShapeKey k{};
   SchedulePlan p{};
   unsigned long long jobs = 0;
-  while (std::fscanf(f, "%d %d %d %llx %d %d %d %d %d", &k.S_bucket, &k.T_bucket, &k.Tmax_bucket, &jobs, &p.mode,
-                     &p.groups, &p.k, &p.warps_per_block, &p.max_blocks) == 9) {
+  while (std::fscanf(f, "%d %d %d %llx %d %d %d %d %d %d", &k.S_bucket, &k.T_bucket, &k.Tmax_bucket, &jobs, &p.mode,
+                     &p.groups, &p.k, &p.warps_per_block, &p.max_blocks, &p.parts) == 10) {
     k.jobs = jobs;
     g_tuned.emplace_back(k, p);
   }
@@ -121,9 +121,9 @@ void remember_plan(const ShapeKey& key, const SchedulePlan& plan) {
   g_tuned.emplace_back(key, plan);
   if (const char* path = std::getenv("TACUDA_B200_TUNE_CACHE")) {
     if (FILE* f = std::fopen(path, "a")) {
-      std::fprintf(f, "%d %d %d %llx %d %d %d %d %d\n", key.S_bucket, key.T_bucket, key.Tmax_bucket,
+      std::fprintf(f, "%d %d %d %llx %d %d %d %d %d %d\n", key.S_bucket, key.T_bucket, key.Tmax_bucket,
                    (unsigned long long)key.jobs, plan.mode, plan.groups, plan.k, plan.warps_per_block,
-                   plan.max_blocks);
+                   plan.max_blocks, plan.parts);
       std::fclose(f);
     }
   }

@@ -13,7 +13,8 @@ namespace tb {
 struct SchedulePlan {
   int mode = 0;            // 0: warp per series (time-parallel lanes), 1: thread per series,
                            // 2: warp per tile with decoupled look-back between tiles
-  int groups = 0;          // series-parallel: 32-series groups per CTA (0 = auto)
+  int groups = 0;          // row-parallel: 32-row groups per CTA (0 = auto)
+  int parts = 0;           // row-parallel: partitions of the job set, one per grid row (0 = auto)
   int k = 8;               // bars per lane; a round covers 32*k bars
   int warps_per_block = 8;
   int max_blocks = 0;      // 0 = as many as fit
@@ -51,7 +52,8 @@ namespace rows {
 // Row-parallel engine (rows.cu): whether it takes this job set and batch, and
 // its launch. Returns cudaErrorNotSupported for job sets it does not take.
 bool supports(const Launch& L, long long max_len);
-cudaError_t launch(Launch& L, long long max_len, cudaStream_t stream, LaunchStats* stats);
+cudaError_t launch(Launch& L, long long max_len, cudaStream_t stream, LaunchStats* stats, int parts = 0,
+                   int groups = 0);
 }  // namespace rows
 
 // Look-back launch with its scratch in a static device array of

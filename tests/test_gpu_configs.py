@@ -192,6 +192,8 @@ def _check_autotuned(plan):
     if best["engine"] != "row-parallel":
         assert (chosen["bars_per_lane"], chosen["warps_per_block"]) == (best["bars_per_lane"],
                                                                          best["warps_per_block"])
+    else:
+        assert (chosen["parts"], chosen["groups"]) == (best["parts"], best["groups"])
     return cands
 
 

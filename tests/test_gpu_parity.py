@@ -11,6 +11,7 @@ import torch
 
 import tacuda_b200 as tb
 from gpu_util import DEFAULTS, SPECS, call_batch_d, device_planes, to_np
+from test_oracle_pin import qstick_inf_rows
 from oracle import oracle as O
 from tacuda_b200 import synthetic, workloads
 from tolerance import compare
@@ -508,4 +509,13 @@ def test_talib_runner_prefix_rule(mode):
         ref = O.run(name, d, **p)[0]
         compare(got, ref, f"prefix {name}")
     assert np.isnan(to_np(call_batch_d("qstick", dp, dict(period=10)))[0][4, 500:]).all()
+    # infinite close - open differences: TA_QSTICK's running sum is inf while
+    # one is in the window and NaN for good once it leaves
+    q = qstick_inf_rows()
+    got = to_np(call_batch_d("qstick", device_planes(q), dict(period=10)))[0]
+    ref = O.run("qstick", q, period=10)[0]
+    for kind in (np.isposinf, np.isneginf):
+        np.testing.assert_array_equal(kind(got), kind(ref))
+    fin = np.isfinite(ref)
+    compare(np.where(fin, got, np.nan), np.where(fin, ref, np.nan), "qstick with infinite differences")
     assert to_np(call_batch_d("ibs", dp, {}))[0][3, -1] == 0.5

@@ -69,6 +69,39 @@ def test_oracle_matches_reference_build(shape, seed):
                                       O.ref_cdl(k, d["open"], d["high"], d["low"], d["close"]), err_msg=f"candle {k}")
 
 
+def qstick_inf_rows():
+    """Rows whose close - open differences hold infinities: TA_QSTICK's running
+    sum turns NaN for good once an infinite difference leaves the window."""
+    d = synthetic.ohlcv(4, 300, seed=31)
+    d["close"][0, 100] = np.inf                       # inf for 10 bars, then NaN
+    d["close"][1, 50] = np.inf
+    d["open"][1, 53] = np.inf                         # -inf difference: NaN at once
+    d["open"][2, 5] = -np.inf                         # inf inside the first window
+    d["close"][3, 200] = np.inf
+    d["open"][3, 200] = np.inf                        # inf - inf: a NaN difference
+    return d
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference CPU build not present")
+def test_qstick_infinite_difference_matches_reference_build():
+    d = qstick_inf_rows()
+    a = O.run("qstick", d, period=10)[0]
+    b = O.ref_run("qstick", d, period=10)[0]
+    for kind in (np.isnan, np.isposinf, np.isneginf):
+        np.testing.assert_array_equal(kind(a), kind(b))
+    fin = np.isfinite(b)
+    compare(np.where(fin, a, np.nan), np.where(fin, b, np.nan), "qstick with infinite differences", rtol=1e-6,
+            row_atol=1e-9)
+
+
+def test_qstick_infinite_difference_rule():
+    a = O.run("qstick", qstick_inf_rows(), period=10)[0]
+    assert np.isposinf(a[0, 100:110]).all() and np.isnan(a[0, 110:]).all() and np.isfinite(a[0, 9:100]).all()
+    assert np.isposinf(a[1, 50:53]).all() and np.isnan(a[1, 53:]).all()
+    assert np.isposinf(a[2, 9:15]).all() and np.isnan(a[2, 15:]).all()
+    assert np.isfinite(a[3, 9:200]).all() and np.isnan(a[3, 200:]).all()
+
+
 # ---- known answers (tests/cpp/test_edge_cases.cpp, tests/python/batch_fused.py) ----
 
 def flat(T=129, value=100.0):

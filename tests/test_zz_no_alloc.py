@@ -1,14 +1,16 @@
 """GPU: the allocation-free look-back entry point (static device scratch)
 against the look-back engine of the regular fused entry point, whose scratch
-comes from the stream-ordered pool. Kept in its own file, collected last, so
+comes from the stream-ordered pool, and against the FP64 oracle. Kept in its own file, collected last, so
 it also runs after every other test has used the library."""
 import ctypes as ct
 import os
 
+import numpy as np
 import pytest
 import torch
 
 import tacuda_b200 as tb
+from oracle import oracle as O
 from tacuda_b200 import synthetic, workloads
 from tolerance import compare
 
@@ -22,35 +24,55 @@ def _entry():
     return f
 
 
-def _pass13(S, T, seed):
+def _jobs(S, T, seed, extra):
+    """The 13-indicator pass, plus (extra) two appended families (QSTICK, RMA),
+    which run on the look-back engine's second set of kernels."""
     d = synthetic.ohlcv(S, T, seed=seed)
     dp = {k: torch.from_numpy(v).cuda() for k, v in d.items()}
-    outs = {n: torch.full((S, T), 777.0, device="cuda") for n in workloads.PASS13_OUTPUTS}
-    jobs = [tb.make_job(fam, p, fp, [outs[o].data_ptr() for o in on]) for _, fam, p, fp, on in workloads.PASS13]
+    spec = [(fam, p, fp, on) for _, fam, p, fp, on in workloads.PASS13]
+    if extra:
+        spec += [("qstick", (10,), (), ("qstick",)), ("rma", (14,), (), ("rma",))]
+    names = [n for *_, on in spec for n in on]
+    outs = {n: torch.full((S, T), 777.0, device="cuda") for n in names}
+    jobs = [tb.make_job(fam, p, fp, [outs[o].data_ptr() for o in on]) for fam, p, fp, on in spec]
     series = tb.make_series({k: v.data_ptr() for k, v in dp.items() if k in tb.PLANE_ID}, S, T)
-    return dp, outs, jobs, series
+    return d, outs, jobs, series, spec
 
 
-def test_static_scratch_matches_pool_scratch_twice():
+@pytest.mark.parametrize("on_stream", [False, True], ids=["null-stream", "user-stream"])
+@pytest.mark.parametrize("extra", [False, True], ids=["pass13", "pass13+qstick+rma"])
+@pytest.mark.parametrize("k", [4, 8, 16])
+def test_static_scratch_matches_pool_scratch_twice(k, extra, on_stream, monkeypatch):
+    """Two calls in a row of the static-scratch entry give the bits of the
+    pool-scratch look-back launch, and both agree with the FP64 oracle."""
     S, T = 2, 40000
-    dp, outs, jobs, series = _pass13(S, T, seed=31)
-    os.environ["TACUDA_B200_MODE"] = "lb"
-    try:
-        tb.fused_batch_d(series, jobs, 0)
-    finally:
-        del os.environ["TACUDA_B200_MODE"]
+    d, outs, jobs, series, spec = _jobs(S, T, seed=31 + k, extra=extra)
+    monkeypatch.setenv("TACUDA_B200_BARS_PER_LANE", str(k))
+    monkeypatch.setenv("TACUDA_B200_MODE", "lb")
+    tb.fused_batch_d(series, jobs, 0)
+    monkeypatch.delenv("TACUDA_B200_MODE")
     torch.cuda.synchronize()
-    ref = {k: v.clone() for k, v in outs.items()}
+    ref = {n: v.cpu().numpy() for n, v in outs.items()}
+    for fam, p, fp, on in spec:
+        params = workloads.ORACLE_PARAMS[fam](p, fp) if fam in workloads.ORACLE_PARAMS else {"period": p[0]}
+        for name, want in zip(on, O.run(fam, d, **params)):
+            compare(ref[name], want, f"pool look-back {name}")
     arr = tb.job_array(jobs)
     f = _entry()
+    stream = torch.cuda.Stream() if on_stream else None
     for call in range(2):
         for v in outs.values():
             v.fill_(777.0)
-        rc = f(ct.addressof(series), ct.addressof(arr), len(jobs), None)
-        tb.call_status(rc, "ct_b200_fused_lookback_static_d")
         torch.cuda.synchronize()
-        for k in outs:
-            compare(outs[k].cpu().numpy(), ref[k].cpu().numpy().astype("float64"), f"static call {call} {k}")
+        rc = f(ct.addressof(series), ct.addressof(arr), len(jobs), stream.cuda_stream if stream else None)
+        tb.call_status(rc, "ct_b200_fused_lookback_static_d")
+        if stream is not None:
+            stream.synchronize()
+        torch.cuda.synchronize()
+        for name, v in outs.items():
+            got = v.cpu().numpy()
+            assert np.array_equal(got.view(np.uint32), ref[name].view(np.uint32)), f"static call {call} {name}"
+    assert tb.take_device_error() == 0
 
 
 def test_static_scratch_rejects_oversized_batch():
