@@ -450,7 +450,7 @@ def profile_case(case: str) -> None:
       cdl          candle tile kernel, 61 patterns, 4000 x 2000 bars
       alpha        alpha forward + adjoint, 4096 x 2048 bars
       lb5          long-row jobs through look-back, 4 x 2,000,000 bars
-      fam:<name>   one job of the 13-indicator pass alone, 4000 x 234 bars"""
+      fam:<names>  jobs of the 13-indicator pass alone (comma-separated), 4000 x 234 bars"""
     import torch
     import tacuda_b200 as tb
     from tacuda_b200 import synthetic, workloads
@@ -466,9 +466,9 @@ def profile_case(case: str) -> None:
             jobs = [tb.make_job("cdl", (), (), [out.data_ptr()], cdl_mask=mask, cdl_stride=S * T, cdl_int32=True)]
         else:
             outs = {n: torch.empty((S, T), device="cuda") for n in workloads.PASS13_OUTPUTS}
-            only = case[4:] if case.startswith("fam:") else None
+            only = case[4:].split(",") if case.startswith("fam:") else None
             jobs = [tb.make_job(fam, p, fp, [outs[o].data_ptr() for o in on])
-                    for name, fam, p, fp, on in workloads.PASS13 if only in (None, name)]
+                    for name, fam, p, fp, on in workloads.PASS13 if only is None or name in only]
             if not jobs:
                 raise SystemExit(f"unknown job {only!r}")
         for _ in range(3):

@@ -213,18 +213,22 @@ __device__ void produce(const Launch& L, const Layout& lay, unsigned char* smem,
   cp_async_wait_all();
 }
 
-// CTA (x, y): partition y of the job set over row groups x*G .. x*G+G-1; each
-// group has its own warps, ring, mbarriers and tables (a block of lay.total
-// bytes of shared memory), so the groups of a CTA run independently.
+// CTA x of partition y (cta0[y] <= x < cta0[y+1]) runs row groups
+// (x - cta0[y])*G[y] .. +G[y]-1 of that partition's jobs; each group has its
+// own warps, ring, mbarriers and tables (a block of lay.total bytes of shared
+// memory), so the groups of a CTA run independently.
 template <bool kAll>
 __global__ void __launch_bounds__(32 * kMaxWarps, 1) rows_kernel(const __grid_constant__ Launch L, const __grid_constant__ Split sp) {
   extern __shared__ __align__(16) unsigned char smem_all[];
-  const Layout& lay = sp.lay[blockIdx.y];
+  int y = 0;
+  while (y + 1 < sp.P && (int)blockIdx.x >= sp.cta0[y + 1]) ++y;
+  const Layout& lay = sp.lay[y];
+  const int G = sp.G[y];
   const int wpg = lay.nconsumers + 1;
   const int gw = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = gw / wpg, warp = gw - sub * wpg;
-  const long long group = (long long)blockIdx.x * sp.G + sub;
-  const bool live = sub < sp.G && group * 32 < (long long)L.S;
+  const long long group = (long long)((int)blockIdx.x - sp.cta0[y]) * G + sub;
+  const bool live = sub < G && group * 32 < (long long)L.S;
   unsigned char* smem = smem_all + (size_t)(live ? sub : 0) * lay.total;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + lay.bar_off);
   uint64_t* empty = full + lay.NS;
@@ -444,7 +448,7 @@ void assign_warps(const Launch& L, const int* jl, int nj, Layout& lay, int budge
 // The shared-memory layout and warps of one row group running jobs jl[0..nj)
 // with at most `budget` job warps, within `limit` bytes: team warps are given
 // up until it fits. False when even one warp per job does not fit.
-bool build_layout(const Launch& L, const int* jl, int nj, int budget, int limit, int depth, Layout& lay) {
+bool build_layout(const Launch& L, const int* jl, int nj, int budget, int limit, int depth, bool split, Layout& lay) {
   std::memset(&lay, 0, sizeof(lay));
   unsigned mask = 0;
   int H = 1;
@@ -469,7 +473,10 @@ bool build_layout(const Launch& L, const int* jl, int nj, int budget, int limit,
   off += 2 * lay.NS * 8;
   lay.tab_off = off;
   off += 64 * 8 + 16;
-  lay.bp_mask = bar_parallel_mask(nj);
+  // a partition of a split job set keeps WILLR / STOCH row-sequential: the
+  // bar-parallel form doubles their instructions, which pays only when they
+  // have an SM's issue slots to themselves
+  lay.bp_mask = split ? (1ull << F_CCI) : bar_parallel_mask(nj);
   // team members cost shared memory (a transpose stage and lines each): give
   // up spare warps until the layout fits
   const int fixed = off;
@@ -550,16 +557,17 @@ bool plan_split(const Launch& L, int parts, int groups, int smem_optin, Split& s
   if (const char* v = std::getenv("TACUDA_B200_ROWS_PARTS")) parts = std::atoi(v);
   if (const char* v = std::getenv("TACUDA_B200_ROWS_GROUPS")) groups = std::atoi(v);
   // Defaults: a job set of five or more jobs is split into five partitions,
-  // each CTA running two row groups (13-indicator pass, 4000 x 234: 210 ->
-  // 152 us; the same jobs over 10,000 ragged rows: 12.6 -> 8.2 ms). A CTA then
-  // holds the code of a few families instead of all of them, and each SM works
-  // on 64 rows of a partition instead of 32 rows of everything.
+  // each CTA running up to two row groups (13-indicator pass, 4000 x 234:
+  // 210 -> 145-155 us; the same jobs over 10,000 ragged rows: 11.3-12.6 ->
+  // 8.2 ms). A CTA then holds the code of a few families instead of all of
+  // them (instruction-cache hit rate 59 -> 90 %), and each SM works on 64 rows
+  // of a partition instead of 32 rows of everything. More partitions or more
+  // groups per CTA measured within noise of this; the autotuner tries 4-6.
   if (parts <= 0) parts = L.njobs >= 5 ? 5 : 1;
   if (groups <= 0) groups = parts > 1 ? 2 : 1;
-  int P = std::max(1, std::min({parts > 0 ? parts : 1, L.njobs, kMaxParts}));
-  int G = std::max(1, std::min(groups > 0 ? groups : 1, kMaxWarps / 2));
+  int P = std::max(1, std::min({parts, L.njobs, kMaxParts}));
   const long long ngroups = ((long long)L.S + 31) / 32;
-  if (G > ngroups) G = (int)ngroups;
+  const int Gmax = (int)std::max(1ll, std::min<long long>(std::min(groups, kMaxWarps / 2), ngroups));
   int part[kMaxJobs];
   P = partition_nonempty(L, P, part);
   std::memset(&sp, 0, sizeof(sp));
@@ -567,24 +575,23 @@ bool plan_split(const Launch& L, int parts, int groups, int smem_optin, Split& s
   // ring depth (chunks past the halo): 4, or less when that lets G groups fit
   int dmax = 4, dmin = 2;
   if (const char* v = std::getenv("TACUDA_B200_ROWS_DEPTH")) dmax = dmin = std::max(2, std::min(4, std::atoi(v)));
-  // the largest G <= the request whose partitions all fit: job warps within
-  // the CTA's warp budget and G groups within the shared memory
-  for (;; --G) {
-    if (G < 1) return false;
-    const int budget = kMaxWarps / G - 1;
-    bool ok = false;
-    for (int depth = dmax; depth >= (G > 1 ? dmin : dmax) && !ok; --depth) {
-      ok = true;
-      for (int q = 0; q < P && ok; ++q) {
-        int jl[kMaxJobs], nj = 0;
-        for (int j = 0; j < L.njobs; ++j)
-          if (part[j] == q) jl[nj++] = j;
-        ok = nj > 0 && build_layout(L, jl, nj, budget, smem_optin / G, depth, sp.lay[q]);
-      }
+  // per partition, the largest G <= Gmax that fits: job warps within the
+  // CTA's warp budget and G groups within the shared memory
+  for (int q = 0; q < P; ++q) {
+    int jl[kMaxJobs], nj = 0;
+    for (int j = 0; j < L.njobs; ++j)
+      if (part[j] == q) jl[nj++] = j;
+    int G = Gmax;
+    for (;; --G) {
+      if (G < 1) return false;
+      bool ok = false;
+      for (int depth = dmax; depth >= (G > 1 ? dmin : dmax) && !ok; --depth)
+        ok = build_layout(L, jl, nj, kMaxWarps / G - 1, smem_optin / G, depth, P > 1, sp.lay[q]);
+      if (ok) break;
     }
-    if (ok) break;
+    sp.G[q] = G;
+    sp.cta0[q + 1] = sp.cta0[q] + (int)((ngroups + G - 1) / G);
   }
-  sp.G = G;
   return true;
 }
 
@@ -626,22 +633,20 @@ cudaError_t launch(Launch& L, long long max_len, cudaStream_t stream, LaunchStat
   }
   Split sp;
   if (!plan_split(L, parts, groups, ds->smem_optin, sp)) return cudaErrorNotSupported;
-  const int P = sp.P, G = sp.G;
-  const long long ngroups = ((long long)L.S + 31) / 32;
   int wmax = 0, smem = 0;
-  for (int q = 0; q < P; ++q) {
-    wmax = std::max(wmax, sp.lay[q].nconsumers + 1);
-    smem = std::max(smem, G * sp.lay[q].total);
+  for (int q = 0; q < sp.P; ++q) {
+    wmax = std::max(wmax, sp.G[q] * (sp.lay[q].nconsumers + 1));
+    smem = std::max(smem, sp.G[q] * sp.lay[q].total);
   }
-  const dim3 grid((unsigned)((ngroups + G - 1) / G), (unsigned)P);
-  const int threads = 32 * G * wmax;
+  const dim3 grid((unsigned)sp.cta0[sp.P]);
+  const int threads = 32 * wmax;
   bool all = false;
   for (int j = 0; j < L.njobs; ++j) all |= !core_family(L.jobs[j].family);
   if (all) rows_kernel<true><<<grid, threads, smem, stream>>>(L, sp);
   else rows_kernel<false><<<grid, threads, smem, stream>>>(L, sp);
   if (stats) {
-    stats->blocks = (int)(grid.x * grid.y);
-    stats->warps_per_block = G * wmax;
+    stats->blocks = (int)grid.x;
+    stats->warps_per_block = wmax;
     stats->smem_per_block = smem;
     stats->k = 0;
     stats->blocks_per_sm = 1;

@@ -71,10 +71,12 @@ struct Layout {
   int total;
 };
 
-// A launch: the job set split into P partitions (grid row y runs partition y
-// with layout lay[y]), each CTA running G row groups of 32 rows.
+// A launch: the job set split into P partitions; CTAs cta0[y] .. cta0[y+1]-1
+// run partition y with layout lay[y], G[y] row groups of 32 rows each.
 struct Split {
-  int P, G;
+  int P;
+  int G[kMaxParts];
+  int cta0[kMaxParts + 1];
   Layout lay[kMaxParts];
 };
 
