@@ -450,7 +450,8 @@ def profile_case(case: str) -> None:
       cdl          candle tile kernel, 61 patterns, 4000 x 2000 bars
       alpha        alpha forward + adjoint, 4096 x 2048 bars
       lb5          long-row jobs through look-back, 4 x 2,000,000 bars
-      fam:<names>  jobs of the 13-indicator pass alone (comma-separated), 4000 x 234 bars"""
+      fam:<names>  jobs of the 13-indicator pass alone (comma-separated), 4000 x 234 bars
+      single100k   SMA20 EMA30 RSI14 MACD12/26/9 over one 100,000-bar series"""
     import torch
     import tacuda_b200 as tb
     from tacuda_b200 import synthetic, workloads
@@ -471,6 +472,15 @@ def profile_case(case: str) -> None:
                     for name, fam, p, fp, on in workloads.PASS13 if only is None or name in only]
             if not jobs:
                 raise SystemExit(f"unknown job {only!r}")
+        for _ in range(3):
+            tb.fused_batch_d(ser, jobs, 0)
+    elif case == "single100k":
+        x = torch.from_numpy(synthetic.single_close(100_000, seed=11).astype(np.float32)).cuda().reshape(1, -1)
+        o = {n: torch.empty_like(x) for n in ("sma", "ema", "rsi", "macd", "sig", "hist")}
+        jobs = [tb.make_job("sma", (20,), (), [o["sma"].data_ptr()]), tb.make_job("ema", (30,), (), [o["ema"].data_ptr()]),
+                tb.make_job("rsi", (14,), (), [o["rsi"].data_ptr()]),
+                tb.make_job("macd", (12, 26, 9), (), [o[k].data_ptr() for k in ("macd", "sig", "hist")])]
+        ser = tb.make_series({"close": x.data_ptr()}, 1, x.shape[1])
         for _ in range(3):
             tb.fused_batch_d(ser, jobs, 0)
     elif case == "alpha":

@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <type_traits>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <vector>
 
@@ -452,7 +453,44 @@ int max_lookback_halo(const Launch& L) {
 
 // Candle jobs run on the bar-parallel tile kernel; consecutive jobs reading
 // the same planes share one launch.
-cudaError_t launch_candles(const Launch& L, const Job* jobs, int n, cudaStream_t stream) {
+// The candle pass of a job set that also has indicator jobs runs beside the
+// indicator engine, on a library-owned stream of the lowest priority forked
+// from and joined back into the caller's stream (events, so graph capture
+// sees an ordinary fork and join). The indicator engine's CTAs are launched
+// first and keep their SMs; candle blocks fill the SMs the engine leaves
+// idle, e.g. while the CTAs of the longest ragged rows finish.
+struct SideStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  std::mutex m;
+};
+std::mutex g_side_mutex;
+std::vector<std::unique_ptr<SideStream>> g_side;
+
+cudaError_t side_stream(SideStream** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(g_side_mutex);
+  if ((int)g_side.size() <= dev) g_side.resize(dev + 1);
+  if (!g_side[dev]) {
+    std::unique_ptr<SideStream> ss(new SideStream);
+    int least = 0, greatest = 0;
+    e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&ss->s, cudaStreamNonBlocking, least);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ss->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ss->join, cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+    g_side[dev] = std::move(ss);
+  }
+  *out = g_side[dev].get();
+  return cudaSuccess;
+}
+
+// `beside`: the pass shares the GPU with another kernel, so every row gets a
+// block of its own (longest rows first) and the block scheduler hands them to
+// SMs as those free up; alone, the pass runs as a persistent grid.
+cudaError_t launch_candles(const Launch& L, const Job* jobs, int n, cudaStream_t stream, bool beside = false) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
@@ -475,7 +513,7 @@ cudaError_t launch_candles(const Launch& L, const Job* jobs, int n, cudaStream_t
     A.S = L.S;
     int b = a;
     while (b < n && std::memcmp(jobs[b].in, jobs[a].in, sizeof(jobs[a].in)) == 0) A.jobs[A.njobs++] = jobs[b++];
-    const long long blocks = std::min<long long>(L.S, (long long)di.cdl_per_sm * di.sms);
+    const long long blocks = beside ? (long long)L.S : std::min<long long>(L.S, (long long)di.cdl_per_sm * di.sms);
     cdl::tile_kernel<<<(int)std::max<long long>(1, blocks), cdl::kTileBars, 0, stream>>>(A);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -741,11 +779,21 @@ cudaError_t launch_batch(Launch& L, const SchedulePlan& plan, long long total_ba
   }
   L.njobs -= ncdl;
   if (ncdl > 0) {
-    if (L.njobs > 0) {
-      const cudaError_t e = launch_batch(L, plan, total_bars, stream, stats);
-      if (e != cudaSuccess) return e;
-    }
-    return launch_candles(L, cdl_jobs, ncdl, stream);
+    if (L.njobs == 0) return launch_candles(L, cdl_jobs, ncdl, stream);
+    SideStream* ss = nullptr;
+    cudaError_t e = side_stream(&ss);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(ss->m);
+    e = cudaEventRecord(ss->fork, stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ss->s, ss->fork, 0);
+    if (e != cudaSuccess) return e;
+    e = launch_batch(L, plan, total_bars, stream, stats);
+    const cudaError_t ec = launch_candles(L, cdl_jobs, ncdl, ss->s, true);
+    // the join is enqueued whatever happened, so the side stream never
+    // outlives the caller's stream (or an open capture) unjoined
+    cudaError_t ej = cudaEventRecord(ss->join, ss->s);
+    if (ej == cudaSuccess) ej = cudaStreamWaitEvent(stream, ss->join, 0);
+    return e != cudaSuccess ? e : (ec != cudaSuccess ? ec : ej);
   }
   L.lb = 0;
   // row-parallel engine; job sets it does not take (or whose layout does not
