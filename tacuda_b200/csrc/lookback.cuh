@@ -33,7 +33,9 @@ constexpr int kLbGroup = 32;
 constexpr int kLbSpan = 1024;  // 32 groups
 
 constexpr int kLbAgg = 1, kLbInc = 2;
-constexpr long long kLbSpinLimit = 1ll << 26;  // polls / 32 at up to 1 us each: about two seconds
+// polls / 32 = 2^21 polls, each a sleep of at most 256 ns plus an L2 round
+// trip: one to two seconds
+constexpr long long kLbSpinLimit = 1ll << 26;
 
 // The polls a wait makes before giving up: err[1] when the host set it (a test
 // that makes a wait run out), else kLbSpinLimit / 32.
@@ -42,29 +44,39 @@ __device__ __forceinline__ long long lb_spin_limit(const int* err) {
   return v > 0 ? (long long)v : (kLbSpinLimit >> 5);
 }
 
-__device__ __forceinline__ int lb_load_flag(const LbDesc* d) {
-  return *reinterpret_cast<const volatile int*>(&d->flag);
+// Flags are published with release stores and polled with acquire loads
+// (GPU scope): the descriptor fields a tile writes before its flag are visible
+// to every thread that reads the flag set, with no separate fence on either
+// side (a full fence per wait and per publish had cost a quarter of the issue
+// slots of a 100,000-bar row in membar stalls). Every publish and every read
+// of the fields behind a flag is done by one thread, the one that stored or
+// acquired that flag.
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.b32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
 }
 
-__device__ __forceinline__ void lb_store_flag(LbDesc* d, int v) {
-  __threadfence();
-  *reinterpret_cast<volatile int*>(&d->flag) = v;
-}
+__device__ __forceinline__ int lb_load_flag(const LbDesc* d) { return ld_acquire(&d->flag); }
+
+__device__ __forceinline__ void lb_store_flag(LbDesc* d, int v) { st_release(&d->flag, v); }
 
 // Wait (bounded) until flag >= want; returns the flag or 0 on timeout.
 __device__ __forceinline__ int lb_wait_on(const int* flag, int want, int* err) {
   long long spins = 0;
   unsigned ns = 32;
   int v;
-  while ((v = *reinterpret_cast<const volatile int*>(flag)) < want) {
+  while ((v = ld_acquire(flag)) < want) {
     if (++spins > lb_spin_limit(err)) {
       atomicExch(err, 1);
       return 0;
     }
     __nanosleep(ns);
-    if (ns < 1024) ns <<= 1;
+    if (ns < 256) ns <<= 1;
   }
-  __threadfence();
   return v;
 }
 
@@ -75,16 +87,15 @@ __device__ __forceinline__ bool lb_wait_all(const int* flag, int want, bool acti
   long long spins = 0;
   unsigned ns = 32;
   for (;;) {
-    const bool ok = !active || *reinterpret_cast<const volatile int*>(flag) >= want;
+    const bool ok = !active || ld_acquire(flag) >= want;
     if (__all_sync(kFull, ok)) break;
     if (++spins > lb_spin_limit(err)) {
       if (active) atomicExch(err, 1);
       return false;
     }
     __nanosleep(ns);
-    if (ns < 1024) ns <<= 1;
+    if (ns < 256) ns <<= 1;
   }
-  __threadfence();
   return true;
 }
 
@@ -98,9 +109,8 @@ __device__ __forceinline__ int lb_wait(const LbDesc* d, int want, int* err) {
       return 0;
     }
     __nanosleep(ns);
-    if (ns < 1024) ns <<= 1;
+    if (ns < 256) ns <<= 1;
   }
-  __threadfence();
   return v;
 }
 
@@ -170,8 +180,7 @@ __device__ __forceinline__ int lb_first_index(LbDesc* base, long long stride, in
     v = earliest(v >= 0 ? v : kNone);
     if (lane == 0) {
       me->gf = v == kNone ? -1 : v;
-      __threadfence();
-      *reinterpret_cast<volatile int*>(&me->gflag) = 1;
+      st_release(&me->gflag, 1);
     }
   }
   // common case first: tile 0 (resolved at once) already holds the index
@@ -294,8 +303,7 @@ __device__ __forceinline__ void lb_resolve(LbDesc* base, long long stride, int t
     if (lane == 0) {
 #pragma unroll
       for (int ch = 0; ch < NC; ++ch) { me->GA[ch] = a[ch]; me->GB[ch] = b[ch]; }
-      __threadfence();
-      *reinterpret_cast<volatile int*>(&me->gflag) = 1;
+      st_release(&me->gflag, 1);
     }
   }
   const int ckpt = ((tile - 1) / kLbSpan) * kLbSpan;
