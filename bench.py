@@ -305,10 +305,25 @@ def run_extras(dev, peak):
           tb.make_job("macd", (12, 26, 9), (), [o1[k].data_ptr() for k in ("macd", "sig", "hist")])]
     s1 = tb.make_series({"close": x.data_ptr()}, 1, x.shape[1])
     st = torch.cuda.current_stream().cuda_stream
-    f_ms = _event_ms(lambda: tb.fused_batch_d(s1, j1, st), 20)
-    p_ms = _event_ms(lambda: [tb.fused_batch_d(s1, [j], st) for j in j1], 20)
+    # the synchronous call (stream 0: returns when done, as the reference's
+    # stream-0 calls do), then the same launch replayed from a CUDA graph on a
+    # user stream (device time, no host work between steps)
+    sync_ms = _event_ms(lambda: tb.fused_batch_d(s1, j1, 0), 20)
+    p_ms = _event_ms(lambda: [tb.fused_batch_d(s1, [j], 0) for j in j1], 20)
+    side = torch.cuda.Stream(device=dev)
+    with torch.cuda.stream(side):
+        tb.fused_batch_d(s1, j1, side.cuda_stream)
+        torch.cuda.synchronize()
+        g1 = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g1, stream=side):
+            tb.fused_batch_d(s1, j1, torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        f_ms = _event_ms(lambda: g1.replay(), 20)
+    del g1
     out["single_series_100k"] = {"workload": "1 series x 100,000 bars: SMA20 EMA30 RSI14 MACD12/26/9 (6 outputs)",
-                                  "fused_us": f_ms * 1e3, "plain_us": p_ms * 1e3,
+                                  "fused_us": f_ms * 1e3, "fused_path": "one fused launch replayed from a CUDA graph",
+                                  "sync_call_us": sync_ms * 1e3, "plain_us": p_ms * 1e3,
+                                  "plain_path": "four synchronous single-job calls on stream 0",
                                   "value": 4 * 100_000 / (f_ms * 1e-3), "unit": "indicator-bars/s",
                                   "bound": "latency"}
     del x, o1

@@ -556,14 +556,15 @@ int partition_nonempty(const Launch& L, int P, int* part) {
 bool plan_split(const Launch& L, int parts, int groups, int smem_optin, Split& sp) {
   if (const char* v = std::getenv("TACUDA_B200_ROWS_PARTS")) parts = std::atoi(v);
   if (const char* v = std::getenv("TACUDA_B200_ROWS_GROUPS")) groups = std::atoi(v);
-  // Defaults: a job set of five or more jobs is split into five partitions,
+  // Defaults: a job set of five or more jobs is split into four partitions,
   // each CTA running up to two row groups (13-indicator pass, 4000 x 234:
-  // 210 -> 145-155 us; the same jobs over 10,000 ragged rows: 11.3-12.6 ->
-  // 8.2 ms). A CTA then holds the code of a few families instead of all of
-  // them (instruction-cache hit rate 59 -> 90 %), and each SM works on 64 rows
-  // of a partition instead of 32 rows of everything. More partitions or more
-  // groups per CTA measured within noise of this; the autotuner tries 4-6.
-  if (parts <= 0) parts = L.njobs >= 5 ? 5 : 1;
+  // 210 -> 124-150 us; the same jobs over 10,000 ragged rows: 11.3-12.6 ->
+  // 8.4 ms). A CTA then holds the code of a few families instead of all of
+  // them (instruction-cache hit rate 59 -> 86 %), and each SM works on 64 rows
+  // of a partition instead of 32 rows of everything. Five or six partitions,
+  // or more groups per CTA, measured within a few percent of this (six were
+  // best on the ragged rows, 7.7 ms); the autotuner tries 4-6.
+  if (parts <= 0) parts = L.njobs >= 5 ? 4 : 1;
   if (groups <= 0) groups = parts > 1 ? 2 : 1;
   int P = std::max(1, std::min({parts, L.njobs, kMaxParts}));
   const long long ngroups = ((long long)L.S + 31) / 32;
@@ -576,7 +577,10 @@ bool plan_split(const Launch& L, int parts, int groups, int smem_optin, Split& s
   int dmax = 4, dmin = 2;
   if (const char* v = std::getenv("TACUDA_B200_ROWS_DEPTH")) dmax = dmin = std::max(2, std::min(4, std::atoi(v)));
   // per partition, the largest G <= Gmax that fits: job warps within the
-  // CTA's warp budget and G groups within the shared memory
+  // CTA's warp budget and G groups within the shared memory. (Fewer groups
+  // with larger teams of chained window jobs measured slower: the 13-indicator
+  // pass with the MFI/STOCH/WILLR partition at one group and teams of three
+  // or four took 195-200 us against 145-155 us.)
   for (int q = 0; q < P; ++q) {
     int jl[kMaxJobs], nj = 0;
     for (int j = 0; j < L.njobs; ++j)
@@ -590,7 +594,7 @@ bool plan_split(const Launch& L, int parts, int groups, int smem_optin, Split& s
       if (ok) break;
     }
     sp.G[q] = G;
-    sp.cta0[q + 1] = sp.cta0[q] + (int)((ngroups + G - 1) / G);
+    sp.cta0[q + 1] = sp.cta0[q] + (int)((ngroups + sp.G[q] - 1) / sp.G[q]);
   }
   return true;
 }
