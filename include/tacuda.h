@@ -84,6 +84,8 @@ CTAPI_EXPORT ctStatus_t ct_rma_batch_d(const float *d_inputs, float *d_outputs, 
 CTAPI_EXPORT ctStatus_t ct_typprice_batch_d(const float *d_highs, const float *d_lows, const float *d_closes, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1300 */
 CTAPI_EXPORT ctStatus_t ct_medprice_batch_d(const float *d_highs, const float *d_lows, float *d_outputs, int seriesLen, int numSeries, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1339 */
 CTAPI_EXPORT ctStatus_t ct_midprice_batch_d(const float *d_highs, const float *d_lows, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1727 */
+CTAPI_EXPORT ctStatus_t ct_aroon_batch_d(const float *d_highs, const float *d_lows, float *d_aroon_downs, float *d_aroon_ups, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1363 */
+CTAPI_EXPORT ctStatus_t ct_aroonosc_batch_d(const float *d_highs, const float *d_lows, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1350 */
 CTAPI_EXPORT ctStatus_t ct_rocp_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1016 */
 CTAPI_EXPORT ctStatus_t ct_rocr_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1026 */
 CTAPI_EXPORT ctStatus_t ct_rocr100_batch_d(const float *d_inputs, float *d_outputs, int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream); /* tacuda.h:1036 */
@@ -198,6 +200,8 @@ CTAPI_EXPORT ctStatus_t ct_roc_d(const float* d_input, float* d_output, int size
 CTAPI_EXPORT ctStatus_t ct_medprice_d(const float* d_high, const float* d_low, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:342 */
 CTAPI_EXPORT ctStatus_t ct_typprice_d(const float* d_high, const float* d_low, const float* d_close, float* d_output, int size, cudaStream_t stream); /* tacuda_device.h:345 */
 CTAPI_EXPORT ctStatus_t ct_midprice_d(const float* d_high, const float* d_low, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:511 */
+CTAPI_EXPORT ctStatus_t ct_aroon_d(const float* d_high, const float* d_low, float* d_aroonDown, float* d_aroonUp, int size, int period, cudaStream_t stream); /* tacuda_device.h:376 */
+CTAPI_EXPORT ctStatus_t ct_aroonosc_d(const float* d_high, const float* d_low, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:380 */
 CTAPI_EXPORT ctStatus_t ct_rma_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:1212 */
 CTAPI_EXPORT ctStatus_t ct_rocp_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:177 */
 CTAPI_EXPORT ctStatus_t ct_rocr_d(const float* d_input, float* d_output, int size, int period, cudaStream_t stream); /* tacuda_device.h:180 */
@@ -341,7 +345,7 @@ typedef enum ctB200Family {
   CT_B200_ROC, CT_B200_RMA, CT_B200_MEDPRICE, CT_B200_TYPPRICE, CT_B200_MIDPRICE,
   CT_B200_ROCP, CT_B200_ROCR, CT_B200_ROCR100, CT_B200_MOM, CT_B200_AVGPRICE, CT_B200_WCLPRICE,
   CT_B200_MIDPOINT, CT_B200_ROLLING_MEAN, CT_B200_ROLLING_MAX, CT_B200_ROLLING_MIN, CT_B200_ROLLING_STD,
-  CT_B200_IBS, CT_B200_MARKETFI, CT_B200_QSTICK
+  CT_B200_IBS, CT_B200_MARKETFI, CT_B200_QSTICK, CT_B200_AROON, CT_B200_AROONOSC
 } ctB200Family_t;
 
 /* Input planes of a batch. */

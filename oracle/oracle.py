@@ -70,6 +70,8 @@ FAMILIES = {
     "ibs": (44, ("high", "low", "close"), ("out",), (), ()),
     "marketfi": (45, ("high", "low", "volume"), ("out",), (), ()),
     "qstick": (46, ("open", "close"), ("out",), ("period",), ()),
+    "aroon": (47, ("high", "low"), ("down", "up"), ("period",), ()),
+    "aroonosc": (48, ("high", "low"), ("out",), ("period",), ()),
 }
 
 _P = ct.c_void_p

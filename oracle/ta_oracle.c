@@ -877,6 +877,37 @@ static void row_midprice(RowCtx* r) {
   }
 }
 
+/* src/indicators/Aroon.cu:11-52 and src/indicators/AroonOscillator.cu:12-40:
+ * from bar t back over p bars, strict comparisons seeded with bar t itself
+ * (ties keep the most recent bar, NaNs never win, a NaN at t keeps t), each
+ * line 100.0f * (p - since) / (float)p in float, from bar p; the oscillator
+ * is up - down in float. Outputs: AROON down then up. */
+static float aroon_line_f(int p, int since) { return 100.0f * (float)(p - since) / (float)p; }
+
+static void aroon_row(RowCtx* r, int osc) {
+  const float* h = r->in[0]; const float* l = r->in[1];
+  int n = r->n, p = r->ip[0];
+  fill_nan(r->out[0], n);
+  if (!osc) fill_nan(r->out[1], n);
+  for (int t = p; t < n; ++t) {
+    float mx = h[t], mn = l[t];
+    int sh = 0, sl = 0;
+    for (int d = 1; d <= p; ++d) {
+      if (h[t - d] > mx) { mx = h[t - d]; sh = d; }
+      if (l[t - d] < mn) { mn = l[t - d]; sl = d; }
+    }
+    const float up = aroon_line_f(p, sh), dn = aroon_line_f(p, sl);
+    if (osc) {
+      r->out[0][t] = (double)(up - dn);
+    } else {
+      r->out[0][t] = (double)dn;
+      r->out[1][t] = (double)up;
+    }
+  }
+}
+static void row_aroon(RowCtx* r) { aroon_row(r, 0); }
+static void row_aroonosc(RowCtx* r) { aroon_row(r, 1); }
+
 /* --------------------------------------------------------------- dispatch */
 
 typedef struct { int nin, nout, nip, nfp; void (*fn)(RowCtx*); int minp; } FamSpec;
@@ -910,6 +941,7 @@ static const FamSpec kFam[ORC_FAMILY_COUNT] = {
   [ORC_RMIN] = {1, 1, 1, 0, row_rmin, 1},    [ORC_RSTD] = {1, 1, 1, 0, row_rstd, 1},
   [ORC_IBS] = {3, 1, 0, 0, row_ibs, 0},      [ORC_MARKETFI] = {3, 1, 0, 0, row_marketfi, 0},
   [ORC_QSTICK] = {2, 1, 1, 0, row_qstick, 1},
+  [ORC_AROON] = {2, 2, 1, 0, row_aroon, 1},  [ORC_AROONOSC] = {2, 1, 1, 0, row_aroonosc, 1},
 };
 
 static int check_params(int family, const int* ip) {

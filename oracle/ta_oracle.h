@@ -38,7 +38,7 @@ enum OracleFamily {
   ORC_CORREL, ORC_DEMA, ORC_TEMA, ORC_T3, ORC_ROC, ORC_RMA, ORC_MEDPRICE,
   ORC_TYPPRICE, ORC_MIDPRICE, ORC_ROCP, ORC_ROCR, ORC_ROCR100, ORC_MOM,
   ORC_AVGPRICE, ORC_WCLPRICE, ORC_MIDPOINT, ORC_RMEAN, ORC_RMAX, ORC_RMIN,
-  ORC_RSTD, ORC_IBS, ORC_MARKETFI, ORC_QSTICK, ORC_FAMILY_COUNT
+  ORC_RSTD, ORC_IBS, ORC_MARKETFI, ORC_QSTICK, ORC_AROON, ORC_AROONOSC, ORC_FAMILY_COUNT
 };
 
 /* ins: the family's input planes (see oracle/oracle.py INPUTS); outs: its output

@@ -36,11 +36,12 @@ FAMILIES = ("sma", "ema", "wma", "rsi", "macd", "atr", "natr", "trange", "adx", 
             "cci", "obv", "ad", "adosc", "mfi", "willr", "sum", "min", "max", "stddev", "var", "linearreg",
             "correl", "dema", "tema", "t3", "cdl", "roc", "rma", "medprice", "typprice", "midprice",
             "rocp", "rocr", "rocr100", "momentum", "avgprice", "wclprice", "midpoint",
-            "rolling_mean", "rolling_max", "rolling_min", "rolling_std", "ibs", "marketfi", "qstick")
+            "rolling_mean", "rolling_max", "rolling_min", "rolling_std", "ibs", "marketfi", "qstick",
+            "aroon", "aroonosc")
 FAMILY_ID = {n: i for i, n in enumerate(FAMILIES)}
 PLANES = ("open", "high", "low", "close", "volume", "aux")
 PLANE_ID = {n: i for i, n in enumerate(PLANES)}
-OUTPUTS = {"macd": 3, "bbands": 3, "stoch": 2}
+OUTPUTS = {"macd": 3, "bbands": 3, "stoch": 2, "aroon": 2}
 
 _P = ct.c_void_p
 _I = ct.c_int

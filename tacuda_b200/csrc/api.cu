@@ -59,7 +59,8 @@ int default_inputs(int family, int* in) {
       in[0] = tb::P_HIGH; in[1] = tb::P_LOW; in[2] = tb::P_CLOSE; return 3;
     case tb::F_MARKETFI: in[0] = tb::P_HIGH; in[1] = tb::P_LOW; in[2] = tb::P_VOLUME; return 3;
     case tb::F_QSTICK: in[0] = tb::P_OPEN; in[1] = tb::P_CLOSE; return 2;
-    case tb::F_MEDPRICE: case tb::F_MIDPRICE: in[0] = tb::P_HIGH; in[1] = tb::P_LOW; return 2;
+    case tb::F_MEDPRICE: case tb::F_MIDPRICE: case tb::F_AROON: case tb::F_AROONOSC:
+      in[0] = tb::P_HIGH; in[1] = tb::P_LOW; return 2;
     case tb::F_AD: case tb::F_ADOSC: case tb::F_MFI:
       in[0] = tb::P_HIGH; in[1] = tb::P_LOW; in[2] = tb::P_CLOSE; in[3] = tb::P_VOLUME; return 4;
     case tb::F_OBV: in[0] = tb::P_CLOSE; in[1] = tb::P_VOLUME; return 2;
@@ -73,7 +74,7 @@ int default_inputs(int family, int* in) {
 int output_count(int family) {
   switch (family) {
     case tb::F_MACD: case tb::F_BBANDS: return 3;
-    case tb::F_STOCH: return 2;
+    case tb::F_STOCH: case tb::F_AROON: return 2;
     default: return 1;
   }
 }
@@ -105,7 +106,7 @@ ctStatus_t make_job(const ctB200Job& u, Job& j, const char* who) {
     case tb::F_LINEARREG: case tb::F_MIN: case tb::F_MAX: case tb::F_WILLR: case tb::F_CCI: case tb::F_MFI:
     case tb::F_CORREL: case tb::F_ROC: case tb::F_MIDPRICE: case tb::F_ROCP: case tb::F_ROCR: case tb::F_ROCR100:
     case tb::F_MOM: case tb::F_MIDPOINT: case tb::F_RMEAN: case tb::F_RMAX: case tb::F_RMIN: case tb::F_RSTD:
-    case tb::F_QSTICK:
+    case tb::F_QSTICK: case tb::F_AROON: case tb::F_AROONOSC:
       if (u.params[0] > kMaxWindow) return fail(CT_STATUS_UNSUPPORTED, std::string(who) + ": window period above 4096");
       break;
     case tb::F_STOCH:
@@ -755,6 +756,51 @@ ctStatus_t ct_midprice_d(const float* d_high, const float* d_low, float* d_outpu
   Planes P;
   P.p[tb::P_HIGH] = d_high; P.p[tb::P_LOW] = d_low;
   return run_single(P.p, u, size, 1, stream, "ct_midprice_d");
+}
+
+// AROON (src/indicators/Aroon.cu:11-52 via api_device.cu:1467-1484): outputs in
+// the reference's order, aroon down then aroon up. The reference's ct_aroon_d
+// turns every exception, an invalid period included, into
+// CT_STATUS_KERNEL_FAILED (api_device.cu:1482-1483); so does this entry.
+static ctStatus_t aroon_bad_period(const char* who) {
+  clear_error();
+  return fail(CT_STATUS_KERNEL_FAILED, std::string(who) + ": invalid period");
+}
+ctStatus_t ct_aroon_batch_d(const float* d_highs, const float* d_lows, float* d_aroon_downs, float* d_aroon_ups,
+                            int seriesLen, int numSeries, int period, int maxConcurrency, cudaStream_t stream) {
+  (void)maxConcurrency;
+  if (period < 1 && d_highs && d_lows && d_aroon_downs && d_aroon_ups && seriesLen > 0 && numSeries > 0)
+    return aroon_bad_period("ct_aroon_batch_d");
+  ctB200Job u = job_of(tb::F_AROON, period);
+  u.outputs[0] = d_aroon_downs;
+  u.outputs[1] = d_aroon_ups;
+  const Planes P = hlc(d_highs, d_lows, nullptr);
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_aroon_batch_d");
+}
+ctStatus_t ct_aroon_d(const float* d_high, const float* d_low, float* d_aroonDown, float* d_aroonUp, int size,
+                      int period, cudaStream_t stream) {
+  if (period < 1 && d_high && d_low && d_aroonDown && d_aroonUp && size > 0) return aroon_bad_period("ct_aroon_d");
+  ctB200Job u = job_of(tb::F_AROON, period);
+  u.outputs[0] = d_aroonDown;
+  u.outputs[1] = d_aroonUp;
+  const Planes P = hlc(d_high, d_low, nullptr);
+  return run_single(P.p, u, size, 1, stream, "ct_aroon_d");
+}
+// AROONOSC (src/indicators/AroonOscillator.cu:12-40 via api_device.cu:1486-1496).
+ctStatus_t ct_aroonosc_batch_d(const float* d_highs, const float* d_lows, float* d_outputs, int seriesLen,
+                               int numSeries, int period, int maxConcurrency, cudaStream_t stream) {
+  (void)maxConcurrency;
+  ctB200Job u = job_of(tb::F_AROONOSC, period);
+  u.outputs[0] = d_outputs;
+  const Planes P = hlc(d_highs, d_lows, nullptr);
+  return run_single(P.p, u, seriesLen, numSeries, stream, "ct_aroonosc_batch_d");
+}
+ctStatus_t ct_aroonosc_d(const float* d_high, const float* d_low, float* d_output, int size, int period,
+                         cudaStream_t stream) {
+  ctB200Job u = job_of(tb::F_AROONOSC, period);
+  u.outputs[0] = d_output;
+  const Planes P = hlc(d_high, d_low, nullptr);
+  return run_single(P.p, u, size, 1, stream, "ct_aroonosc_d");
 }
 
 // ------------------------------------------------------------ candles

@@ -100,4 +100,8 @@ __host__ __device__ inline void talib_ema_coeffs(int p, double& beta, double& k)
   k = kk;
 }
 
+// One AROON line as the reference's kernels round it (src/indicators/Aroon.cu:
+// 37, 49): 100.0f times the bars left in the window, divided by the period.
+__device__ __forceinline__ float aroon_line(int p, int since) { return 100.0f * (float)(p - since) / (float)p; }
+
 }  // namespace tb

@@ -90,6 +90,8 @@ __device__ __forceinline__ void run_job_ext(const Ctx<K>& c, const Job& j, Carry
     case F_IBS: talib_bar_round(c, j, cy, 0); break;
     case F_MARKETFI: talib_bar_round(c, j, cy, 1); break;
     case F_QSTICK: qstick_round(c, j, cy); break;
+    case F_AROON: aroon_round(c, j, 0); break;
+    case F_AROONOSC: aroon_round(c, j, 1); break;
     default: break;
   }
 }

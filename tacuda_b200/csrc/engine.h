@@ -16,6 +16,7 @@ enum Family : int {
   F_MAX, F_STDDEV, F_VAR, F_LINEARREG, F_CORREL, F_DEMA, F_TEMA, F_T3, F_CDL,
   F_ROC, F_RMA, F_MEDPRICE, F_TYPPRICE, F_MIDPRICE, F_ROCP, F_ROCR, F_ROCR100, F_MOM,
   F_AVGPRICE, F_WCLPRICE, F_MIDPOINT, F_RMEAN, F_RMAX, F_RMIN, F_RSTD, F_IBS, F_MARKETFI, F_QSTICK,
+  F_AROON, F_AROONOSC,
   F_COUNT
 };
 

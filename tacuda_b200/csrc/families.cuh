@@ -1052,6 +1052,44 @@ __device__ __forceinline__ void midprice_round(const Ctx<K>& c, const Job& j) {
   c.flush(0, (float*)j.out[0]);
 }
 
+// AROON / AROONOSC(p) as the reference's float kernels compute them
+// (src/indicators/Aroon.cu:11-52, src/indicators/AroonOscillator.cu:12-40):
+// from bar t back over p bars, the latest bar holding the window's highest
+// high (lowest low), found with strict comparisons seeded with bar t itself
+// (so ties keep the most recent bar and NaNs are skipped, a NaN at bar t
+// keeping t); up = 100.0f * (p - since) / (float)p, down alike, osc = up -
+// down, from bar p. mode 0: AROON (out[0] down, out[1] up); 1: AROONOSC.
+
+template <int K>
+__device__ __forceinline__ void aroon_round(const Ctx<K>& c, const Job& j, int mode) {
+  const int ph = j.in[0], plo = j.in[1], p = j.ip[0];
+  const int g0 = c.gb0();
+  for (int k = 0; k < K; ++k) {
+    const int t = g0 + k;
+    if (!c.valid(t)) break;
+    float up = qnan(), dn = qnan();
+    if (t >= p) {
+      float mx = c.x(ph, t), mn = c.x(plo, t);
+      int sh = 0, sl = 0;
+      for (int d = 1; d <= p; ++d) {
+        const float h = c.x(ph, t - d), l = c.x(plo, t - d);
+        if (h > mx) { mx = h; sh = d; }
+        if (l < mn) { mn = l; sl = d; }
+      }
+      up = aroon_line(p, sh);
+      dn = aroon_line(p, sl);
+    }
+    if (mode == 0) {
+      c.put(0, k, dn);
+      c.put(1, k, up);
+    } else {
+      c.put(0, k, t >= p ? up - dn : qnan());
+    }
+  }
+  c.flush(0, (float*)j.out[0]);
+  if (mode == 0) c.flush(1, (float*)j.out[1]);
+}
+
 // MIDPOINT(p): src/indicators/MIDPOINT.cu:13-35: fmaxf / fminf over the
 // window of one plane, 0.5f * (max + min) from bar p-1; a window starting in
 // the row's leading NaN run stays NaN (LeadingNaN.cuh:22-28, as MIN/MAX).

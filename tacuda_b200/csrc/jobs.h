@@ -36,6 +36,7 @@ inline int job_halo(const Job& j) {
     case F_MFI: case F_ROC: case F_ROCP: case F_ROCR: case F_ROCR100: case F_MOM: return j.ip[0];
     case F_MIDPOINT: case F_RMEAN: case F_RMAX: case F_RMIN: case F_RSTD: case F_QSTICK: return j.ip[0] - 1;
     case F_MIDPRICE: return j.ip[0] - 1;
+    case F_AROON: case F_AROONOSC: return j.ip[0];
     case F_STOCH: return j.ip[0] - 1 + 2 * (j.ip[1] - 1);
     case F_CDL: return 16;  // 10-bar averages anchored up to 5 bars back
     default: return 1;  // previous bar
@@ -51,7 +52,8 @@ inline unsigned job_planes(const Job& j) {
     case F_TEMA: case F_T3: case F_ROC: case F_RMA: case F_ROCP: case F_ROCR: case F_ROCR100:
     case F_MOM: case F_MIDPOINT: case F_RMEAN: case F_RMAX: case F_RMIN: case F_RSTD:
       n = 1; break;
-    case F_OBV: case F_CORREL: case F_MEDPRICE: case F_MIDPRICE: case F_QSTICK: n = 2; break;
+    case F_OBV: case F_CORREL: case F_MEDPRICE: case F_MIDPRICE: case F_QSTICK: case F_AROON: case F_AROONOSC:
+      n = 2; break;
     case F_ATR: case F_NATR: case F_TRANGE: case F_ADX: case F_DX: case F_STOCH: case F_WILLR:
     case F_TYPPRICE: case F_WCLPRICE: case F_IBS: case F_MARKETFI:
       n = 3; break;

@@ -65,7 +65,7 @@ __host__ __device__ inline int line_bytes(const Job& j, unsigned long long bp) {
 }
 
 __host__ __device__ inline int out_count(int family) {
-  return family == F_MACD || family == F_BBANDS ? 3 : (family == F_STOCH ? 2 : 1);
+  return family == F_MACD || family == F_BBANDS ? 3 : (family == F_STOCH || family == F_AROON ? 2 : 1);
 }
 
 // Families of the core kernel: the indicators of the reference's fused batch
@@ -154,6 +154,8 @@ __device__ void run_job(const Warp& w, const Job& j, unsigned char* line) {
           case F_IBS: w_talib_bar(w, j, 0); return;
           case F_MARKETFI: w_talib_bar(w, j, 1); return;
           case F_QSTICK: w_qstick(w, j); return;
+          case F_AROON: w_aroon(w, j, 0); return;
+          case F_AROONOSC: w_aroon(w, j, 1); return;
           default: break;
         }
       }
@@ -309,7 +311,7 @@ bool family_supported(int f) {
     case F_T3: case F_LINEARREG: case F_CORREL: case F_MIN: case F_MAX: case F_MIDPOINT: case F_ROC:
     case F_ROCP: case F_ROCR: case F_ROCR100: case F_MOM: case F_MEDPRICE: case F_TYPPRICE: case F_AVGPRICE:
     case F_WCLPRICE: case F_MIDPRICE: case F_RMEAN: case F_RMAX: case F_RMIN: case F_RSTD: case F_IBS:
-    case F_MARKETFI: case F_QSTICK:
+    case F_MARKETFI: case F_QSTICK: case F_AROON: case F_AROONOSC:
       return true;
     default:
       return false;

@@ -1595,5 +1595,41 @@ __device__ void w_qstick(const Warp& w, const Job& j) {
   }
 }
 
+// AROON / AROONOSC (aroon_round in families.cuh): each bar scans its window
+// back from itself with strict comparisons, as the reference's kernels do.
+__device__ void w_aroon(const Warp& w, const Job& j, int mode) {
+  const int ph = j.in[0], plo = j.in[1], p = j.ip[0];
+  for (int c = 0; c < w.nchunks; ++c) {
+    if (!w.wait(c)) return;
+    const float* H = w.X(c, ph);
+    const float* Lo = w.X(c, plo);
+    const int t0 = c * C, lim = w.lim(c);
+    for (int r = 0; r < lim; ++r) {
+      const int t = t0 + r;
+      float up = qnan(), dn = qnan();
+      if (t >= p) {
+        float mx = H[r], mn = Lo[r];
+        int sh = 0, sl = 0;
+        for (int d = 1; d <= p; ++d) {
+          const float h = H[r - d], l = Lo[r - d];
+          if (h > mx) { mx = h; sh = d; }
+          if (l < mn) { mn = l; sl = d; }
+        }
+        up = aroon_line(p, sh);
+        dn = aroon_line(p, sl);
+      }
+      if (mode == 0) {
+        w.put(0, r, dn);
+        w.put(1, r, up);
+      } else {
+        w.put(0, r, t >= p ? up - dn : qnan());
+      }
+    }
+    w.flush(0, (float*)j.out[0], c);
+    if (mode == 0) w.flush(1, (float*)j.out[1], c);
+    w.release(c);
+  }
+}
+
 }  // namespace rows
 }  // namespace tb

@@ -61,6 +61,8 @@ SPECS = {
     "ibs": ("ct_ibs_batch_d", HLC, 1, []),
     "marketfi": ("ct_marketfi_batch_d", ["high", "low", "volume"], 1, []),
     "qstick": ("ct_qstick_batch_d", ["open", "close"], 1, [("i", "period")]),
+    "aroon": ("ct_aroon_batch_d", ["high", "low"], 2, [("i", "period")]),
+    "aroonosc": ("ct_aroonosc_batch_d", ["high", "low"], 1, [("i", "period")]),
 }
 
 DEFAULTS = {
@@ -76,6 +78,7 @@ DEFAULTS = {
     "avgprice": {}, "wclprice": {}, "midpoint": dict(period=14), "change": dict(period=10),
     "rolling_mean": dict(period=20), "rolling_max": dict(period=20), "rolling_min": dict(period=20),
     "rolling_std": dict(period=20), "ibs": {}, "marketfi": {}, "qstick": dict(period=10),
+    "aroon": dict(period=14), "aroonosc": dict(period=14),
 }
 
 

@@ -84,6 +84,10 @@ def test_appended_families_validate_like_the_reference():
         assert getattr(lib, f"ct_{name}_batch_d")(fake, fake, I(10), I(2), I(0), I(0), P(0)) == 4, name
         assert "invalid period" in tb.get_last_error()
     assert lib.ct_midprice_batch_d(fake, fake, fake, I(10), I(2), I(-3), I(0), P(0)) == 4
+    # Aroon.cu throws on period <= 0; the reference's ct_aroon_d turns every
+    # exception into KERNEL_FAILED, its ct_aroonosc_d classifies it as invalid
+    assert lib.ct_aroon_batch_d(fake, fake, fake, fake, I(10), I(2), I(0), I(0), P(0)) == 3
+    assert lib.ct_aroonosc_batch_d(fake, fake, fake, I(10), I(2), I(0), I(0), P(0)) == 4
     # TA_RMA's period range ends at 100000
     assert lib.ct_rma_batch_d(fake, fake, I(10), I(2), I(100001), I(0), P(0)) == 4
     # staged windows end at 4096 bars

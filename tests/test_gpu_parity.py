@@ -90,6 +90,8 @@ VARIANTS = {
     "midpoint": [dict(period=1), dict(period=2), dict(period=40)],
     "momentum": [dict(period=1), dict(period=250)],
     "qstick": [dict(period=1), dict(period=2), dict(period=64)],
+    "aroon": [dict(period=1), dict(period=2), dict(period=25), dict(period=90)],
+    "aroonosc": [dict(period=1), dict(period=14), dict(period=90)],
 }
 
 
@@ -432,6 +434,31 @@ def test_float_kernel_families_bit_exact(name, mode):
         np.testing.assert_array_equal(np.isnan(got), np.isnan(ref), err_msg=f"{name}{p}")
         m = ~np.isnan(ref)
         np.testing.assert_array_equal(got[m].view(np.uint32), ref[m].view(np.uint32), err_msg=f"{name}{p}")
+
+
+@pytest.mark.parametrize("name", ["aroon", "aroonosc"])
+def test_aroon_bit_exact(name, mode):
+    """AROON and AROONOSC repeat the reference kernels' float arithmetic
+    (src/indicators/Aroon.cu, AroonOscillator.cu), so every output word equals
+    the oracle's float result, with ties (flat highs and lows, where the most
+    recent bar wins), NaN and infinite bars, and a NaN at the current bar."""
+    d = synthetic.ohlcv(8, 1500, seed=43)
+    d["high"][1, 100:160] = 105.0
+    d["low"][1, 100:160] = 95.0
+    d["high"][2, 300:310] = np.nan
+    d["low"][3, 500] = np.nan
+    d["high"][4, 700] = np.inf
+    d["low"][5, 800] = -np.inf
+    d["high"][6, :] = np.nan
+    dp = device_planes(d)
+    for p in (1, 7, 14, 40, 100):
+        got = to_np(call_batch_d(name, dp, dict(period=p)))
+        ref = O.run(name, d, period=p)
+        for i, (g, r) in enumerate(zip(got, ref)):
+            r = r.astype(np.float32)
+            np.testing.assert_array_equal(np.isnan(g), np.isnan(r), err_msg=f"{name}[{i}] p={p}")
+            m = ~np.isnan(r)
+            np.testing.assert_array_equal(g[m].view(np.uint32), r[m].view(np.uint32), err_msg=f"{name}[{i}] p={p}")
 
 
 def test_rma_period_one_propagates_nan(mode):

@@ -94,6 +94,35 @@ def test_qstick_infinite_difference_matches_reference_build():
             row_atol=1e-9)
 
 
+def test_aroon_known_answers():
+    """src/indicators/Aroon.cu: rising highs put the high at the current bar
+    (up = 100), falling lows the low there too (down = 100); flat windows tie
+    and the most recent bar wins (100); the oscillator is up - down; warm-up
+    NaN for the first p bars."""
+    T, p = 40, 10
+    h = np.arange(T, dtype=np.float32)[None, :] + 100.0
+    lo = (200.0 - np.arange(T, dtype=np.float32))[None, :]
+    dn, up = O.run("aroon", {"high": h, "low": lo}, period=p)
+    assert np.isnan(up[0, :p]).all() and (up[0, p:] == 100.0).all() and (dn[0, p:] == 100.0).all()
+    flat = np.full((1, T), 50.0, np.float32)
+    dn, up = O.run("aroon", {"high": flat, "low": flat}, period=p)
+    assert (up[0, p:] == 100.0).all() and (dn[0, p:] == 100.0).all()
+    # the highest high 3 bars back, the lowest low at the window's oldest bar
+    h2 = np.full((1, 12), 10.0, np.float32)
+    h2[0, 8] = 20.0
+    l2 = np.full((1, 12), 5.0, np.float32)
+    l2[0, 1] = 1.0
+    dn, up = O.run("aroon", {"high": h2, "low": l2}, period=p)
+    assert up[0, 11] == np.float32(100.0) * np.float32(p - 3) / np.float32(p)
+    assert dn[0, 11] == np.float32(0.0)
+    osc = O.run("aroonosc", {"high": h2, "low": l2}, period=p)[0]
+    assert osc[0, 11] == up[0, 11] - dn[0, 11]
+    # a NaN high at the current bar keeps the current bar (strict comparisons)
+    h3 = h2.copy()
+    h3[0, 11] = np.nan
+    assert O.run("aroon", {"high": h3, "low": l2}, period=p)[1][0, 11] == 100.0
+
+
 def test_qstick_infinite_difference_rule():
     a = O.run("qstick", qstick_inf_rows(), period=10)[0]
     assert np.isposinf(a[0, 100:110]).all() and np.isnan(a[0, 110:]).all() and np.isfinite(a[0, 9:100]).all()
