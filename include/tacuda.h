@@ -443,15 +443,23 @@ CTAPI_EXPORT int ct_b200_cdl_count(void);
 CTAPI_EXPORT const char* ct_b200_cdl_name(int pattern);
 CTAPI_EXPORT int ct_b200_cdl_lookback(int pattern);
 
-/* Allocation-free look-back launch (no counterpart in the reference): the jobs
- * of a uniform batch (no candle jobs) on the look-back engine, with its scratch
- * in a static 8 MiB device array per device instead of the stream-ordered pool.
- * The batch must need at most 8 MiB of scratch: 256 B plus 144 B per
- * (round of a row, recurrence stage); larger batches fail with
+/* Allocation-free look-back launch (no counterpart in the reference), for
+ * callers that cannot allocate memory on the launch path: services that
+ * reserve all device memory up front and forbid later growth, latency-critical
+ * loops where an allocation (or the pool's first growth) would stall, and code
+ * running while the device is fully committed. The jobs of a uniform batch (no
+ * candle jobs) run on the look-back engine with their scratch in a static
+ * 8 MiB device array per device (held by every GPU that loads the library
+ * until exit) instead of the stream-ordered pool; the call makes no cudaMalloc,
+ * cudaMallocHost or cudaFree, and on stream 0 it reads the device's error word
+ * into a stack variable. The batch must need at most 8 MiB of scratch: 256 B
+ * plus 144 B per (round of a row, recurrence stage); larger batches fail with
  * CT_STATUS_INVALID_ARGUMENT. The first call on a device looks up the array's
  * address and must come before any stream capture. Each call zeroes the
  * scratch on its stream before the launch; calls that overlap in time (other
- * streams or threads) race on the one array and must be serialised. */
+ * streams or threads) race on the one array and must be serialised. On a user
+ * stream a bounded wait that ran out is reported by the next synchronous call
+ * or by ct_b200_take_device_error. */
 CTAPI_EXPORT ctStatus_t ct_b200_fused_lookback_static_d(const ctB200Series* series, const ctB200Job* jobs,
                                                         int numJobs, cudaStream_t stream);
 

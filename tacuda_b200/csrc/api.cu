@@ -898,7 +898,24 @@ ctStatus_t ct_b200_fused_lookback_static_d(const ctB200Series* series, const ctB
   }
   if (e != cudaSuccess) return cuda_fail(CT_STATUS_KERNEL_FAILED, who, e);
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  return finish(stream, who);
+  if (stream != 0) return CT_STATUS_SUCCESS;
+  // stream 0: synchronise, then read the device's error word into a stack
+  // variable (the regular entries read it into a pinned per-thread slot,
+  // which is allocated on a thread's first call)
+  cudaError_t es = cudaStreamSynchronize(0);
+  if (es != cudaSuccess) return cuda_fail(CT_STATUS_DEVICE_ERROR, who, es);
+  int* sticky = tb::sticky_word();
+  int flag = 0;
+  if (sticky) {
+    es = cudaMemcpy(&flag, sticky, sizeof(int), cudaMemcpyDeviceToHost);
+    if (es != cudaSuccess) return cuda_fail(CT_STATUS_DEVICE_ERROR, who, es);
+  }
+  if (flag != 0) {
+    cudaMemset(sticky, 0, sizeof(int));
+    return fail(CT_STATUS_KERNEL_FAILED,
+                std::string(who) + ": a bounded wait of the engine ran out; the outputs are not valid");
+  }
+  return CT_STATUS_SUCCESS;
 }
 
 // ------------------------------------------------------------ alpha API
