@@ -596,8 +596,29 @@ bool plan_split(const Launch& L, int parts, int groups, int smem_optin, Split& s
       if (ok) break;
     }
     sp.G[q] = G;
-    sp.cta0[q + 1] = sp.cta0[q] + (int)((ngroups + sp.G[q] - 1) / sp.G[q]);
   }
+  // CTAs of the partitions with the longest chains first: a CTA lasts about
+  // as long as its slowest warp (a job's measured cost over its team size), so
+  // the long ones start in the first wave and the short ones fill the tail
+  // (13-indicator pass at 4000 x 234: 132 -> 122 us against partition order)
+  double len[kMaxParts];
+  int ord[kMaxParts];
+  for (int q = 0; q < P; ++q) {
+    len[q] = 0.0;
+    ord[q] = q;
+    const Layout& y = sp.lay[q];
+    for (int w = 0; w <= y.nconsumers; ++w)
+      if (y.warp_job[w] >= 0)
+        len[q] = std::max(len[q], (double)family_cost(L.jobs[y.warp_job[w]], y.bp_mask) / (y.warp_team[w] >> 8));
+  }
+  std::stable_sort(ord, ord + P, [&](int a, int b) { return len[a] > len[b]; });
+  Split tmp = sp;
+  for (int i = 0; i < P; ++i) {
+    sp.lay[i] = tmp.lay[ord[i]];
+    sp.G[i] = tmp.G[ord[i]];
+  }
+  sp.cta0[0] = 0;
+  for (int q = 0; q < P; ++q) sp.cta0[q + 1] = sp.cta0[q] + (int)((ngroups + sp.G[q] - 1) / sp.G[q]);
   return true;
 }
 
